@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Benchmark of the fluid hot path: particle-steps/s of FluidSim.step + SplatField.bake.
+
+One particle-step is one particle advanced one frame (all substeps) plus that frame's bake.
+The default workload is the batched configuration: 256 independent scenes (particle counts
+log-uniform over 1k-64k, a 64^3 collider from 8 seeded brushes each, a 64^3 x 3 bake each,
+every third scene also carrying a clay-body shell of ~3k particles baked into a 32^3 volume
+unioned into its collider), all advanced one frame per batched launch captured in one CUDA
+graph. The same scenes stepped one scene per launch sequence give the plain rate reported
+beside it. Inputs are seeded synthetic data (no dataset): jittered lattices of spacing 0.1.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU: one process per GPU under torchrun; each rank steps its own 256 scenes (weak
+scaling, no collective on the data path); timings are the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/sec (step+bake) batched/served vs plain, 1 B200; p99 request latency"
+UNIT = "particle-steps/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scenes", type=int, default=256)
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--small", action="store_true", help="a small case for profiling (16 scenes)")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------
+# Workload
+
+def fluid_opts(n):
+    from clay_engine_b200 import scenes
+
+    o = dict(scenes.CONFIG3["fluid"])
+    o["capacity"] = int(n)
+    return o
+
+
+def build_scenes(root, n_scenes, seed, with_bodies=True):
+    """The batched configuration on this GPU. Returns (sims, bodies, keepalive)."""
+    import torch
+
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    cfg = scenes.CONFIG3
+    counts = scenes.log_uniform_counts(n_scenes, cfg["n_lo"], cfg["n_hi"], seed)
+    sims, bodies, keep = [], [], []
+    bcfg = cfg["body"]
+    shell, shell_n = scenes.surface_net_sphere(bcfg["radius"], bcfg["cell"])
+    for i, n in enumerate(counts):
+        vol = ce.SdfVolume(root, resolution=cfg["collider"]["resolution"], worldSize=24.0, origin=scenes.WORLD_ORIGIN)
+        vol.build(scenes.random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10), hi=(10, 1.0, 10)))
+        world = ce.volumeField(vol)
+        keep += [vol, world]
+        if with_bodies and i % cfg["body_every"] == 0:
+            center = (2.0, -1.4, 1.0)
+            parts, body = scenes.body_records(shell + np.array(center, np.float32), shell_n, center)
+            dp = torch.from_numpy(parts.view(np.uint8)).cuda()
+            db = torch.from_numpy(body.view(np.uint8)).cuda()
+            cloud = ce.bodyCloud(dp, db, 0)
+            box = bcfg["bake_box"]
+            splat = ce.SplatField(root, cloud, radius=(box / bcfg["bake_res"]) * 1.15, resolution=bcfg["bake_res"],
+                                  band=bcfg["band"], worldSize=box)
+            splat.setCenter(center)
+            bodies.append(splat)
+            world = ce.unionField(world, splat.field)
+            keep += [dp, db, splat, world]
+        sim = ce.FluidSim(root, world, fluid_opts(n))
+        side = math.ceil(n ** (1 / 3)) * 0.1
+        p = scenes.lattice_block(int(n), 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i)
+        sim.upload(p)
+        sims.append(sim)
+    return sims, bodies, keep
+
+
+# ---------------------------------------------------------------------------------------
+# Clocks during the timed region
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+# Distributed plumbing
+
+def dist_init(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(ws, x):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(ws, x):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------
+# CPU baseline: the oracle (the f32 restatement of the reference WGSL) on host cores.
+
+def cpu_sample(n_scenes, seed, max_particles, threads):
+    """Runs the oracle on a bounded sample of the batched scenes, one frame each, and returns
+    (particle-steps/s, particles, seconds, sample description)."""
+    from clay_engine_b200 import brushes as _b  # noqa: F401  (brush records for the colliders)
+    from clay_engine_b200 import scenes
+    from oracle import oracle
+    from oracle.fluid_frame import OracleFluid
+
+    oracle.build()
+    cfg = scenes.CONFIG3
+    counts = scenes.log_uniform_counts(n_scenes, cfg["n_lo"], cfg["n_hi"], seed)
+    order = np.argsort(np.abs(np.log(counts) - np.median(np.log(counts))))
+    chosen, total = [], 0
+    for i in order:
+        if total + counts[i] > max_particles and chosen:
+            break
+        chosen.append(int(i))
+        total += int(counts[i])
+    frames = []
+    for i in chosen:
+        vd = oracle.VolumeData(64, 3, scenes.WORLD_ORIGIN, 24.0, 4.0)
+        d, m = oracle.build_brushes(vd, scenes.random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10),
+                                                               hi=(10, 1.0, 10)), threads=threads)
+        vd.dist[:], vd.mat[:] = d, m
+        o = dict(fluid_opts(counts[i]))
+        ref = OracleFluid(oracle, [vd], threads=threads, **o)
+        side = math.ceil(counts[i] ** (1 / 3)) * 0.1
+        ref.upload(scenes.lattice_block(int(counts[i]), 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i))
+        frames.append(ref)
+    t0 = time.perf_counter()
+    for ref in frames:
+        ref.step()
+    dt = time.perf_counter() - t0
+    desc = f"{len(chosen)} of the {n_scenes} batched scenes nearest the median size, {total} particles, 1 frame each"
+    return total / dt, total, dt, desc
+
+
+def reference_arm(args, ws, rank):
+    """--impl reference: the oracle (the reference's algorithm restated on the CPU; the reference
+    itself is WebGPU/TypeScript and cannot run here) timed on host cores."""
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    vals = []
+    for s in range(args.warmup + args.steps):
+        v, total, dt, desc = cpu_sample(args.scenes, 3, 20000, threads)
+        if s >= args.warmup:
+            vals.append((total, dt))
+    tot = sum(t for t, _ in vals)
+    sec = sum(d for _, d in vals)
+    value = tot / sec
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sec / max(len(vals), 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched-256-scenes (bounded CPU sample)", "scenes": args.scenes,
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+
+def load_peaks():
+    try:
+        with open(PEAKS_FILE) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# Algorithmic bytes per unit of each kernel (the compulsory DRAM traffic if every input were
+# read once and every output written once; neighbour re-reads are cache reuse, not counted).
+BYTES_PER_PARTICLE = {
+    "cell_key": 16 + 4,            # pos in, key out
+    "cell_count": 4 + 4 + 4,       # key in, local key + rank out
+    "cell_scatter": 4 + 4 + 4,     # key, rank in, id out
+    "cell_order": 4 + 4 + 32 + 4 + 32,  # id, key in, pos+vel in; id, pos+vel out
+    "density": 16 + 8,             # pos in, density+pressure out
+    "forces_integrate": 16 + 16 + 8 + 4 + 48,  # pos, vel, rho/p, id in; particle record out
+}
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_init(args)
+    if args.impl == "reference":
+        reference_arm(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+
+    import torch
+
+    import clay_engine_b200 as ce
+
+    torch.cuda.set_device(local)
+    root = ce.init(local)
+    n_scenes = 16 if args.small else args.scenes
+    seed = 3 + rank
+    sims, bodies, keep = build_scenes(root, n_scenes, seed)
+    particles = sum(s.particleCount for s in sims)
+    batch = ce.Batch(root, sims, extra_splats=bodies, use_graph=True)
+    stream = torch.cuda.Stream()
+    torch.cuda.synchronize()
+
+    # warm-up (also captures the graph)
+    for _ in range(max(args.warmup, 1)):
+        batch.step(stream)
+    stream.synchronize()
+
+    # ---- device-resident throughput: K batched frames, CUDA events on the launching stream
+    l0 = ce.kernel_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            batch.step(stream)
+        ev1.record(stream)
+        ev1.synchronize()
+    torch.cuda.synchronize()
+    barrier(ws)
+    launches = ce.kernel_launch_count() - l0
+    ms = max_over_ranks(ws, ev0.elapsed_time(ev1))
+    total_particles = sum_over_ranks(ws, particles)
+    value = total_particles * args.steps / (ms / 1000)
+
+    # ---- end to end through the public API: per frame the inputs (every scene's FluidParams)
+    # go up from pinned memory and every scene's ContactList comes back to pinned memory.
+    h_contacts = torch.empty(len(sims) * 528, dtype=torch.uint8, pin_memory=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_steps = max(2, args.steps // 2)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        batch.step(stream)
+        batch.read_contacts_async(h_contacts.data_ptr(), stream)
+        stream.synchronize()
+    e1.record(stream)
+    e1.synchronize()
+    barrier(ws)
+    e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
+    e2e_value = total_particles * e2e_steps / (e2e_ms / 1000)
+
+    # ---- per-kernel times of one frame (events around each launch) for the roofline
+    prof = batch.profile(stream)
+    frame_ms = sum(v[0] for v in prof.values())
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+    peak, peak_kind = load_peaks()
+    roof = None
+    if top[0] in BYTES_PER_PARTICLE:
+        per_launch_bytes = BYTES_PER_PARTICLE[top[0]] * particles
+        avg_ms = top[1][0] / top[1][1]
+        achieved = per_launch_bytes / (avg_ms / 1000) / 1e9
+        roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_ms}
+    else:
+        roof = {"bound": "hbm", "kernel": top[0], "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                "traffic": None, "peak_source": peak_kind}
+
+    # ---- plain path: the same scenes, one scene per launch sequence, no graph
+    plain_value = None
+    if args.plain_steps > 0:
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for s in sims[:4]:
+            s.step(stream)
+        p0.record(stream)
+        for _ in range(args.plain_steps):
+            for s in bodies:
+                s.bake(stream)
+            for s in sims:
+                s.step(stream)
+        p1.record(stream)
+        p1.synchronize()
+        plain_ms = max_over_ranks(ws, p0.elapsed_time(p1))
+        plain_value = total_particles * args.plain_steps / (plain_ms / 1000)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        v, total, dt, desc = cpu_sample(n_scenes, seed, 20000, os.cpu_count() or 1)
+        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port", "sample": desc}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched-256-scenes" if not args.small else "batched-16-scenes",
+                       "scenes_per_gpu": n_scenes, "particles_per_gpu": particles, "substeps": 2,
+                       "bake": "64^3 x 3 mips band 4 (+32^3 x 2 body bakes)", "collider": "64^3 from 8 brushes",
+                       "parallelism": f"{ws} GPU(s), independent scenes per GPU", "cuda_graph": True,
+                       "l2": "working set larger than L2 (no flush needed)"},
+            "plain": {"value": plain_value, "unit": UNIT, "ratio_batched_over_plain":
+                      (value / plain_value) if plain_value else None},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 80 * len(sims) * ws,
+                    "d2h_bytes_per_step": 528 * len(sims) * ws},
+            "gpu_launches": int(launches),
+            "roofline": roof,
+            "kernels_ms_per_frame": {k: round(v[0], 4) for k, v in prof.items()},
+            "frame_ms_unfused": frame_ms,
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+    batch.destroy()
+    for s in sims:
+        s.destroy()
+    root.destroy()
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

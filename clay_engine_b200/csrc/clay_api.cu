@@ -1,0 +1,1541 @@
+// clay_api.cu - host object model behind the C ABI of include/clay_fluid.h.
+//
+// Mirrors the reference's classes: SdfVolume (lib/src/field/volume.ts), volumeField /
+// unionField / offsetField (lib/src/trace/field.ts), SplatField (lib/src/sim/splat.ts) and
+// FluidSim (lib/src/sim/fluid.ts). Host-side derivations are done in binary64 exactly as
+// the reference's JavaScript does them and rounded once to the f32 values the kernels use.
+// Uniforms (FluidParams, VolumeParams, collider descriptors) live in device memory and are
+// rewritten through a pinned staging ring whenever the host copy changes, which is the
+// reference's `uniform.write` before a dispatch.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/clay_fluid.h"
+#include "clay_device.cuh"
+#include "launch.h"
+
+using namespace clay;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(x)                                                                                 \
+  do {                                                                                        \
+    cudaError_t e_ = (x);                                                                     \
+    if (e_ != cudaSuccess) return fail(CLAY_ECUDA, "%s: %s", #x, cudaGetErrorString(e_));     \
+  } while (0)
+
+constexpr int TILE = 8;
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// Context and staging ring.
+struct clay_ctx {
+  int device = 0;
+  std::atomic<uint64_t> bytes{0};
+  // Pinned staging ring for small host->device uniform writes.
+  static constexpr int kSlots = 1024;
+  static constexpr size_t kSlotBytes = 1024;
+  char* ring = nullptr;
+  cudaEvent_t ev[kSlots];
+  bool used[kSlots];
+  int next = 0;
+  std::mutex mu;
+
+  int dev_alloc(void** p, size_t n) {
+    cudaError_t e = cudaMalloc(p, n == 0 ? 16 : n);
+    if (e != cudaSuccess) {
+      *p = nullptr;
+      return fail(CLAY_ENOMEM, "cudaMalloc(%zu bytes): %s", n, cudaGetErrorString(e));
+    }
+    bytes += n;
+    return CLAY_OK;
+  }
+  void dev_free(void* p, size_t n) {
+    if (p) {
+      cudaFree(p);
+      bytes -= n;
+    }
+  }
+  // Enqueues an H2D copy of `n` bytes through a pinned slot; the host buffer may be reused
+  // as soon as this returns.
+  int upload(void* dst, const void* src, size_t n, cudaStream_t s) {
+    if (n > kSlotBytes) {
+      CK(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, s));
+      return CLAY_OK;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    int slot = next;
+    next = (next + 1) % kSlots;
+    if (used[slot]) CK(cudaEventSynchronize(ev[slot]));
+    char* h = ring + static_cast<size_t>(slot) * kSlotBytes;
+    std::memcpy(h, src, n);
+    CK(cudaMemcpyAsync(dst, h, n, cudaMemcpyHostToDevice, s));
+    CK(cudaEventRecord(ev[slot], s));
+    used[slot] = true;
+    return CLAY_OK;
+  }
+};
+
+namespace {
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+};
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+struct clay_volume {
+  clay_ctx* ctx = nullptr;
+  int res = 0, mips = 0;
+  double world = 0, band = 0, gradv = 1, origin[3] = {0, 0, 0};
+  int64_t total = 0;
+  int64_t off[16] = {0};
+  int tile_res[16] = {0};
+  int total_cells = 0;
+  __half* dist = nullptr;
+  __half* mat = nullptr;
+  VolParamsDev h{};
+  VolParamsDev* d = nullptr;
+  bool dirty = true;
+
+  void refresh_uniform() {
+    double half = world / 2;
+    for (int k = 0; k < 3; k++) {
+      h.origin[k] = static_cast<float>(origin[k]);
+      h.center[k] = static_cast<float>(origin[k] + half);
+    }
+    h.voxel = static_cast<float>(world / res);
+    h.extent = static_cast<float>(world);
+    h.half = static_cast<float>(half);
+    h.band = static_cast<float>(band);
+    // volume.ts:302: `layout.$.params.voxelSize * gradScale`, an f32 product.
+    h.grad_h = h.voxel * static_cast<float>(gradv);
+    h.res = res;
+    h.dist = dist;
+    h.mat = mat;
+    dirty = true;
+  }
+  int flush(cudaStream_t s) {
+    if (!dirty) return CLAY_OK;
+    int rc = ctx->upload(d, &h, sizeof(h), s);
+    if (rc == CLAY_OK) dirty = false;
+    return rc;
+  }
+};
+
+struct clay_field {
+  clay_ctx* ctx = nullptr;
+  struct Leaf {
+    clay_volume* vol;
+    double off[3];
+  };
+  std::vector<Leaf> leaves;
+  FieldDev h{};
+  FieldDev* d = nullptr;
+  bool dirty = true;
+
+  void refresh() {
+    std::memset(&h, 0, sizeof(h));
+    h.n = static_cast<int>(leaves.size());
+    for (size_t i = 0; i < leaves.size(); i++) {
+      h.leaf[i].vp = leaves[i].vol->d;
+      bool any = false;
+      for (int k = 0; k < 3; k++) {
+        h.leaf[i].offset[k] = static_cast<float>(leaves[i].off[k]);
+        any = any || leaves[i].off[k] != 0.0;
+      }
+      h.leaf[i].has_offset = any ? 1 : 0;
+    }
+    dirty = true;
+  }
+  int flush(cudaStream_t s) {
+    for (auto& l : leaves) {
+      int rc = l.vol->flush(s);
+      if (rc) return rc;
+    }
+    if (!dirty) return CLAY_OK;
+    int rc = ctx->upload(d, &h, sizeof(h), s);
+    if (rc == CLAY_OK) dirty = false;
+    return rc;
+  }
+};
+
+struct clay_splat {
+  clay_ctx* ctx = nullptr;
+  clay_volume* vol = nullptr;
+  clay_field* field = nullptr;
+  clay_cloud_desc cloud{};
+  double radius = 0, material = 0, band = 0;
+  int res = 0, mips = 0;
+  uint32_t* keys = nullptr;
+  SplatDev h{};
+  SplatDev* d = nullptr;          // cloud in index order
+  SplatDev* d_ordered = nullptr;  // the fluid's cloud in cell order (fluid-owned splats)
+  const uint32_t* order = nullptr;
+  bool desc_dirty = true;
+
+  int flush(cudaStream_t s) {
+    int rc = vol->flush(s);
+    if (rc) return rc;
+    if (!desc_dirty) return CLAY_OK;
+    h.order = nullptr;
+    rc = ctx->upload(d, &h, sizeof(h), s);
+    if (rc) return rc;
+    if (d_ordered) {
+      SplatDev o = h;
+      o.order = order;
+      rc = ctx->upload(d_ordered, &o, sizeof(o), s);
+      if (rc) return rc;
+    }
+    desc_dirty = false;
+    return CLAY_OK;
+  }
+};
+
+struct clay_fluid {
+  clay_ctx* ctx = nullptr;
+  const clay_field* world = nullptr;
+  int64_t capacity = 0;
+  double spacing = 0, h = 0, radius = 0, surf_r = 0, material = 0, band = 0, world_size = 0;
+  double origin[3] = {0, 0, 0};
+  int bucket = 0, bake_res = 0, bake_mips = 0, substeps = 0;
+  // Host state of fluid.ts:134-138.
+  int64_t live = 0, cursor = 0, pending = 0;
+  uint32_t seed = 1;
+  clay_fluid_params frozen{};
+  clay_fluid_params written{};
+  bool written_valid = false;
+  // Derived (fluid.ts:168-182,239-247).
+  double rest = 0, poly6 = 0, spiky = 0, mass = 0;
+  int G = 0;
+  double gorig[3] = {0, 0, 0};
+  int mode = CLAY_MODE_FAST;
+  uint32_t parts_scan = 1;
+  // Device memory.
+  std::vector<DevBuf> bufs;
+  ParticleDev* parts = nullptr;
+  ParamsDev* prm = nullptr;
+  ContactsDev* contacts = nullptr;
+  GridState* gs = nullptr;
+  SceneDev hs{};
+  SceneDev* d_scene = nullptr;
+  clay_splat* surface = nullptr;
+  uint64_t own_bytes = 0;
+
+  template <class T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    int rc = ctx->dev_alloc(&q, sizeof(T) * count);
+    if (rc) return rc;
+    bufs.push_back({q, sizeof(T) * count});
+    own_bytes += sizeof(T) * count;
+    *p = static_cast<T*>(q);
+    return CLAY_OK;
+  }
+};
+
+// ------------------------------------------------------------------------------------------
+namespace {
+
+// SdfVolume mip rule (volume.ts:140-160).
+int volume_mips(int resolution, int requested, bool has_req, int* out) {
+  int mips = requested;
+  if (!has_req) {
+    int halvings = 0;
+    double n = static_cast<double>(resolution) / TILE;
+    while (n == std::floor(n) && std::fmod(n, 2.0) == 0.0) {
+      halvings++;
+      n /= 2;
+    }
+    int lg = static_cast<int>(std::log2(static_cast<double>(resolution) / TILE));
+    mips = std::max(1, std::min(lg, halvings + 1));
+  }
+  if (mips < 1 || mips > kMaxMips)
+    return fail(CLAY_EINVAL, "SdfVolume: %d mip levels is outside the supported 1..%d", mips, kMaxMips);
+  long long need = static_cast<long long>(TILE) << (mips - 1);
+  if (resolution <= 0 || resolution % need != 0)
+    return fail(CLAY_EINVAL, "SdfVolume: resolution %d must be a multiple of %lld for %d mip levels", resolution, need,
+                mips);
+  *out = mips;
+  return CLAY_OK;
+}
+
+int make_volume(clay_ctx* ctx, int res, int mips_req, bool has_mips, double world, const double origin[3], double band,
+                double gradv, clay_volume** out) {
+  int mips = 0;
+  int rc = volume_mips(res, mips_req, has_mips, &mips);
+  if (rc) return rc;
+  clay_volume* v = new clay_volume();
+  v->ctx = ctx;
+  v->res = res;
+  v->mips = mips;
+  v->world = world;
+  v->band = band;
+  v->gradv = gradv;
+  for (int k = 0; k < 3; k++) v->origin[k] = origin[k];
+  int64_t t = 0;
+  int cells = 0;
+  for (int m = 0; m < mips; m++) {
+    int64_t r = res >> m;
+    v->off[m] = t;
+    t += r * r * r;
+    v->tile_res[m] = (res / TILE) >> m;
+    cells += v->tile_res[m] * v->tile_res[m] * v->tile_res[m];
+  }
+  v->total = t;
+  v->total_cells = cells;
+  void* p = nullptr;
+  if ((rc = ctx->dev_alloc(&p, sizeof(__half) * t))) {
+    delete v;
+    return rc;
+  }
+  v->dist = static_cast<__half*>(p);
+  if ((rc = ctx->dev_alloc(&p, sizeof(__half) * t))) {
+    ctx->dev_free(v->dist, sizeof(__half) * t);
+    delete v;
+    return rc;
+  }
+  v->mat = static_cast<__half*>(p);
+  if ((rc = ctx->dev_alloc(&p, sizeof(VolParamsDev)))) {
+    ctx->dev_free(v->dist, sizeof(__half) * t);
+    ctx->dev_free(v->mat, sizeof(__half) * t);
+    delete v;
+    return rc;
+  }
+  v->d = static_cast<VolParamsDev*>(p);
+  // An unwritten volume reads as saturated (+1), not as a surface.
+  std::vector<uint16_t> one(static_cast<size_t>(t), 0x3C00u);
+  cudaMemcpy(v->dist, one.data(), sizeof(uint16_t) * t, cudaMemcpyHostToDevice);
+  cudaMemset(v->mat, 0, sizeof(__half) * t);
+  v->refresh_uniform();
+  cudaMemcpy(v->d, &v->h, sizeof(v->h), cudaMemcpyHostToDevice);
+  v->dirty = false;
+  *out = v;
+  return CLAY_OK;
+}
+
+void free_volume(clay_volume* v) {
+  if (!v) return;
+  v->ctx->dev_free(v->dist, sizeof(__half) * v->total);
+  v->ctx->dev_free(v->mat, sizeof(__half) * v->total);
+  v->ctx->dev_free(v->d, sizeof(VolParamsDev));
+  delete v;
+}
+
+int make_field(clay_ctx* ctx, std::vector<clay_field::Leaf> leaves, clay_field** out) {
+  if (leaves.empty() || leaves.size() > static_cast<size_t>(kMaxLeaves))
+    return fail(CLAY_EINVAL, "a collider holds 1..%d volume leaves, got %zu", kMaxLeaves, leaves.size());
+  clay_field* f = new clay_field();
+  f->ctx = ctx;
+  f->leaves = std::move(leaves);
+  void* p = nullptr;
+  int rc = ctx->dev_alloc(&p, sizeof(FieldDev));
+  if (rc) {
+    delete f;
+    return rc;
+  }
+  f->d = static_cast<FieldDev*>(p);
+  f->refresh();
+  cudaMemcpy(f->d, &f->h, sizeof(f->h), cudaMemcpyHostToDevice);
+  f->dirty = false;
+  *out = f;
+  return CLAY_OK;
+}
+
+void free_field(clay_field* f) {
+  if (!f) return;
+  f->ctx->dev_free(f->d, sizeof(FieldDev));
+  delete f;
+}
+
+int make_splat(clay_ctx* ctx, const clay_cloud_desc* cloud, const clay_splat_opts* o, bool with_order,
+               clay_splat** out) {
+  if (!cloud || !o) return fail(CLAY_EINVAL, "SplatField: cloud and options are required");
+  if (!cloud->positions && cloud->capacity > 0) return fail(CLAY_EINVAL, "SplatField: cloud has no positions");
+  if (cloud->position_stride < 12 && cloud->capacity > 1)
+    return fail(CLAY_EINVAL, "SplatField: position stride %u is below 12 bytes", cloud->position_stride);
+  if (cloud->live_mode > CLAY_LIVE_RANGE) return fail(CLAY_EINVAL, "SplatField: unknown live mode %u", cloud->live_mode);
+  if (cloud->live_mode == CLAY_LIVE_COUNT && !cloud->live_count)
+    return fail(CLAY_EINVAL, "SplatField: CLAY_LIVE_COUNT needs live_count");
+  if (cloud->live_mode == CLAY_LIVE_RANGE && (!cloud->live_first || !cloud->live_range_count))
+    return fail(CLAY_EINVAL, "SplatField: CLAY_LIVE_RANGE needs live_first and live_range_count");
+  // splat.ts:148-153
+  int res = (o->set & CLAY_SPLAT_RESOLUTION) ? o->resolution : 64;
+  bool has_m = (o->set & CLAY_SPLAT_MIP_LEVELS) != 0;
+  int mips = has_m ? o->mip_levels : std::max(1, static_cast<int>(std::log2(static_cast<double>(res) / TILE)));
+  double band = (o->set & CLAY_SPLAT_BAND) ? o->band : 2.0;
+  double material = (o->set & CLAY_SPLAT_MATERIAL) ? o->material : 0.0;
+  double world = (o->set & CLAY_SPLAT_WORLD_SIZE) ? o->world_size : 24.0;
+  double origin[3] = {-12, -4, -12};
+  if (o->set & CLAY_SPLAT_ORIGIN)
+    for (int k = 0; k < 3; k++) origin[k] = o->origin[k];
+  if (!(o->radius >= 0)) return fail(CLAY_EINVAL, "SplatField: radius must be a non-negative number");
+  clay_volume* vol = nullptr;
+  int rc = make_volume(ctx, res, mips, true, world, origin, band, 1.0, &vol);
+  if (rc) return rc;
+  clay_splat* s = new clay_splat();
+  s->ctx = ctx;
+  s->vol = vol;
+  s->cloud = *cloud;
+  s->radius = o->radius;
+  s->material = material;
+  s->band = band;
+  s->res = res;
+  s->mips = vol->mips;
+  rc = make_field(ctx, {{vol, {0, 0, 0}}}, &s->field);
+  if (rc) {
+    free_volume(vol);
+    delete s;
+    return rc;
+  }
+  void* p = nullptr;
+  if ((rc = ctx->dev_alloc(&p, sizeof(uint32_t) * vol->total))) goto fail_out;
+  s->keys = static_cast<uint32_t*>(p);
+  // The key grid holds 65535 between bakes (see k_resolve).
+  {
+    std::vector<uint32_t> sat(static_cast<size_t>(vol->total), 65535u);
+    cudaMemcpy(s->keys, sat.data(), sizeof(uint32_t) * vol->total, cudaMemcpyHostToDevice);
+    // The material channel is the constant `material` (splat.ts:273): written once here.
+    uint16_t mh;
+    __half hm = __float2half_rn(static_cast<float>(material));
+    std::memcpy(&mh, &hm, 2);
+    std::vector<uint16_t> mv(static_cast<size_t>(vol->total), mh);
+    cudaMemcpy(vol->mat, mv.data(), sizeof(uint16_t) * vol->total, cudaMemcpyHostToDevice);
+    // Before the first bake the volume reads as the clear value 65535 -> +1.
+  }
+  if ((rc = ctx->dev_alloc(&p, sizeof(SplatDev)))) goto fail_out;
+  s->d = static_cast<SplatDev*>(p);
+  if (with_order) {
+    if ((rc = ctx->dev_alloc(&p, sizeof(SplatDev)))) goto fail_out;
+    s->d_ordered = static_cast<SplatDev*>(p);
+  }
+  {
+    SplatDev& h = s->h;
+    std::memset(&h, 0, sizeof(h));
+    h.pos = static_cast<const char*>(cloud->positions);
+    h.nrm = static_cast<const char*>(cloud->normals);
+    h.quat = cloud->rotation;
+    h.live_count = cloud->live_count;
+    h.live_first = cloud->live_first;
+    h.live_range_count = cloud->live_range_count;
+    h.keys = s->keys;
+    h.dist_out = vol->dist;
+    h.key_capture = nullptr;
+    h.vp = vol->d;
+    h.pos_stride = cloud->position_stride;
+    h.nrm_stride = cloud->normal_stride;
+    h.capacity = cloud->capacity;
+    h.live_mode = cloud->live_mode;
+    h.mips = vol->mips;
+    h.radius = static_cast<float>(o->radius);
+    for (int m = 0; m < vol->mips; m++) {
+      // splat.ts:215-238 with voxelSizeAt(m) = (worldSize / resolution) * 2**m (volume.ts:165,336).
+      double voxel = (world / res) * std::pow(2.0, m);
+      double bw = band * voxel;
+      h.r[m] = res >> m;
+      h.off[m] = vol->off[m];
+      h.voxel[m] = static_cast<float>(voxel);
+      h.bw[m] = static_cast<float>(bw);
+      h.reach[m] = static_cast<float>(o->radius + bw);
+      h.inv_voxel[m] = static_cast<float>(1 / voxel);
+    }
+    h.total = vol->total;
+    s->desc_dirty = true;
+    cudaStream_t st = nullptr;
+    rc = s->flush(st);
+    if (rc) goto fail_out;
+  }
+  *out = s;
+  return CLAY_OK;
+fail_out:
+  if (s->keys) ctx->dev_free(s->keys, sizeof(uint32_t) * vol->total);
+  if (s->d) ctx->dev_free(s->d, sizeof(SplatDev));
+  if (s->d_ordered) ctx->dev_free(s->d_ordered, sizeof(SplatDev));
+  free_field(s->field);
+  free_volume(vol);
+  delete s;
+  return rc;
+}
+
+void free_splat(clay_splat* s) {
+  if (!s) return;
+  s->ctx->dev_free(s->keys, sizeof(uint32_t) * s->vol->total);
+  s->ctx->dev_free(s->d, sizeof(SplatDev));
+  if (s->d_ordered) s->ctx->dev_free(s->d_ordered, sizeof(SplatDev));
+  free_field(s->field);
+  free_volume(s->vol);
+  delete s;
+}
+
+// Blocks over the cloud's iteration space for every mip (plain bake).
+int splat_bake(clay_splat* s, cudaStream_t st, bool ordered, int64_t iter_n) {
+  int rc = s->flush(st);
+  if (rc) return rc;
+  const SplatDev* d = (ordered && s->d_ordered) ? s->d_ordered : s->d;
+  int64_t n = iter_n;
+  if (n > 0) {
+    int blocks = static_cast<int>((n + kSplatThreads - 1) / kSplatThreads);
+    CK(L_splat(d, nullptr, blocks, s->mips, st));
+  }
+  int64_t quads = (s->vol->total + 3) / 4;
+  int rblocks = static_cast<int>((quads + kResolveThreads - 1) / kResolveThreads);
+  CK(L_resolve(d, nullptr, rblocks, st));
+  return CLAY_OK;
+}
+
+}  // namespace
+
+// ==========================================================================================
+extern "C" {
+
+const char* clay_last_error(void) { return g_err.c_str(); }
+const char* clay_version(void) { return "clay-fluid-b200 0.1 (sm_100a)"; }
+uint64_t clay_kernel_launch_count(void) { return clay::launch_count(); }
+
+int clay_ctx_create(int device, clay_ctx** out) {
+  if (!out) return fail(CLAY_EINVAL, "clay_ctx_create: out is NULL");
+  int n = 0;
+  CK(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return fail(CLAY_EINVAL, "clay_ctx_create: device %d of %d", device, n);
+  CK(cudaSetDevice(device));
+  clay_ctx* c = new clay_ctx();
+  c->device = device;
+  cudaError_t e = cudaMallocHost(&c->ring, clay_ctx::kSlots * clay_ctx::kSlotBytes);
+  if (e != cudaSuccess) {
+    delete c;
+    return fail(CLAY_ECUDA, "cudaMallocHost: %s", cudaGetErrorString(e));
+  }
+  for (int i = 0; i < clay_ctx::kSlots; i++) {
+    cudaEventCreateWithFlags(&c->ev[i], cudaEventDisableTiming);
+    c->used[i] = false;
+  }
+  *out = c;
+  return CLAY_OK;
+}
+
+void clay_ctx_destroy(clay_ctx* ctx) {
+  if (!ctx) return;
+  cudaDeviceSynchronize();
+  for (int i = 0; i < clay_ctx::kSlots; i++) cudaEventDestroy(ctx->ev[i]);
+  cudaFreeHost(ctx->ring);
+  delete ctx;
+}
+
+int clay_ctx_bytes_in_use(const clay_ctx* ctx, uint64_t* out) {
+  if (!ctx || !out) return fail(CLAY_EINVAL, "clay_ctx_bytes_in_use: NULL argument");
+  *out = ctx->bytes.load();
+  return CLAY_OK;
+}
+
+// ---- SdfVolume ----------------------------------------------------------------------------
+int clay_volume_create(clay_ctx* ctx, const clay_volume_opts* o, clay_volume** out) {
+  if (!ctx || !out) return fail(CLAY_EINVAL, "clay_volume_create: NULL argument");
+  clay_volume_opts d{};
+  if (o) d = *o;
+  int res = (d.set & CLAY_VOL_RESOLUTION) ? d.resolution : 128;
+  double world = (d.set & CLAY_VOL_WORLD_SIZE) ? d.world_size : 16.0;
+  double band = (d.set & CLAY_VOL_BAND) ? d.band : 4.0;
+  double gv = (d.set & CLAY_VOL_GRADIENT_VOXELS) ? d.gradient_voxels : 1.0;
+  double origin[3] = {0, 0, 0};
+  if (d.set & CLAY_VOL_ORIGIN)
+    for (int k = 0; k < 3; k++) origin[k] = d.origin[k];
+  return make_volume(ctx, res, d.mip_levels, (d.set & CLAY_VOL_MIP_LEVELS) != 0, world, origin, band, gv, out);
+}
+
+void clay_volume_destroy(clay_volume* v) { free_volume(v); }
+
+int clay_volume_get_info(const clay_volume* v, clay_volume_info* out) {
+  if (!v || !out) return fail(CLAY_EINVAL, "clay_volume_get_info: NULL argument");
+  std::memset(out, 0, sizeof(*out));
+  out->resolution = v->res;
+  out->mip_levels = v->mips;
+  out->world_size = v->world;
+  out->voxel_size = v->world / v->res;
+  out->band = v->band;
+  for (int k = 0; k < 3; k++) out->origin[k] = v->origin[k];
+  for (int m = 0; m < v->mips; m++) {
+    out->tile_res_per_mip[m] = v->tile_res[m];
+    out->level_offset[m] = v->off[m];
+  }
+  out->total_voxels = v->total;
+  out->total_cells = v->total_cells;
+  return CLAY_OK;
+}
+
+int clay_volume_set_origin(clay_volume* v, double x, double y, double z) {
+  if (!v) return fail(CLAY_EINVAL, "clay_volume_set_origin: NULL volume");
+  v->origin[0] = x;
+  v->origin[1] = y;
+  v->origin[2] = z;
+  v->refresh_uniform();
+  return CLAY_OK;
+}
+
+double clay_volume_voxel_size_at(const clay_volume* v, int mip) {
+  if (!v) return 0;
+  return (v->world / v->res) * std::pow(2.0, mip);
+}
+
+int clay_volume_device_planes(clay_volume* v, void** dist, void** mat) {
+  if (!v) return fail(CLAY_EINVAL, "clay_volume_device_planes: NULL volume");
+  if (dist) *dist = v->dist;
+  if (mat) *mat = v->mat;
+  return CLAY_OK;
+}
+
+int clay_volume_upload(clay_volume* v, const uint16_t* dist, const uint16_t* mat, void* stream) {
+  if (!v) return fail(CLAY_EINVAL, "clay_volume_upload: NULL volume");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (dist) CK(cudaMemcpyAsync(v->dist, dist, sizeof(uint16_t) * v->total, cudaMemcpyHostToDevice, s));
+  if (mat) CK(cudaMemcpyAsync(v->mat, mat, sizeof(uint16_t) * v->total, cudaMemcpyHostToDevice, s));
+  return CLAY_OK;
+}
+
+int clay_volume_download(const clay_volume* v, uint16_t* dist, uint16_t* mat, void* stream) {
+  if (!v) return fail(CLAY_EINVAL, "clay_volume_download: NULL volume");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (dist) CK(cudaMemcpyAsync(dist, v->dist, sizeof(uint16_t) * v->total, cudaMemcpyDeviceToHost, s));
+  if (mat) CK(cudaMemcpyAsync(mat, v->mat, sizeof(uint16_t) * v->total, cudaMemcpyDeviceToHost, s));
+  return CLAY_OK;
+}
+
+int clay_volume_download_rgba16f(const clay_volume* v, int mip, uint16_t* rgba, void* stream) {
+  if (!v || !rgba) return fail(CLAY_EINVAL, "clay_volume_download_rgba16f: NULL argument");
+  if (mip < 0 || mip >= v->mips) return fail(CLAY_EINVAL, "mip %d out of range 0..%d", mip, v->mips - 1);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int64_t r = v->res >> mip;
+  int64_t n = r * r * r;
+  std::vector<uint16_t> d(n), m(n);
+  CK(cudaMemcpyAsync(d.data(), v->dist + v->off[mip], sizeof(uint16_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(m.data(), v->mat + v->off[mip], sizeof(uint16_t) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int64_t i = 0; i < n; i++) {
+    rgba[4 * i] = d[i];
+    rgba[4 * i + 1] = m[i];
+    rgba[4 * i + 2] = 0x0000u;
+    rgba[4 * i + 3] = 0x3C00u;
+  }
+  return CLAY_OK;
+}
+
+int clay_volume_build_brushes(clay_volume* v, const clay_brush* brushes, int count, void* stream) {
+  if (!v) return fail(CLAY_EINVAL, "clay_volume_build_brushes: NULL volume");
+  if (count < 0 || (count > 0 && !brushes)) return fail(CLAY_EINVAL, "clay_volume_build_brushes: bad brush list");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int n = std::min(count, 256);  // builder.ts:57,148-153
+  BrushDev* db = nullptr;
+  void* p = nullptr;
+  int rc = v->ctx->dev_alloc(&p, sizeof(BrushDev) * std::max(n, 1));
+  if (rc) return rc;
+  db = static_cast<BrushDev*>(p);
+  if (n > 0) CK(cudaMemcpyAsync(db, brushes, sizeof(BrushDev) * n, cudaMemcpyHostToDevice, s));
+  for (int m = 0; m < v->mips; m++) {
+    double voxel = (v->world / v->res) * std::pow(2.0, m);
+    double tile_size = voxel * TILE;
+    double bw = v->band * voxel;
+    BuildLevelDev L;
+    L.dist = v->dist + v->off[m];
+    L.mat = v->mat + v->off[m];
+    L.R = v->res >> m;
+    L.tiles = v->tile_res[m];
+    // The builder bakes the origin the volume had at construction (builder.ts:75).
+    L.ox = static_cast<float>(v->origin[0]);
+    L.oy = static_cast<float>(v->origin[1]);
+    L.oz = static_cast<float>(v->origin[2]);
+    L.voxel = static_cast<float>(voxel);
+    L.tile_size = static_cast<float>(tile_size);
+    L.tile_half = static_cast<float>(tile_size / 2);
+    L.bw = static_cast<float>(bw);
+    L.empty = static_cast<float>(bw * 4);
+    CK(L_build(L, db, n, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  v->ctx->dev_free(db, sizeof(BrushDev) * std::max(n, 1));
+  return CLAY_OK;
+}
+
+// ---- TracedField --------------------------------------------------------------------------
+int clay_field_from_volume(clay_volume* vol, clay_field** out) {
+  if (!vol || !out) return fail(CLAY_EINVAL, "clay_field_from_volume: NULL argument");
+  return make_field(vol->ctx, {{vol, {0, 0, 0}}}, out);
+}
+
+int clay_field_union(const clay_field* a, const clay_field* b, clay_field** out) {
+  if (!a || !b || !out) return fail(CLAY_EINVAL, "clay_field_union: NULL argument");
+  std::vector<clay_field::Leaf> l = a->leaves;
+  l.insert(l.end(), b->leaves.begin(), b->leaves.end());
+  return make_field(a->ctx, std::move(l), out);
+}
+
+int clay_field_offset(const clay_field* f, double dx, double dy, double dz, clay_field** out) {
+  if (!f || !out) return fail(CLAY_EINVAL, "clay_field_offset: NULL argument");
+  std::vector<clay_field::Leaf> l = f->leaves;
+  for (auto& x : l) {
+    x.off[0] += dx;
+    x.off[1] += dy;
+    x.off[2] += dz;
+  }
+  return make_field(f->ctx, std::move(l), out);
+}
+
+int clay_field_set_offset(clay_field* f, double dx, double dy, double dz) {
+  if (!f) return fail(CLAY_EINVAL, "clay_field_set_offset: NULL field");
+  for (auto& x : f->leaves) {
+    x.off[0] = dx;
+    x.off[1] = dy;
+    x.off[2] = dz;
+  }
+  f->refresh();
+  return CLAY_OK;
+}
+
+void clay_field_destroy(clay_field* f) { free_field(f); }
+
+int clay_field_query(const clay_field* f, const float* pts, int n, float* sxy, float* nrm, void* stream) {
+  if (!f || n < 0 || (n > 0 && (!pts || !sxy || !nrm))) return fail(CLAY_EINVAL, "clay_field_query: bad argument");
+  if (n == 0) return CLAY_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = const_cast<clay_field*>(f)->flush(s);
+  if (rc) return rc;
+  float *dp = nullptr, *ds = nullptr, *dn = nullptr;
+  CK(cudaMalloc(&dp, sizeof(float) * 3 * n));
+  CK(cudaMalloc(&ds, sizeof(float) * 2 * n));
+  CK(cudaMalloc(&dn, sizeof(float) * 3 * n));
+  CK(cudaMemcpyAsync(dp, pts, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
+  CK(L_field_query(f->d, dp, n, ds, dn, s));
+  CK(cudaMemcpyAsync(sxy, ds, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(nrm, dn, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  cudaFree(dp);
+  cudaFree(ds);
+  cudaFree(dn);
+  return CLAY_OK;
+}
+
+// ---- SplatField ---------------------------------------------------------------------------
+int clay_splat_create(clay_ctx* ctx, const clay_cloud_desc* cloud, const clay_splat_opts* opts, clay_splat** out) {
+  if (!ctx || !out) return fail(CLAY_EINVAL, "clay_splat_create: NULL argument");
+  return make_splat(ctx, cloud, opts, false, out);
+}
+
+void clay_splat_destroy(clay_splat* s) { free_splat(s); }
+
+int clay_splat_set_center(clay_splat* s, double x, double y, double z) {
+  if (!s) return fail(CLAY_EINVAL, "clay_splat_set_center: NULL splat");
+  double half = s->vol->world / 2;  // splat.ts:284-287
+  return clay_volume_set_origin(s->vol, x - half, y - half, z - half);
+}
+
+int clay_splat_bake(clay_splat* s, void* stream) {
+  if (!s) return fail(CLAY_EINVAL, "clay_splat_bake: NULL splat");
+  return splat_bake(s, static_cast<cudaStream_t>(stream), false, s->cloud.capacity);
+}
+
+clay_volume* clay_splat_volume(clay_splat* s) { return s ? s->vol : nullptr; }
+clay_field* clay_splat_field(clay_splat* s) { return s ? s->field : nullptr; }
+
+int clay_splat_capture_keys(clay_splat* s, uint32_t* keys_device) {
+  if (!s) return fail(CLAY_EINVAL, "clay_splat_capture_keys: NULL splat");
+  s->h.key_capture = keys_device;
+  s->desc_dirty = true;
+  return CLAY_OK;
+}
+
+// ---- FluidSim -----------------------------------------------------------------------------
+static int fluid_derive(clay_fluid* f) {
+  // fluid.ts:168-182
+  double h = f->h;
+  f->poly6 = 315 / (64 * M_PI * std::pow(h, 9));
+  f->spiky = -45 / (M_PI * std::pow(h, 6));
+  f->mass = std::pow(f->spacing, 3);
+  double rest = 0;
+  int reach = static_cast<int>(std::ceil(h / f->spacing));
+  for (int z = -reach; z <= reach; z++)
+    for (int y = -reach; y <= reach; y++)
+      for (int x = -reach; x <= reach; x++) {
+        double r2 = static_cast<double>(x * x + y * y + z * z) * f->spacing * f->spacing;
+        if (r2 < h * h) rest += f->mass * f->poly6 * std::pow(h * h - r2, 3);
+      }
+  f->rest = rest;
+  // fluid.ts:239-244
+  double g = std::ceil(f->world_size / h) + 2;
+  if (!(g >= 3 && g <= 1024))
+    return fail(CLAY_EINVAL, "FluidSim: grid resolution %.0f (worldSize / smoothing + 2) must be in 3..1024", g);
+  f->G = static_cast<int>(g);
+  for (int k = 0; k < 3; k++) f->gorig[k] = f->origin[k] - h;
+  return CLAY_OK;
+}
+
+static void fill_scene(clay_fluid* f) {
+  SceneDev& s = f->hs;
+  s.h = static_cast<float>(f->h);
+  s.h2 = static_cast<float>(f->h * f->h);
+  s.inv_h = static_cast<float>(1 / f->h);
+  s.h6 = static_cast<float>(std::pow(f->h, 6));
+  s.mass = static_cast<float>(f->mass);
+  s.mass_poly6 = static_cast<float>(f->mass * f->poly6);
+  s.spiky = static_cast<float>(f->spiky);
+  s.rest = static_cast<float>(f->rest);
+  s.rest_floor = static_cast<float>(f->rest * 0.1);
+  s.radius = static_cast<float>(f->radius);
+  for (int k = 0; k < 3; k++) {
+    s.gorig[k] = static_cast<float>(f->gorig[k]);
+    // fluid.ts:444-447: walls of the bake volume's box, summed in binary64.
+    s.wlo[k] = static_cast<float>(f->origin[k] + f->radius);
+    s.whi[k] = static_cast<float>(f->origin[k] + f->world_size - f->radius);
+  }
+  s.G = f->G;
+  s.capacity = static_cast<uint32_t>(f->capacity);
+  s.bucket = static_cast<uint32_t>(f->bucket);
+  s.parts_scan = f->parts_scan;
+  s.substeps = f->substeps;
+  s.world = f->world ? f->world->d : nullptr;
+}
+
+int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_opts* opts, clay_fluid** out) {
+  if (!ctx || !out) return fail(CLAY_EINVAL, "clay_fluid_create: NULL argument");
+  clay_fluid_opts o{};
+  if (opts) o = *opts;
+  clay_fluid* f = new clay_fluid();
+  f->ctx = ctx;
+  f->world = world;
+  // fluid.ts:141-160
+  f->capacity = (o.set & CLAY_FLUID_CAPACITY) ? o.capacity : 8192;
+  f->spacing = (o.set & CLAY_FLUID_SPACING) ? o.spacing : 0.45;
+  f->h = (o.set & CLAY_FLUID_SMOOTHING) ? o.smoothing : f->spacing * 2.2;
+  f->bucket = (o.set & CLAY_FLUID_BUCKET) ? o.bucket : 64;
+  f->radius = (o.set & CLAY_FLUID_RADIUS) ? o.radius : f->spacing * 0.5;
+  f->surf_r = (o.set & CLAY_FLUID_SURFACE_RADIUS) ? o.surface_radius : f->spacing * 1.1;
+  f->material = (o.set & CLAY_FLUID_MATERIAL) ? o.material : 0.0;
+  f->bake_res = (o.set & CLAY_FLUID_BAKE_RESOLUTION) ? o.bake_resolution : 64;
+  f->bake_mips = (o.set & CLAY_FLUID_BAKE_MIP_LEVELS)
+                     ? o.bake_mip_levels
+                     : std::max(1, static_cast<int>(std::log2(static_cast<double>(f->bake_res) / TILE)));
+  f->band = (o.set & CLAY_FLUID_BAKE_BAND) ? o.bake_band : 2.0;
+  f->world_size = (o.set & CLAY_FLUID_WORLD_SIZE) ? o.world_size : 24.0;
+  double org[3] = {-12, -4, -12};
+  if (o.set & CLAY_FLUID_ORIGIN)
+    for (int k = 0; k < 3; k++) org[k] = o.origin[k];
+  for (int k = 0; k < 3; k++) f->origin[k] = org[k];
+  f->substeps = (o.set & CLAY_FLUID_SUBSTEPS) ? o.substeps : 3;
+  if (f->capacity <= 0 || f->capacity > (1ll << 30)) {
+    long long cap = static_cast<long long>(f->capacity);
+    delete f;
+    return fail(CLAY_EINVAL, "FluidSim: capacity %lld must be in 1..2^30", cap);
+  }
+  if (!(f->spacing > 0) || !(f->h > 0) || f->bucket <= 0 || f->substeps < 0) {
+    delete f;
+    return fail(CLAY_EINVAL, "FluidSim: spacing, smoothing and bucket must be positive and substeps non-negative");
+  }
+  if (world && world->ctx != ctx) {
+    delete f;
+    return fail(CLAY_EINVAL, "FluidSim: the collider belongs to another context");
+  }
+  int rc = fluid_derive(f);
+  if (rc) {
+    delete f;
+    return rc;
+  }
+  // frozen (fluid.ts:184-203)
+  clay_fluid_params& P = f->frozen;
+  std::memset(&P, 0, sizeof(P));
+  double g[3] = {0, -9.81, 0};
+  if (o.set & CLAY_FLUID_GRAVITY)
+    for (int k = 0; k < 3; k++) g[k] = o.gravity[k];
+  for (int k = 0; k < 3; k++) P.gravity[k] = static_cast<float>(g[k]);
+  P.dt = static_cast<float>(1.0 / 60 / f->substeps);
+  P.emit_radius = static_cast<float>(f->spacing);
+  P.max_speed = static_cast<float>((o.set & CLAY_FLUID_MAX_SPEED) ? o.max_speed : 15);
+  P.stiffness = static_cast<float>((o.set & CLAY_FLUID_STIFFNESS) ? o.stiffness : 220);
+  P.viscosity = static_cast<float>((o.set & CLAY_FLUID_VISCOSITY) ? o.viscosity : 0.4);
+  P.damping = static_cast<float>((o.set & CLAY_FLUID_DAMPING) ? o.damping : 0.995);
+  P.emit_seed = 1;
+  P.contact_depth = static_cast<float>(f->radius * 1.5);
+  // Scan parts: enough blocks that one part covers at most ~32k cells of a full box.
+  int64_t cells = static_cast<int64_t>(f->G) * f->G * f->G;
+  f->parts_scan = static_cast<uint32_t>(std::min<int64_t>(kMaxParts, std::max<int64_t>(1, std::min(cells, f->capacity * 4) / 32768)));
+  const int64_t C = f->capacity;
+  if ((rc = f->alloc(&f->parts, C)) || (rc = f->alloc(&f->prm, 1)) || (rc = f->alloc(&f->contacts, 1)) ||
+      (rc = f->alloc(&f->gs, 1)) || (rc = f->alloc(&f->hs.key, C)) || (rc = f->alloc(&f->hs.rank, C)) ||
+      (rc = f->alloc(&f->hs.tmp, C)) || (rc = f->alloc(&f->hs.sorted_id, C)) || (rc = f->alloc(&f->hs.spos, C)) ||
+      (rc = f->alloc(&f->hs.svel, C)) || (rc = f->alloc(&f->hs.sdp, C)) ||
+      (rc = f->alloc(&f->hs.counts, cells + 1)) || (rc = f->alloc(&f->hs.cell_start, cells + 2)) ||
+      (rc = f->alloc(&f->d_scene, 1))) {
+    clay_fluid_destroy(f);
+    return rc;
+  }
+  f->hs.parts = f->parts;
+  f->hs.prm = f->prm;
+  f->hs.contacts = f->contacts;
+  f->hs.gs = f->gs;
+  CK(cudaMemset(f->parts, 0, sizeof(ParticleDev) * C));
+  CK(cudaMemset(f->contacts, 0, sizeof(ContactsDev)));
+  CK(cudaMemset(f->hs.counts, 0, sizeof(uint32_t) * (cells + 1)));
+  CK(cudaMemset(f->hs.cell_start, 0, sizeof(uint32_t) * (cells + 2)));
+  {
+    GridState gsh;
+    std::memset(&gsh, 0, sizeof(gsh));
+    for (int k = 0; k < 3; k++) {
+      gsh.lo[k] = 0xffffffffu;
+      gsh.hi_inv[k] = 0xffffffffu;
+    }
+    CK(cudaMemcpy(f->gs, &gsh, sizeof(gsh), cudaMemcpyHostToDevice));
+    std::vector<uint32_t> ident(static_cast<size_t>(C));
+    for (int64_t i = 0; i < C; i++) ident[i] = static_cast<uint32_t>(i);
+    CK(cudaMemcpy(f->hs.sorted_id, ident.data(), sizeof(uint32_t) * C, cudaMemcpyHostToDevice));
+  }
+  fill_scene(f);
+  CK(cudaMemcpy(f->d_scene, &f->hs, sizeof(SceneDev), cudaMemcpyHostToDevice));
+  ParamsDev pd;
+  std::memcpy(&pd, &f->frozen, sizeof(pd));
+  CK(cudaMemcpy(f->prm, &pd, sizeof(pd), cudaMemcpyHostToDevice));
+  // The surface (fluid.ts:215-234): live = i < params.count, position = particles[i].pos.
+  clay_cloud_desc cd{};
+  cd.capacity = static_cast<uint32_t>(C);
+  cd.positions = f->parts;
+  cd.position_stride = sizeof(ParticleDev);
+  cd.live_mode = CLAY_LIVE_COUNT;
+  cd.live_count = &f->prm->count;
+  clay_splat_opts so{};
+  so.set = CLAY_SPLAT_MATERIAL | CLAY_SPLAT_RESOLUTION | CLAY_SPLAT_MIP_LEVELS | CLAY_SPLAT_BAND | CLAY_SPLAT_ORIGIN |
+           CLAY_SPLAT_WORLD_SIZE;
+  so.radius = f->surf_r;
+  so.material = f->material;
+  so.resolution = f->bake_res;
+  so.mip_levels = f->bake_mips;
+  so.band = f->band;
+  so.world_size = f->world_size;
+  for (int k = 0; k < 3; k++) so.origin[k] = f->origin[k];
+  rc = make_splat(ctx, &cd, &so, true, &f->surface);
+  if (rc) {
+    clay_fluid_destroy(f);
+    return rc;
+  }
+  f->surface->order = f->hs.sorted_id;
+  f->surface->desc_dirty = true;
+  rc = f->surface->flush(nullptr);
+  if (rc) {
+    clay_fluid_destroy(f);
+    return rc;
+  }
+  CK(cudaDeviceSynchronize());
+  *out = f;
+  return CLAY_OK;
+}
+
+void clay_fluid_destroy(clay_fluid* f) {
+  if (!f) return;
+  for (auto& b : f->bufs) f->ctx->dev_free(b.p, b.n);
+  free_splat(f->surface);
+  delete f;
+}
+
+int clay_fluid_set_mode(clay_fluid* f, int mode) {
+  if (!f) return fail(CLAY_EINVAL, "clay_fluid_set_mode: NULL sim");
+  if (mode != CLAY_MODE_FAST && mode != CLAY_MODE_REFERENCE) return fail(CLAY_EINVAL, "unknown mode %d", mode);
+  f->mode = mode;
+  return CLAY_OK;
+}
+
+int clay_fluid_spawn(clay_fluid* f, int64_t n, const double pos[3], const double vel[3], const double* spread) {
+  if (!f || !pos || !vel) return fail(CLAY_EINVAL, "clay_fluid_spawn: NULL argument");
+  // fluid.ts:511-525
+  double sp = spread ? *spread : f->spacing * std::cbrt(static_cast<double>(std::max<int64_t>(n, 1))) * 0.62;
+  f->pending = std::max<int64_t>(0, std::min(n, f->capacity));
+  for (int k = 0; k < 3; k++) {
+    f->frozen.emit_pos[k] = static_cast<float>(pos[k]);
+    f->frozen.emit_vel[k] = static_cast<float>(vel[k]);
+  }
+  f->frozen.emit_radius = static_cast<float>(sp);
+  f->frozen.emit_seed = f->seed++;
+  return CLAY_OK;
+}
+
+int clay_fluid_configure(clay_fluid* f, const clay_fluid_params* p, uint32_t mask) {
+  if (!f || !p) return fail(CLAY_EINVAL, "clay_fluid_configure: NULL argument");
+  clay_fluid_params& q = f->frozen;
+  if (mask & CLAY_P_GRAVITY) std::memcpy(q.gravity, p->gravity, sizeof(q.gravity));
+  if (mask & CLAY_P_DT) q.dt = p->dt;
+  if (mask & CLAY_P_EMIT_POS) std::memcpy(q.emit_pos, p->emit_pos, sizeof(q.emit_pos));
+  if (mask & CLAY_P_EMIT_RADIUS) q.emit_radius = p->emit_radius;
+  if (mask & CLAY_P_EMIT_VEL) std::memcpy(q.emit_vel, p->emit_vel, sizeof(q.emit_vel));
+  if (mask & CLAY_P_MAX_SPEED) q.max_speed = p->max_speed;
+  if (mask & CLAY_P_STIFFNESS) q.stiffness = p->stiffness;
+  if (mask & CLAY_P_VISCOSITY) q.viscosity = p->viscosity;
+  if (mask & CLAY_P_DAMPING) q.damping = p->damping;
+  if (mask & CLAY_P_CONTACT_DEPTH) q.contact_depth = p->contact_depth;
+  return CLAY_OK;
+}
+
+namespace {
+// Host bookkeeping of fluid.ts:537-545: the uniform this frame writes.
+clay_fluid_params fluid_frame_params(clay_fluid* f) {
+  int64_t ec = f->pending;
+  f->pending = 0;
+  int64_t base = f->cursor;
+  if (ec > 0) {
+    f->cursor = (base + ec) % f->capacity;
+    f->live = std::min(f->capacity, std::max(f->live, base + ec));
+  }
+  clay_fluid_params p = f->frozen;
+  p.count = static_cast<uint32_t>(f->live);
+  p.emit_base = static_cast<uint32_t>(base);
+  p.emit_count = static_cast<uint32_t>(ec);
+  return p;
+}
+
+// The bookkeeping, then the uniform upload if it differs from the last one written.
+int fluid_begin_frame(clay_fluid* f, cudaStream_t s, uint32_t* emit_count) {
+  clay_fluid_params p = fluid_frame_params(f);
+  const uint32_t ec = p.emit_count;
+  if (!f->written_valid || std::memcmp(&p, &f->written, sizeof(p)) != 0) {
+    int rc = f->ctx->upload(f->prm, &p, sizeof(p), s);
+    if (rc) return rc;
+    f->written = p;
+    f->written_valid = true;
+  }
+  *emit_count = static_cast<uint32_t>(ec);
+  if (f->world) {
+    int rc = const_cast<clay_field*>(f->world)->flush(s);
+    if (rc) return rc;
+  }
+  return CLAY_OK;
+}
+
+int fluid_substep_plain(clay_fluid* f, cudaStream_t s, int sub) {
+  const SceneDev* d = f->d_scene;
+  const int T = kBlock;
+  int pb = static_cast<int>((f->live + T - 1) / T);
+  CK(L_cell_key(d, nullptr, pb, T, sub, s));
+  CK(L_cell_count(d, nullptr, pb, T, sub, s));
+  CK(L_scan_partial(d, nullptr, static_cast<int>(f->parts_scan), sub, s));
+  CK(L_scan_final(d, nullptr, static_cast<int>(f->parts_scan), sub, s));
+  CK(L_cell_scatter(d, nullptr, pb, T, sub, s));
+  CK(L_cell_order(d, nullptr, pb, T, sub, s));
+  if (f->mode == CLAY_MODE_REFERENCE) {
+    CK(L_density_ref(d, nullptr, pb, T, sub, s));
+    CK(L_forces_ref(d, nullptr, pb, T, sub, s));
+  } else {
+    CK(L_density_fast(d, nullptr, pb, T, sub, s));
+    CK(L_forces_fast(d, nullptr, pb, T, sub, s));
+  }
+  return CLAY_OK;
+}
+}  // namespace
+
+int clay_fluid_step(clay_fluid* f, void* stream) {
+  if (!f) return fail(CLAY_EINVAL, "clay_fluid_step: NULL sim");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  uint32_t ec = 0;
+  int rc = fluid_begin_frame(f, s, &ec);
+  if (rc) return rc;
+  if (ec > 0) CK(L_emit(f->d_scene, nullptr, static_cast<int>((ec + kBlock - 1) / kBlock), kBlock, s));
+  // fluid.ts:550: the substep loop is skipped entirely when nothing is alive.
+  for (int sub = 0; sub < f->substeps && f->live > 0; sub++) {
+    rc = fluid_substep_plain(f, s, sub);
+    if (rc) return rc;
+  }
+  bool ordered = f->substeps > 0 && f->live > 0;
+  return splat_bake(f->surface, s, ordered, ordered ? f->live : f->capacity);
+}
+
+int64_t clay_fluid_particle_count(const clay_fluid* f) { return f ? f->live : -1; }
+
+int clay_fluid_get_params(const clay_fluid* f, clay_fluid_params* out) {
+  if (!f || !out) return fail(CLAY_EINVAL, "clay_fluid_get_params: NULL argument");
+  *out = f->frozen;
+  out->count = static_cast<uint32_t>(f->live);
+  return CLAY_OK;
+}
+
+int clay_fluid_read_contacts_async(clay_fluid* f, clay_contact_list* host, void* stream) {
+  if (!f || !host) return fail(CLAY_EINVAL, "clay_fluid_read_contacts_async: NULL argument");
+  static_assert(sizeof(clay_contact_list) == sizeof(ContactsDev), "ContactList layout");
+  CK(cudaMemcpyAsync(host, f->contacts, sizeof(ContactsDev), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+  return CLAY_OK;
+}
+
+int clay_fluid_particles_device(clay_fluid* f, clay_fluid_particle** ptr, uint32_t* stride) {
+  if (!f) return fail(CLAY_EINVAL, "clay_fluid_particles_device: NULL sim");
+  static_assert(sizeof(clay_fluid_particle) == sizeof(ParticleDev), "FluidParticle layout");
+  if (ptr) *ptr = reinterpret_cast<clay_fluid_particle*>(f->parts);
+  if (stride) *stride = sizeof(ParticleDev);
+  return CLAY_OK;
+}
+
+int clay_fluid_upload(clay_fluid* f, const clay_fluid_particle* host, int64_t count, void* stream) {
+  if (!f || (count > 0 && !host)) return fail(CLAY_EINVAL, "clay_fluid_upload: NULL argument");
+  if (count < 0 || count > f->capacity)
+    return fail(CLAY_EINVAL, "clay_fluid_upload: count %lld outside 0..capacity %lld", static_cast<long long>(count),
+                static_cast<long long>(f->capacity));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (count > 0) CK(cudaMemcpyAsync(f->parts, host, sizeof(ParticleDev) * count, cudaMemcpyHostToDevice, s));
+  f->live = count;
+  f->cursor = count % f->capacity;
+  f->pending = 0;
+  return CLAY_OK;
+}
+
+int clay_fluid_download(const clay_fluid* f, clay_fluid_particle* host, int64_t count, void* stream) {
+  if (!f || (count > 0 && !host)) return fail(CLAY_EINVAL, "clay_fluid_download: NULL argument");
+  if (count < 0 || count > f->capacity) return fail(CLAY_EINVAL, "clay_fluid_download: count out of range");
+  if (count > 0)
+    CK(cudaMemcpyAsync(host, f->parts, sizeof(ParticleDev) * count, cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+  return CLAY_OK;
+}
+
+int clay_fluid_cell_indices(clay_fluid* f, uint32_t* host, void* stream) {
+  if (!f || !host) return fail(CLAY_EINVAL, "clay_fluid_cell_indices: NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (f->live == 0) return CLAY_OK;
+  uint32_t* d = nullptr;
+  CK(cudaMalloc(&d, sizeof(uint32_t) * f->live));
+  // the uniform's count must be current for the kernel
+  clay_fluid_params p = f->frozen;
+  p.count = static_cast<uint32_t>(f->live);
+  p.emit_base = static_cast<uint32_t>(f->cursor);
+  p.emit_count = 0;
+  if (!f->written_valid || std::memcmp(&p, &f->written, sizeof(p)) != 0) {
+    int rc = f->ctx->upload(f->prm, &p, sizeof(p), s);
+    if (rc) return rc;
+    f->written = p;
+    f->written_valid = true;
+  }
+  CK(L_cell_index(f->d_scene, d, static_cast<int>(f->live), s));
+  CK(cudaMemcpyAsync(host, d, sizeof(uint32_t) * f->live, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  cudaFree(d);
+  return CLAY_OK;
+}
+
+clay_splat* clay_fluid_surface(clay_fluid* f) { return f ? f->surface : nullptr; }
+clay_field* clay_fluid_field(clay_fluid* f) { return f ? f->surface->field : nullptr; }
+
+int clay_fluid_get_info(const clay_fluid* f, clay_fluid_info* out) {
+  if (!f || !out) return fail(CLAY_EINVAL, "clay_fluid_get_info: NULL argument");
+  std::memset(out, 0, sizeof(*out));
+  out->capacity = f->capacity;
+  out->substeps = f->substeps;
+  out->bucket = f->bucket;
+  out->grid_res = f->G;
+  out->smoothing = f->h;
+  out->rest_density = f->rest;
+  for (int k = 0; k < 3; k++) out->grid_origin[k] = f->gorig[k];
+  out->spacing = f->spacing;
+  out->radius = f->radius;
+  out->device_bytes = f->own_bytes;
+  return CLAY_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// Batched stepping.
+struct clay_batch {
+  clay_ctx* ctx = nullptr;
+  std::vector<clay_fluid*> sims;
+  std::vector<clay_splat*> extra;
+  int mode = CLAY_MODE_FAST;
+  int max_substeps = 0;
+  clay_batch_tuning tune{kBlock, kSplatThreads, 1};
+  // device tables
+  SceneDev* d_scenes = nullptr;
+  size_t n_scenes_alloc = 0;
+  SplatDev* d_extra = nullptr;   // extra clouds, index order
+  SplatDev* d_surf = nullptr;    // fluid surfaces, cell order
+  Work *w_part = nullptr, *w_emit = nullptr, *w_scan = nullptr, *w_xsplat = nullptr, *w_xres = nullptr,
+       *w_ssplat = nullptr, *w_sres = nullptr;
+  int n_part = 0, n_emit = 0, n_scan = 0, n_xsplat = 0, n_xres = 0, n_ssplat = 0, n_sres = 0;
+  std::vector<DevBuf> bufs;
+  bool built = false;
+  cudaGraphExec_t graph = nullptr;
+  int64_t launches_per_step = 0;
+  // The scenes' FluidParams, contiguous, written from pinned memory in one copy per frame
+  // (double-buffered so the host never overwrites a copy still in flight).
+  ParamsDev* d_params = nullptr;
+  ParamsDev* h_params[2] = {nullptr, nullptr};
+  cudaEvent_t params_ev[2] = {nullptr, nullptr};
+  bool params_used[2] = {false, false};
+  int params_slot = 0;
+  ContactsDev* d_contacts = nullptr;
+
+  ~clay_batch() {
+    release();
+    for (int k = 0; k < 2; k++) {
+      if (h_params[k]) cudaFreeHost(h_params[k]);
+      if (params_ev[k]) cudaEventDestroy(params_ev[k]);
+    }
+  }
+  void release() {
+    if (graph) {
+      cudaGraphExecDestroy(graph);
+      graph = nullptr;
+    }
+    for (int k = 0; k < 2; k++) {
+      if (h_params[k]) cudaFreeHost(h_params[k]);
+      h_params[k] = nullptr;
+      params_used[k] = false;
+    }
+    for (auto& b : bufs) ctx->dev_free(b.p, b.n);
+    bufs.clear();
+    built = false;
+  }
+  template <class T>
+  int upload_table(T** d, const std::vector<T>& h) {
+    void* p = nullptr;
+    int rc = ctx->dev_alloc(&p, sizeof(T) * std::max<size_t>(h.size(), 1));
+    if (rc) return rc;
+    bufs.push_back({p, sizeof(T) * std::max<size_t>(h.size(), 1)});
+    if (!h.empty()) CK(cudaMemcpy(p, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    *d = static_cast<T*>(p);
+    return CLAY_OK;
+  }
+};
+
+namespace {
+
+void add_splat_work(std::vector<Work>& ws, std::vector<Work>& wr, uint32_t obj, const clay_splat* s, int64_t iter_n,
+                    int splat_block) {
+  for (int m = 0; m < s->mips; m++)
+    for (int64_t f = 0; f < iter_n; f += splat_block)
+      ws.push_back({obj, static_cast<uint32_t>(m), static_cast<uint32_t>(f),
+                    static_cast<uint32_t>(std::min<int64_t>(splat_block, iter_n - f))});
+  int64_t quads = (s->vol->total + 3) / 4;
+  for (int64_t q = 0; q < quads; q += kResolveThreads) wr.push_back({obj, 0u, static_cast<uint32_t>(q), kResolveThreads});
+}
+
+// Work tables sized by capacity: blocks past a scene's live count exit at once, so the
+// tables (and a captured graph) stay valid while the live counts grow.
+int batch_build(clay_batch* b) {
+  b->release();
+  const int T = b->tune.sph_block;
+  std::vector<SceneDev> scenes;
+  std::vector<Work> wp, we, wsc;
+  b->max_substeps = 0;
+  for (size_t i = 0; i < b->sims.size(); i++) {
+    clay_fluid* f = b->sims[i];
+    scenes.push_back(f->hs);
+    b->max_substeps = std::max(b->max_substeps, f->substeps);
+    uint32_t obj = static_cast<uint32_t>(i);
+    for (int64_t x = 0; x < f->capacity; x += T)
+      wp.push_back({obj, 0u, static_cast<uint32_t>(x), static_cast<uint32_t>(std::min<int64_t>(T, f->capacity - x))});
+    int eb = static_cast<int>(std::min<int64_t>(8, (f->capacity + T - 1) / T));
+    for (int e = 0; e < eb; e++) we.push_back({obj, 0u, static_cast<uint32_t>(e * T), static_cast<uint32_t>(eb * T)});
+    for (uint32_t p = 0; p < f->parts_scan; p++) wsc.push_back({obj, p, 0u, 0u});
+  }
+  std::vector<SplatDev> xs, ss;
+  std::vector<Work> wxs, wxr, wss, wsr;
+  for (size_t i = 0; i < b->extra.size(); i++) {
+    xs.push_back(b->extra[i]->h);
+    xs.back().order = nullptr;
+    add_splat_work(wxs, wxr, static_cast<uint32_t>(i), b->extra[i], b->extra[i]->cloud.capacity, kSplatThreads);
+  }
+  for (size_t i = 0; i < b->sims.size(); i++) {
+    clay_splat* s = b->sims[i]->surface;
+    SplatDev d = s->h;
+    d.order = s->order;
+    ss.push_back(d);
+    add_splat_work(wss, wsr, static_cast<uint32_t>(i), s, b->sims[i]->capacity, kSplatThreads);
+  }
+  int rc;
+  {
+    std::vector<ParamsDev> prm(b->sims.size());
+    for (size_t i = 0; i < b->sims.size(); i++) std::memcpy(&prm[i], &b->sims[i]->frozen, sizeof(ParamsDev));
+    if ((rc = b->upload_table(&b->d_params, prm))) return rc;
+    std::vector<ContactsDev> ct(b->sims.size());
+    if ((rc = b->upload_table(&b->d_contacts, ct))) return rc;
+    for (size_t i = 0; i < b->sims.size(); i++) {
+      scenes[i].prm = b->d_params + i;
+      ss[i].live_count = &b->d_params[i].count;
+    }
+    for (int k = 0; k < 2; k++) {
+      CK(cudaMallocHost(&b->h_params[k], sizeof(ParamsDev) * std::max<size_t>(b->sims.size(), 1)));
+      if (!b->params_ev[k]) CK(cudaEventCreateWithFlags(&b->params_ev[k], cudaEventDisableTiming));
+    }
+  }
+  if ((rc = b->upload_table(&b->d_scenes, scenes)) || (rc = b->upload_table(&b->w_part, wp)) ||
+      (rc = b->upload_table(&b->w_emit, we)) || (rc = b->upload_table(&b->w_scan, wsc)) ||
+      (rc = b->upload_table(&b->d_extra, xs)) || (rc = b->upload_table(&b->d_surf, ss)) ||
+      (rc = b->upload_table(&b->w_xsplat, wxs)) || (rc = b->upload_table(&b->w_xres, wxr)) ||
+      (rc = b->upload_table(&b->w_ssplat, wss)) || (rc = b->upload_table(&b->w_sres, wsr)))
+    return rc;
+  b->n_part = static_cast<int>(wp.size());
+  b->n_emit = static_cast<int>(we.size());
+  b->n_scan = static_cast<int>(wsc.size());
+  b->n_xsplat = static_cast<int>(wxs.size());
+  b->n_xres = static_cast<int>(wxr.size());
+  b->n_ssplat = static_cast<int>(wss.size());
+  b->n_sres = static_cast<int>(wsr.size());
+  b->built = true;
+  return CLAY_OK;
+}
+
+// The passes of one batched frame. Order as in a game frame: the extra clouds (clay-body
+// shells, which the fluids collide with) bake first, then every fluid steps and bakes.
+int batch_enqueue(clay_batch* b, cudaStream_t s) {
+  const int T = b->tune.sph_block;
+  const SceneDev* d = b->d_scenes;
+  if (b->n_xsplat) CK(L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, s));
+  if (b->n_xres) CK(L_resolve(b->d_extra, b->w_xres, b->n_xres, s));
+  if (b->n_part) {
+    CK(L_emit(d, b->w_emit, b->n_emit, T, s));
+    for (int sub = 0; sub < b->max_substeps; sub++) {
+      CK(L_cell_key(d, b->w_part, b->n_part, T, sub, s));
+      CK(L_cell_count(d, b->w_part, b->n_part, T, sub, s));
+      CK(L_scan_partial(d, b->w_scan, b->n_scan, sub, s));
+      CK(L_scan_final(d, b->w_scan, b->n_scan, sub, s));
+      CK(L_cell_scatter(d, b->w_part, b->n_part, T, sub, s));
+      CK(L_cell_order(d, b->w_part, b->n_part, T, sub, s));
+      if (b->mode == CLAY_MODE_REFERENCE) {
+        CK(L_density_ref(d, b->w_part, b->n_part, T, sub, s));
+        CK(L_forces_ref(d, b->w_part, b->n_part, T, sub, s));
+      } else {
+        CK(L_density_fast(d, b->w_part, b->n_part, T, sub, s));
+        CK(L_forces_fast(d, b->w_part, b->n_part, T, sub, s));
+      }
+    }
+  }
+  if (b->n_ssplat) CK(L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, s));
+  if (b->n_sres) CK(L_resolve(b->d_surf, b->w_sres, b->n_sres, s));
+  return CLAY_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int clay_batch_create(clay_ctx* ctx, clay_fluid* const* sims, int n, clay_batch** out) {
+  if (!ctx || !out || n < 0 || (n > 0 && !sims)) return fail(CLAY_EINVAL, "clay_batch_create: bad argument");
+  clay_batch* b = new clay_batch();
+  b->ctx = ctx;
+  for (int i = 0; i < n; i++) {
+    if (!sims[i] || sims[i]->ctx != ctx) {
+      delete b;
+      return fail(CLAY_EINVAL, "clay_batch_create: scene %d is NULL or from another context", i);
+    }
+    b->sims.push_back(sims[i]);
+  }
+  if (n > 0) {
+    b->mode = sims[0]->mode;
+    for (int i = 1; i < n; i++)
+      if (sims[i]->mode != b->mode) {
+        delete b;
+        return fail(CLAY_EINVAL, "clay_batch_create: every scene of a batch must use the same arithmetic mode");
+      }
+  }
+  *out = b;
+  return CLAY_OK;
+}
+
+void clay_batch_destroy(clay_batch* b) { delete b; }
+
+int clay_batch_add_splat(clay_batch* b, clay_splat* s) {
+  if (!b || !s) return fail(CLAY_EINVAL, "clay_batch_add_splat: NULL argument");
+  b->extra.push_back(s);
+  b->release();
+  return CLAY_OK;
+}
+
+int clay_batch_set_tuning(clay_batch* b, const clay_batch_tuning* t) {
+  if (!b || !t) return fail(CLAY_EINVAL, "clay_batch_set_tuning: NULL argument");
+  if (t->sph_block < 64 || t->sph_block > 512 || (t->sph_block & 31))
+    return fail(CLAY_EINVAL, "sph_block %d must be a multiple of 32 in 64..512", t->sph_block);
+  b->tune = *t;
+  b->tune.splat_block = kSplatThreads;
+  b->release();
+  return CLAY_OK;
+}
+
+int clay_batch_get_tuning(const clay_batch* b, clay_batch_tuning* t) {
+  if (!b || !t) return fail(CLAY_EINVAL, "clay_batch_get_tuning: NULL argument");
+  *t = b->tune;
+  return CLAY_OK;
+}
+
+int clay_batch_step(clay_batch* b, void* stream) {
+  if (!b) return fail(CLAY_EINVAL, "clay_batch_step: NULL batch");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc;
+  if (!b->built && (rc = batch_build(b))) return rc;
+  {
+    // this frame's uniforms of every scene (fluid.ts:545), one pinned copy
+    int k = b->params_slot;
+    b->params_slot ^= 1;
+    if (b->params_used[k]) CK(cudaEventSynchronize(b->params_ev[k]));
+    for (size_t i = 0; i < b->sims.size(); i++) {
+      clay_fluid* f = b->sims[i];
+      clay_fluid_params p = fluid_frame_params(f);
+      std::memcpy(&b->h_params[k][i], &p, sizeof(ParamsDev));
+      if (f->world && (rc = const_cast<clay_field*>(f->world)->flush(s))) return rc;
+    }
+    if (!b->sims.empty()) {
+      CK(cudaMemcpyAsync(b->d_params, b->h_params[k], sizeof(ParamsDev) * b->sims.size(), cudaMemcpyHostToDevice, s));
+      CK(cudaEventRecord(b->params_ev[k], s));
+      b->params_used[k] = true;
+    }
+  }
+  for (clay_splat* x : b->extra)
+    if ((rc = x->flush(s))) return rc;
+  for (clay_fluid* f : b->sims)
+    if ((rc = f->surface->flush(s))) return rc;
+  if (!b->tune.use_graph) {
+    uint64_t before = launch_count();
+    rc = batch_enqueue(b, s);
+    b->launches_per_step = static_cast<int64_t>(launch_count() - before);
+    return rc;
+  }
+  if (!b->graph) {
+    // Capture on a private stream so the caller's stream can be the legacy default.
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    uint64_t before = launch_count();
+    rc = batch_enqueue(b, cs);
+    b->launches_per_step = static_cast<int64_t>(launch_count() - before);
+    cudaError_t e = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(CLAY_ECUDA, "cudaStreamEndCapture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(CLAY_ECUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+  }
+  CK(cudaGraphLaunch(b->graph, s));
+  count_launches(static_cast<uint64_t>(b->launches_per_step));
+  return CLAY_OK;
+}
+
+int clay_batch_launches_per_step(const clay_batch* b, int64_t* out) {
+  if (!b || !out) return fail(CLAY_EINVAL, "clay_batch_launches_per_step: NULL argument");
+  *out = b->launches_per_step;
+  return CLAY_OK;
+}
+
+int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int cap, int* n_out) {
+  if (!b || !out || !n_out) return fail(CLAY_EINVAL, "clay_batch_profile: NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc;
+  if (!b->built && (rc = batch_build(b))) return rc;
+  // One frame without the graph, every launch bracketed by events on `stream`.
+  struct Rec {
+    const char* name;
+    cudaEvent_t a, z;
+  };
+  std::vector<Rec> recs;
+  auto timed = [&](const char* name, auto&& launch) -> int {
+    Rec r{name, nullptr, nullptr};
+    CK(cudaEventCreate(&r.a));
+    CK(cudaEventCreate(&r.z));
+    CK(cudaEventRecord(r.a, s));
+    CK(launch());
+    CK(cudaEventRecord(r.z, s));
+    recs.push_back(r);
+    return CLAY_OK;
+  };
+  {
+    int k = b->params_slot;
+    b->params_slot ^= 1;
+    if (b->params_used[k]) CK(cudaEventSynchronize(b->params_ev[k]));
+    for (size_t i = 0; i < b->sims.size(); i++) {
+      clay_fluid_params p = fluid_frame_params(b->sims[i]);
+      std::memcpy(&b->h_params[k][i], &p, sizeof(ParamsDev));
+    }
+    if (!b->sims.empty()) {
+      CK(cudaMemcpyAsync(b->d_params, b->h_params[k], sizeof(ParamsDev) * b->sims.size(), cudaMemcpyHostToDevice, s));
+      CK(cudaEventRecord(b->params_ev[k], s));
+      b->params_used[k] = true;
+    }
+  }
+  const int T = b->tune.sph_block;
+  const SceneDev* d = b->d_scenes;
+  const bool ref = b->mode == CLAY_MODE_REFERENCE;
+  if (b->n_xsplat && (rc = timed("body_splat", [&] { return L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, s); }))) return rc;
+  if (b->n_xres && (rc = timed("body_resolve", [&] { return L_resolve(b->d_extra, b->w_xres, b->n_xres, s); }))) return rc;
+  if (b->n_part) {
+    if ((rc = timed("emit", [&] { return L_emit(d, b->w_emit, b->n_emit, T, s); }))) return rc;
+    for (int sub = 0; sub < b->max_substeps; sub++) {
+      if ((rc = timed("cell_key", [&] { return L_cell_key(d, b->w_part, b->n_part, T, sub, s); }))) return rc;
+      if ((rc = timed("cell_count", [&] { return L_cell_count(d, b->w_part, b->n_part, T, sub, s); }))) return rc;
+      if ((rc = timed("scan_partial", [&] { return L_scan_partial(d, b->w_scan, b->n_scan, sub, s); }))) return rc;
+      if ((rc = timed("scan_final", [&] { return L_scan_final(d, b->w_scan, b->n_scan, sub, s); }))) return rc;
+      if ((rc = timed("cell_scatter", [&] { return L_cell_scatter(d, b->w_part, b->n_part, T, sub, s); }))) return rc;
+      if ((rc = timed("cell_order", [&] { return L_cell_order(d, b->w_part, b->n_part, T, sub, s); }))) return rc;
+      if ((rc = timed("density", [&] {
+             return ref ? L_density_ref(d, b->w_part, b->n_part, T, sub, s) : L_density_fast(d, b->w_part, b->n_part, T, sub, s);
+           })))
+        return rc;
+      if ((rc = timed("forces_integrate", [&] {
+             return ref ? L_forces_ref(d, b->w_part, b->n_part, T, sub, s) : L_forces_fast(d, b->w_part, b->n_part, T, sub, s);
+           })))
+        return rc;
+    }
+  }
+  if (b->n_ssplat && (rc = timed("splat", [&] { return L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, s); }))) return rc;
+  if (b->n_sres && (rc = timed("resolve", [&] { return L_resolve(b->d_surf, b->w_sres, b->n_sres, s); }))) return rc;
+  CK(cudaStreamSynchronize(s));
+  std::vector<clay_phase_time> agg;
+  for (auto& r : recs) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, r.a, r.z);
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.z);
+    bool found = false;
+    for (auto& a : agg)
+      if (std::strcmp(a.name, r.name) == 0) {
+        a.ms += ms;
+        a.launches++;
+        found = true;
+      }
+    if (!found) {
+      clay_phase_time t{};
+      std::snprintf(t.name, sizeof(t.name), "%s", r.name);
+      t.ms = ms;
+      t.launches = 1;
+      agg.push_back(t);
+    }
+  }
+  int n = std::min(cap, static_cast<int>(agg.size()));
+  for (int i = 0; i < n; i++) out[i] = agg[i];
+  *n_out = n;
+  return CLAY_OK;
+}
+
+int clay_batch_read_contacts_async(clay_batch* b, clay_contact_list* host, void* stream) {
+  if (!b || (!host && !b->sims.empty())) return fail(CLAY_EINVAL, "clay_batch_read_contacts_async: NULL argument");
+  if (!b->built) return fail(CLAY_ESTATE, "clay_batch_read_contacts_async: the batch has not stepped yet");
+  if (b->sims.empty()) return CLAY_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int n = static_cast<int>(b->sims.size());
+  CK(L_gather_contacts(b->d_scenes, n, b->d_contacts, s));
+  CK(cudaMemcpyAsync(host, b->d_contacts, sizeof(ContactsDev) * n, cudaMemcpyDeviceToHost, s));
+  return CLAY_OK;
+}
+
+int clay_batch_step_subset(clay_batch* b, const int32_t* scenes, int n, void* stream) {
+  return fail(CLAY_ESTATE, "clay_batch_step_subset: not available in this build");
+}
+
+}  // extern "C"

@@ -1,0 +1,1251 @@
+// clay_device.cuh - device-side data layout and kernels of the fluid hot path.
+//
+// Included by two translation units: kern_ref.cu (compiled with -fmad=false: every f32
+// expression rounds exactly as written, which is what makes the bake, the cell build and
+// the reference-mode SPH passes reproduce the f32 CPU restatement bit for bit) and
+// kern_fast.cu (multiply-adds contracted; compensated density sums) for the fast-mode
+// neighbour passes. Kernels take a table of scenes and a table of work items, so the same
+// code runs one scene per launch (the plain path) or every scene of a batch in one launch.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace clay {
+
+constexpr uint32_t kSentinel = 0xffffffffu;
+constexpr int kMaxLeaves = 8;
+constexpr int kMaxParts = 64;
+constexpr int kMaxMips = 8;
+constexpr int kSplatWarps = 8;  // warps per block of the splat pass
+
+// FluidParticle (fluid.ts:20-26): (pos, density), (vel, pressure), (nvel, pad).
+struct __align__(16) ParticleDev {
+  float4 a, b, c;
+};
+
+// FluidParams (fluid.ts:28-51), WGSL uniform layout, 80 bytes.
+struct __align__(16) ParamsDev {
+  float gravity[3];
+  float dt;
+  float emit_pos[3];
+  float emit_radius;
+  float emit_vel[3];
+  float max_speed;
+  float stiffness;
+  float viscosity;
+  float damping;
+  uint32_t count;
+  uint32_t emit_base;
+  uint32_t emit_count;
+  uint32_t emit_seed;
+  float contact_depth;
+};
+static_assert(sizeof(ParamsDev) == 80, "FluidParams layout");
+
+// ContactList (fluid.ts:55-58).
+struct __align__(16) ContactsDev {
+  uint32_t count;
+  uint32_t pad[3];
+  float4 points[32];
+};
+
+// The f32 VolumeParams uniform of an SdfVolume (volume.ts:10-23,220-230), plus the
+// gradient stencil and the plane pointers. Written by the host whenever it changes.
+struct __align__(16) VolParamsDev {
+  float origin[3];
+  float voxel;
+  float center[3];
+  float extent;
+  float half;
+  float band;
+  float grad_h;
+  int32_t res;
+  const __half* dist;  // mip 0 plane
+  const __half* mat;
+};
+
+// One leaf of a collider: volumeField(volume), optionally offsetField-moved.
+struct LeafDev {
+  const VolParamsDev* vp;
+  float offset[3];
+  int32_t has_offset;
+};
+struct __align__(16) FieldDev {
+  int32_t n;
+  int32_t pad[3];
+  LeafDev leaf[kMaxLeaves];
+};
+
+// Per-scene cell-build state. `lo`/`hi_inv` accumulate the bounding box of occupied cells
+// (both with atomicMin; hi is stored complemented); the derived box is written once per
+// substep by the count pass and read by the later passes.
+struct __align__(16) GridState {
+  uint32_t lo[3];
+  uint32_t hi_inv[3];
+  uint32_t overflow;
+  uint32_t L;  // bbox cells; local index L is the out-of-grid bucket
+  int32_t x0, y0, z0;
+  uint32_t bx, by, bz;
+  uint32_t part_sum[kMaxParts];
+};
+
+// One FluidSim as the kernels see it. Constants are the f32 literals of fluid.ts,
+// computed in binary64 on the host and rounded once.
+struct __align__(16) SceneDev {
+  ParticleDev* parts;
+  ParamsDev* prm;
+  ContactsDev* contacts;
+  GridState* gs;
+  uint32_t* key;
+  uint32_t* rank;
+  uint32_t* tmp;
+  uint32_t* sorted_id;
+  float4* spos;
+  float4* svel;
+  float2* sdp;
+  uint32_t* counts;
+  uint32_t* cell_start;
+  const FieldDev* world;
+  float h, h2, inv_h, h6, mass, mass_poly6, spiky, rest, rest_floor, radius;
+  float gorig[3], wlo[3], whi[3];
+  int32_t G;
+  uint32_t capacity, bucket, parts_scan;
+  int32_t substeps;
+  int32_t pad_[3];
+};
+
+// A ParticleCloud plus the SplatField it bakes into (splat.ts:136-276).
+struct __align__(16) SplatDev {
+  const char* pos;
+  const char* nrm;
+  const float* quat;
+  const uint32_t* order;  // optional iteration order (the fluid's cell order)
+  const uint32_t* live_count;
+  const uint32_t* live_first;
+  const uint32_t* live_range_count;
+  uint32_t* keys;
+  __half* dist_out;
+  uint32_t* key_capture;
+  const VolParamsDev* vp;
+  uint32_t pos_stride, nrm_stride, capacity, live_mode;
+  int32_t mips;
+  float radius;
+  int32_t r[kMaxMips];
+  long long off[kMaxMips];
+  float voxel[kMaxMips], bw[kMaxMips], reach[kMaxMips], inv_voxel[kMaxMips];
+  long long total;
+};
+
+// A unit of work of one launch: object index (scene or splat), sub-index (mip level or
+// scan part), first element, element count.
+struct Work {
+  uint32_t obj, sub, first, n;
+};
+
+// The brush record (brush.ts:52-78), 80 bytes.
+struct BrushDev {
+  float pos[3];
+  float scale;
+  float rot[4];
+  float size[3];
+  float radius;
+  float material;
+  float blend;
+  float bound;
+  float mask;
+  uint32_t kind, op, slot, pad;
+};
+static_assert(sizeof(BrushDev) == 80, "Brush layout");
+
+struct BuildLevelDev {
+  __half* dist;
+  __half* mat;
+  int32_t R, tiles;
+  float ox, oy, oz, voxel, tile_size, tile_half, bw, empty;
+};
+
+}  // namespace clay
+
+#ifdef CLAY_DEFINE_KERNELS
+// =======================================================================================
+// Device code. Only translation units that define CLAY_DEFINE_KERNELS compile it.
+namespace clay {
+
+__device__ __forceinline__ int f2i(float f) {
+  // Saturating conversion, NaN -> 0 (WGSL value conversion).
+  return __float2int_rz(f);
+}
+__device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz) {
+  return (ax * bx + ay * by) + az * bz;
+}
+__device__ __forceinline__ float len3(float x, float y, float z) { return sqrtf(dot3(x, y, z, x, y, z)); }
+__device__ __forceinline__ float clampf(float x, float lo, float hi) { return fminf(fmaxf(x, lo), hi); }
+
+// hash1 (math/gpu.ts:103-112).
+__device__ __forceinline__ float hash1(uint32_t x) {
+  x = x ^ (x >> 16);
+  x = x * 0x7feb352du;
+  x = x ^ (x >> 15);
+  x = x * 0x846ca68bu;
+  x = x ^ (x >> 16);
+  return static_cast<float>(x & 0xffffffu) * (1.0f / 16777216.0f);
+}
+
+__device__ __forceinline__ uint32_t work_count(const SceneDev& S) { return min(S.prm->count, S.capacity); }
+
+// ---------------------------------------------------------------------------------------
+// Collider: volumeField.sample(p, 0) / normal(p) (trace/field.ts:102-180, volume.ts:262-313)
+// with a software trilinear filter of exact f32 weights.
+struct Vol {
+  float ox, oy, oz, voxel, cx, cy, cz, extent, half, band, grad_h;
+  int res;
+  const __half* dist;
+};
+
+__device__ __forceinline__ Vol load_vol(const VolParamsDev* vp) {
+  Vol v;
+  v.ox = vp->origin[0];
+  v.oy = vp->origin[1];
+  v.oz = vp->origin[2];
+  v.voxel = vp->voxel;
+  v.cx = vp->center[0];
+  v.cy = vp->center[1];
+  v.cz = vp->center[2];
+  v.extent = vp->extent;
+  v.half = vp->half;
+  v.band = vp->band;
+  v.grad_h = vp->grad_h;
+  v.res = vp->res;
+  v.dist = vp->dist;
+  return v;
+}
+
+__device__ __forceinline__ float sd_box(float px, float py, float pz, float b) {
+  float qx = fabsf(px) - b, qy = fabsf(py) - b, qz = fabsf(pz) - b;
+  float mx = fmaxf(qx, 0.0f), my = fmaxf(qy, 0.0f), mz = fmaxf(qz, 0.0f);
+  return len3(mx, my, mz) + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.0f);
+}
+
+__device__ __forceinline__ float texel(const Vol& v, int x, int y, int z) {
+  size_t idx = static_cast<size_t>(x) + static_cast<size_t>(v.res) * (static_cast<size_t>(y) + static_cast<size_t>(v.res) * z);
+  return __half2float(__ldg(v.dist + idx));
+}
+
+__device__ __forceinline__ void tri_axis(float u, int R, int& i0, int& i1, float& fr) {
+  float t = u * static_cast<float>(R) - 0.5f;
+  float fl = floorf(t);
+  fr = t - fl;
+  int ii = f2i(fl);
+  i0 = min(max(ii, 0), R - 1);
+  int jj = ii == 2147483647 ? ii : ii + 1;
+  i1 = min(max(jj, 0), R - 1);
+}
+
+__device__ __forceinline__ float lerpf(float a, float b, float f) { return a + (b - a) * f; }
+
+__device__ __forceinline__ float trilinear(const Vol& v, float px, float py, float pz) {
+  float ux = __fdiv_rn(px - v.ox, v.extent);
+  float uy = __fdiv_rn(py - v.oy, v.extent);
+  float uz = __fdiv_rn(pz - v.oz, v.extent);
+  int x0, x1, y0, y1, z0, z1;
+  float fx, fy, fz;
+  tri_axis(ux, v.res, x0, x1, fx);
+  tri_axis(uy, v.res, y0, y1, fy);
+  tri_axis(uz, v.res, z0, z1, fz);
+  float c00 = lerpf(texel(v, x0, y0, z0), texel(v, x1, y0, z0), fx);
+  float c10 = lerpf(texel(v, x0, y1, z0), texel(v, x1, y1, z0), fx);
+  float c01 = lerpf(texel(v, x0, y0, z1), texel(v, x1, y0, z1), fx);
+  float c11 = lerpf(texel(v, x0, y1, z1), texel(v, x1, y1, z1), fx);
+  float c0 = lerpf(c00, c10, fy);
+  float c1 = lerpf(c01, c11, fy);
+  return lerpf(c0, c1, fz);
+}
+
+__device__ __forceinline__ void vol_sample(const Vol& v, float px, float py, float pz, float& sx, float& sy) {
+  float dbox = sd_box(px - v.cx, py - v.cy, pz - v.cz, v.half);
+  if (dbox > 0.0f) {
+    sx = dbox;
+    sy = 1.0f;
+    return;
+  }
+  float raw = trilinear(v, px, py, pz);
+  float bw = v.band * v.voxel * 1.0f;
+  sx = raw * bw;
+  sy = raw;
+}
+
+__device__ __forceinline__ float vol_dist(const Vol& v, float px, float py, float pz) {
+  float dbox = sd_box(px - v.cx, py - v.cy, pz - v.cz, v.half);
+  if (dbox > 0.0f) return dbox;
+  return trilinear(v, px, py, pz) * (v.band * v.voxel * 1.0f);
+}
+
+__device__ __forceinline__ void vol_normal(const Vol& v, float px, float py, float pz, float& nx, float& ny, float& nz) {
+  float h = v.grad_h;
+  float gx = vol_dist(v, px + h, py, pz) - vol_dist(v, px - h, py, pz);
+  float gy = vol_dist(v, px, py + h, pz) - vol_dist(v, px, py - h, pz);
+  float gz = vol_dist(v, px, py, pz + h) - vol_dist(v, px, py, pz - h);
+  float len = len3(gx, gy, gz);
+  if (len > 1e-8f) {
+    float inv = __frcp_rn(len);
+    nx = gx * inv;
+    ny = gy * inv;
+    nz = gz * inv;
+  } else {
+    nx = 0.0f;
+    ny = 1.0f;
+    nz = 0.0f;
+  }
+}
+
+// unionField: the pair of the nearer child, the later child on ties.
+__device__ __forceinline__ int field_pick(const FieldDev* f, float px, float py, float pz, float& sx, float& sy) {
+  int best = -1;
+  float bx = 0.0f, by = 0.0f;
+  int n = f->n;
+  for (int i = 0; i < n; i++) {
+    const LeafDev& lf = f->leaf[i];
+    Vol v = load_vol(lf.vp);
+    float qx = px, qy = py, qz = pz;
+    if (lf.has_offset) {
+      qx = px - lf.offset[0];
+      qy = py - lf.offset[1];
+      qz = pz - lf.offset[2];
+    }
+    float s0, s1;
+    vol_sample(v, qx, qy, qz, s0, s1);
+    if (best < 0 || !(bx < s0)) {
+      best = i;
+      bx = s0;
+      by = s1;
+    }
+  }
+  sx = bx;
+  sy = by;
+  return best;
+}
+
+__device__ __forceinline__ void field_normal(const FieldDev* f, int child, float px, float py, float pz, float& nx, float& ny,
+                                             float& nz) {
+  const LeafDev& lf = f->leaf[child];
+  Vol v = load_vol(lf.vp);
+  float qx = px, qy = py, qz = pz;
+  if (lf.has_offset) {
+    qx = px - lf.offset[0];
+    qy = py - lf.offset[1];
+    qz = pz - lf.offset[2];
+  }
+  vol_normal(v, qx, qy, qz, nx, ny, nz);
+}
+
+// ---------------------------------------------------------------------------------------
+// Work-item decoding: `work` == nullptr means "one object, blocks tile [0, n)".
+__device__ __forceinline__ Work get_work(const Work* work) {
+  if (work) return work[blockIdx.x];
+  Work w;
+  w.obj = 0;
+  w.sub = blockIdx.y;
+  w.first = blockIdx.x * blockDim.x;
+  w.n = blockDim.x;
+  return w;
+}
+
+// cellOf (fluid.ts:253-257).
+__device__ __forceinline__ void cell_of(const SceneDev& S, float px, float py, float pz, int& cx, int& cy, int& cz) {
+  cx = f2i(floorf((px - S.gorig[0]) * S.inv_h));
+  cy = f2i(floorf((py - S.gorig[1]) * S.inv_h));
+  cz = f2i(floorf((pz - S.gorig[2]) * S.inv_h));
+}
+
+struct BoxInfo {
+  int x0, y0, z0;
+  uint32_t bx, by, bz, L;
+};
+
+__device__ __forceinline__ BoxInfo box_from_acc(const GridState* gs) {
+  BoxInfo b;
+  uint32_t lx = gs->lo[0], ly = gs->lo[1], lz = gs->lo[2];
+  if (lx == 0xffffffffu) {  // no particle in the grid
+    b.x0 = b.y0 = b.z0 = 0;
+    b.bx = b.by = b.bz = 0;
+    b.L = 0;
+    return b;
+  }
+  uint32_t hx = ~gs->hi_inv[0], hy = ~gs->hi_inv[1], hz = ~gs->hi_inv[2];
+  b.x0 = static_cast<int>(lx);
+  b.y0 = static_cast<int>(ly);
+  b.z0 = static_cast<int>(lz);
+  b.bx = hx - lx + 1;
+  b.by = hy - ly + 1;
+  b.bz = hz - lz + 1;
+  b.L = b.bx * b.by * b.bz;
+  return b;
+}
+
+__device__ __forceinline__ BoxInfo box_from_state(const GridState* gs) {
+  BoxInfo b;
+  b.x0 = gs->x0;
+  b.y0 = gs->y0;
+  b.z0 = gs->z0;
+  b.bx = gs->bx;
+  b.by = gs->by;
+  b.bz = gs->bz;
+  b.L = gs->L;
+  return b;
+}
+
+__device__ __forceinline__ uint32_t local_of(const BoxInfo& b, uint32_t key) {
+  if (key == kSentinel) return b.L;
+  int x = static_cast<int>(key & 1023u), y = static_cast<int>((key >> 10) & 1023u), z = static_cast<int>(key >> 20);
+  return static_cast<uint32_t>(x - b.x0) + b.bx * (static_cast<uint32_t>(y - b.y0) + b.by * static_cast<uint32_t>(z - b.z0));
+}
+
+#ifndef CLAY_ONLY_NEIGHBOUR_PASSES
+// ---------------------------------------------------------------------------------------
+// emit (fluid.ts:268-291). pow(r.x, 1/3) is taken in binary64 and rounded to f32;
+// normalize(v) = v / length(v).
+__global__ void k_emit(const SceneDev* __restrict__ scenes, const Work* __restrict__ work) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  const ParamsDev& P = *S.prm;
+  for (uint32_t i = w.first + threadIdx.x; i < P.emit_count; i += (work ? w.n : gridDim.x * blockDim.x)) {
+    uint32_t slot = (P.emit_base + i) % S.capacity;
+    uint32_t seed = P.emit_seed * 9781u + i;
+    float r0 = hash1(seed * 3u + 0u), r1 = hash1(seed * 3u + 1u), r2 = hash1(seed * 3u + 2u);
+    float dx = (r0 * 2.0f - 1.0f) + 1e-4f, dy = (r1 * 2.0f - 1.0f) + 1e-4f, dz = (r2 * 2.0f - 1.0f) + 1e-4f;
+    float len = len3(dx, dy, dz);
+    float ux = __fdiv_rn(dx, len), uy = __fdiv_rn(dy, len), uz = __fdiv_rn(dz, len);
+    const float third = 0.333333343267440796f;  // f32(1/3)
+    float pw = static_cast<float>(pow(static_cast<double>(r0), static_cast<double>(third)));
+    float s = P.emit_radius * pw;
+    ParticleDev q;
+    q.a = make_float4(P.emit_pos[0] + ux * s, P.emit_pos[1] + uy * s, P.emit_pos[2] + uz * s, 0.0f);
+    q.b = make_float4(P.emit_vel[0], P.emit_vel[1], P.emit_vel[2], 0.0f);
+    q.c = make_float4(P.emit_vel[0], P.emit_vel[1], P.emit_vel[2], 0.0f);
+    S.parts[slot] = q;
+    if (!work) break;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// Cell build, pass 1: the cell of every live particle (packed x|y<<10|z<<20, or the
+// sentinel when !inGrid, fluid.ts:318-322) and the bounding box of occupied cells. The
+// first block of a scene also clears the contact counter (fluid.ts:302-304) and the
+// bucket-overflow flag.
+__global__ void k_cell_key(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  uint32_t count = work_count(S);
+  uint32_t i = w.first + threadIdx.x;
+  if (w.first == 0 && threadIdx.x == 0) {
+    S.contacts->count = 0u;
+    S.gs->overflow = 0u;
+  }
+  uint32_t lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
+  uint32_t hinv[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
+  if (i < count && threadIdx.x < w.n) {
+    float4 p = S.parts[i].a;
+    int cx, cy, cz;
+    cell_of(S, p.x, p.y, p.z, cx, cy, cz);
+    bool in = cx >= 0 && cy >= 0 && cz >= 0 && cx < S.G && cy < S.G && cz < S.G;
+    uint32_t key = kSentinel;
+    if (in) {
+      key = static_cast<uint32_t>(cx) | (static_cast<uint32_t>(cy) << 10) | (static_cast<uint32_t>(cz) << 20);
+      lo[0] = cx;
+      lo[1] = cy;
+      lo[2] = cz;
+      hinv[0] = ~static_cast<uint32_t>(cx);
+      hinv[1] = ~static_cast<uint32_t>(cy);
+      hinv[2] = ~static_cast<uint32_t>(cz);
+    }
+    S.key[i] = key;
+  }
+  // warp then block reduction of the box
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    lo[k] = __reduce_min_sync(0xffffffffu, lo[k]);
+    hinv[k] = __reduce_min_sync(0xffffffffu, hinv[k]);
+  }
+  __shared__ uint32_t s_box[6];
+  if (threadIdx.x < 6) s_box[threadIdx.x] = 0xffffffffu;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      if (lo[k] != 0xffffffffu) atomicMin(&s_box[k], lo[k]);
+      if (hinv[k] != 0xffffffffu) atomicMin(&s_box[3 + k], hinv[k]);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    if (s_box[threadIdx.x] != 0xffffffffu) atomicMin(&S.gs->lo[threadIdx.x], s_box[threadIdx.x]);
+  } else if (threadIdx.x < 6) {
+    if (s_box[threadIdx.x] != 0xffffffffu) atomicMin(&S.gs->hi_inv[threadIdx.x - 3], s_box[threadIdx.x]);
+  }
+}
+
+// Cell build, pass 2: per-cell counts with warp-aggregated atomics; every particle keeps
+// its provisional slot. The scene's first block publishes the box for the later passes.
+__global__ void k_cell_count(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  uint32_t count = work_count(S);
+  BoxInfo b = box_from_acc(S.gs);
+  if (w.first == 0 && threadIdx.x == 0) {
+    GridState* g = S.gs;
+    g->x0 = b.x0;
+    g->y0 = b.y0;
+    g->z0 = b.z0;
+    g->bx = b.bx;
+    g->by = b.by;
+    g->bz = b.bz;
+    g->L = b.L;
+  }
+  uint32_t i = w.first + threadIdx.x;
+  bool act = i < count && threadIdx.x < w.n;
+  uint32_t l = 0xffffffffu;
+  if (act) {
+    l = local_of(b, S.key[i]);
+    S.key[i] = l;
+  }
+  // warp-aggregated increment: one atomic per distinct cell per warp
+  uint32_t peers = __match_any_sync(0xffffffffu, l);
+  if (act) {
+    int leader = __ffs(peers) - 1;
+    uint32_t lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    if (static_cast<int>(lane) == leader) base = atomicAdd(&S.counts[l], static_cast<uint32_t>(__popc(peers)));
+    base = __shfl_sync(peers, base, leader);
+    uint32_t rank = base + __popc(peers & ((1u << lane) - 1u));
+    S.rank[i] = rank;
+    if (l != b.L && base + __popc(peers) > S.bucket) S.gs->overflow = 1u;
+  }
+}
+
+// Cell build, pass 3a: partial sums of the counts of [0, L] split into `parts_scan`
+// parts. Part 0 also resets the box accumulators for the next substep.
+__global__ void k_scan_partial(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  if (work_count(S) == 0) return;
+  GridState* gs = S.gs;
+  uint32_t n = gs->L + 1;
+  uint32_t P = S.parts_scan;
+  uint32_t per = (n + P - 1) / P;
+  uint32_t beg = min(w.sub * per, n), end = min(beg + per, n);
+  uint32_t s = 0;
+  for (uint32_t c = beg + threadIdx.x; c < end; c += blockDim.x) s += S.counts[c];
+  s = __reduce_add_sync(0xffffffffu, s);
+  __shared__ uint32_t red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint32_t v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0u;
+    v = __reduce_add_sync(0xffffffffu, v);
+    if (threadIdx.x == 0) gs->part_sum[w.sub] = v;
+  }
+  if (w.sub == 0 && threadIdx.x < 6) {
+    if (threadIdx.x < 3) gs->lo[threadIdx.x] = 0xffffffffu;
+    else gs->hi_inv[threadIdx.x - 3] = 0xffffffffu;
+  }
+}
+
+// Cell build, pass 3b: exclusive scan into cell_start[0 .. L+1], counts cleared behind.
+__global__ void k_scan_final(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  if (work_count(S) == 0) return;
+  const GridState* gs = S.gs;
+  uint32_t n = gs->L + 1;
+  uint32_t P = S.parts_scan;
+  uint32_t per = (n + P - 1) / P;
+  uint32_t beg = min(w.sub * per, n), end = min(beg + per, n);
+  __shared__ uint32_t s_off;
+  __shared__ uint32_t s_warp[32];
+  if (threadIdx.x == 0) {
+    uint32_t o = 0;
+    for (uint32_t q = 0; q < w.sub; q++) o += gs->part_sum[q];
+    s_off = o;
+  }
+  __syncthreads();
+  uint32_t run = s_off;
+  const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (uint32_t c0 = beg; c0 < end; c0 += blockDim.x) {
+    uint32_t c = c0 + threadIdx.x;
+    uint32_t v = c < end ? S.counts[c] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= static_cast<uint32_t>(o)) x += y;
+    }
+    if (lane == 31) s_warp[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t t = lane < nw ? s_warp[lane] : 0u;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= static_cast<uint32_t>(o)) t += y;
+      }
+      s_warp[lane] = t;
+    }
+    __syncthreads();
+    uint32_t before = (wid > 0 ? s_warp[wid - 1] : 0u) + x - v;
+    if (c < end) {
+      S.cell_start[c] = run + before;
+      S.counts[c] = 0u;
+    }
+    uint32_t tot = s_warp[nw - 1];
+    __syncthreads();
+    run += tot;
+  }
+  if (end == n && beg < end && threadIdx.x == 0) S.cell_start[n] = run;
+  if (n == 0 && threadIdx.x == 0 && w.sub == 0) S.cell_start[0] = 0;
+}
+
+// Cell build, pass 4: provisional placement.
+__global__ void k_cell_scatter(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  uint32_t count = work_count(S);
+  uint32_t i = w.first + threadIdx.x;
+  if (i >= count || threadIdx.x >= w.n) return;
+  S.tmp[S.cell_start[S.key[i]] + S.rank[i]] = i;
+}
+
+// Cell build, pass 5: deterministic order inside each cell (ascending particle index, so
+// a full cell keeps its `bucket` lowest indices, fluid.ts:323-329) and the gather of the
+// particle state into cell order.
+__global__ void k_cell_order(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  uint32_t count = work_count(S);
+  uint32_t k = w.first + threadIdx.x;
+  if (k >= count || threadIdx.x >= w.n) return;
+  uint32_t id = S.tmp[k];
+  uint32_t l = S.key[id];
+  uint32_t s = S.cell_start[l], e = S.cell_start[l + 1];
+  uint32_t r = 0;
+  for (uint32_t q = s; q < e; q++) r += (S.tmp[q] < id) ? 1u : 0u;
+  uint32_t f = s + r;
+  S.sorted_id[f] = id;
+  const ParticleDev& P = S.parts[id];
+  S.spos[f] = P.a;
+  S.svel[f] = P.b;
+}
+
+#endif  // CLAY_ONLY_NEIGHBOUR_PASSES
+
+// ---------------------------------------------------------------------------------------
+// Neighbour iteration over the 27 cells (fluid.ts:346-364) in the reference's order: dz,
+// dy, dx ascending, then ascending index inside a cell. Cells along x are adjacent in the
+// cell order, so each (dy, dz) row is one contiguous range unless some cell of the scene
+// holds more than `bucket` particles.
+template <class F>
+__device__ __forceinline__ void for_neighbours(const SceneDev& S, const BoxInfo& b, bool overflow, int cx, int cy, int cz,
+                                               F&& f) {
+  const int G = S.G;
+  cx = min(max(cx, -2), G + 1);
+  cy = min(max(cy, -2), G + 1);
+  cz = min(max(cz, -2), G + 1);
+  const int x1b = b.x0 + static_cast<int>(b.bx) - 1;
+  const int y1b = b.y0 + static_cast<int>(b.by) - 1;
+  const int z1b = b.z0 + static_cast<int>(b.bz) - 1;
+  if (b.L == 0) return;
+  int xl = max(cx - 1, b.x0), xh = min(cx + 1, x1b);
+  if (xl > xh) return;
+  for (int dz = -1; dz <= 1; dz++) {
+    int z = cz + dz;
+    if (z < b.z0 || z > z1b) continue;
+    for (int dy = -1; dy <= 1; dy++) {
+      int y = cy + dy;
+      if (y < b.y0 || y > y1b) continue;
+      uint32_t row = b.bx * (static_cast<uint32_t>(y - b.y0) + b.by * static_cast<uint32_t>(z - b.z0));
+      uint32_t l0 = row + static_cast<uint32_t>(xl - b.x0);
+      uint32_t l1 = row + static_cast<uint32_t>(xh - b.x0);
+      if (!overflow) {
+        uint32_t s = __ldg(S.cell_start + l0), e = __ldg(S.cell_start + l1 + 1);
+        for (uint32_t q = s; q < e; q++) f(q);
+      } else {
+        for (uint32_t l = l0; l <= l1; l++) {
+          uint32_t s = __ldg(S.cell_start + l), e = __ldg(S.cell_start + l + 1);
+          uint32_t n = min(e - s, S.bucket);
+          for (uint32_t q = s; q < s + n; q++) f(q);
+        }
+      }
+    }
+  }
+}
+
+// density (fluid.ts:333-368). kFast accumulates with Kahan-Neumaier compensation.
+template <bool kFast>
+__global__ void k_density(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  uint32_t count = work_count(S);
+  uint32_t k = w.first + threadIdx.x;
+  if (k >= count || threadIdx.x >= w.n) return;
+  const BoxInfo b = box_from_state(S.gs);
+  const bool overflow = S.gs->overflow != 0u;
+  const float4 me = S.spos[k];
+  int cx, cy, cz;
+  cell_of(S, me.x, me.y, me.z, cx, cy, cz);
+  const float h2 = S.h2, mp6 = S.mass_poly6;
+  float rho = 0.0f, comp = 0.0f;
+  const float4* __restrict__ spos = S.spos;
+  for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
+    float4 o = __ldg(spos + q);
+    float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+    float r2 = (dx * dx + dy * dy) + dz * dz;
+    if (r2 < h2) {
+      float wv = h2 - r2;
+      float term = mp6 * ((wv * wv) * wv);
+      if (kFast) {
+        // Neumaier: explicit round-to-nearest adds so nothing is contracted into an FMA.
+        float t = __fadd_rn(rho, term);
+        if (fabsf(rho) >= fabsf(term)) comp = __fadd_rn(comp, __fadd_rn(__fsub_rn(rho, t), term));
+        else comp = __fadd_rn(comp, __fadd_rn(__fsub_rn(term, t), rho));
+        rho = t;
+      } else {
+        rho = rho + term;
+      }
+    }
+  });
+  if (kFast) rho = __fadd_rn(rho, comp);
+  const float stiff = S.prm->stiffness;
+  S.sdp[k] = make_float2(fmaxf(rho, S.rest_floor), fmaxf(stiff * (rho - S.rest), 0.0f));
+}
+
+// forces (fluid.ts:370-439) fused with integrate (fluid.ts:449-491). The neighbour pass
+// reads only the cell-ordered copies made by the cell build, and writes only the particle
+// records, so no neighbour can observe a half-updated particle.
+template <bool kFast>
+__global__ void k_forces_integrate(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  uint32_t count = work_count(S);
+  uint32_t k = w.first + threadIdx.x;
+  if (k >= count || threadIdx.x >= w.n) return;
+  const BoxInfo b = box_from_state(S.gs);
+  const bool overflow = S.gs->overflow != 0u;
+  const ParamsDev& P = *S.prm;
+  const float4 me = S.spos[k];
+  const float4 mv = S.svel[k];
+  const float2 mdp = S.sdp[k];
+  int cx, cy, cz;
+  cell_of(S, me.x, me.y, me.z, cx, cy, cz);
+  const float h2 = S.h2, h = S.h, mass = S.mass, spiky = S.spiky;
+  const float mp = mdp.y;
+  float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+  float vsx = mv.x * S.h6, vsy = mv.y * S.h6, vsz = mv.z * S.h6;
+  float wsum = S.h6;
+  const float4* __restrict__ spos = S.spos;
+  const float4* __restrict__ svel = S.svel;
+  const float2* __restrict__ sdp = S.sdp;
+  for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
+    if (q == k) return;
+    float4 o = __ldg(spos + q);
+    float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+    float r2 = (dx * dx + dy * dy) + dz * dz;
+    if (r2 >= h2) return;
+    float2 odp = __ldg(sdp + q);
+    float inv = __frcp_rn(odp.x);
+    float w0 = h2 - r2;
+    float wv = (w0 * w0) * w0;
+    float4 ov = __ldg(svel + q);
+    vsx = vsx + ov.x * wv;
+    vsy = vsy + ov.y * wv;
+    vsz = vsz + ov.z * wv;
+    wsum = wsum + wv;
+    float r = __fsqrt_rn(r2);
+    if (r > 1e-6f) {
+      float hr = h - r;
+      float s = mass * (mp + odp.y) * 0.5f * inv * spiky * (hr * hr);
+      float ir = __frcp_rn(r);
+      fx = fx - (dx * ir) * s;
+      fy = fy - (dy * ir) * s;
+      fz = fz - (dz * ir) * s;
+    }
+  });
+  float id = __frcp_rn(mdp.x);
+  float ax = fx * id + P.gravity[0], ay = fy * id + P.gravity[1], az = fz * id + P.gravity[2];
+  float t = clampf(P.viscosity, 0.0f, 1.0f);
+  float iw = __frcp_rn(wsum);
+  float mx = vsx * iw, my = vsy * iw, mz = vsz * iw;
+  float omt = 1.0f - t;
+  float vx = mv.x * omt + mx * t, vy = mv.y * omt + my * t, vz = mv.z * omt + mz * t;
+  vx = (vx + ax * P.dt) * P.damping;
+  vy = (vy + ay * P.dt) * P.damping;
+  vz = (vz + az * P.dt) * P.damping;
+  float speed = len3(vx, vy, vz);
+  if (speed > P.max_speed) {
+    float sc = __fdiv_rn(P.max_speed, speed);
+    vx = vx * sc;
+    vy = vy * sc;
+    vz = vz * sc;
+  }
+  const float nvx = vx, nvy = vy, nvz = vz;
+  // integrate
+  float px = me.x + vx * P.dt, py = me.y + vy * P.dt, pz = me.z + vz * P.dt;
+  const FieldDev* world = S.world;
+  if (world && world->n > 0) {
+    float sx, sy;
+    int child = field_pick(world, px, py, pz, sx, sy);
+    float dw = sx;
+    if (dw < S.radius) {
+      float nx, ny, nz;
+      field_normal(world, child, px, py, pz, nx, ny, nz);
+      float push = S.radius - dw;
+      px = px + nx * push;
+      py = py + ny * push;
+      pz = pz + nz * push;
+      float vn = fminf(dot3(vx, vy, vz, nx, ny, nz), 0.0f);
+      vx = vx - nx * vn;
+      vy = vy - ny * vn;
+      vz = vz - nz * vn;
+      if (dw < P.contact_depth) {
+        uint32_t slot = atomicAdd(&S.contacts->count, 1u);
+        if (slot < 32u) S.contacts->points[slot] = make_float4(px, py, pz, len3(vx, vy, vz));
+      }
+    }
+  }
+  float clx = clampf(px, S.wlo[0], S.whi[0]), cly = clampf(py, S.wlo[1], S.whi[1]), clz = clampf(pz, S.wlo[2], S.whi[2]);
+  ParticleDev out;
+  out.a = make_float4(clx, cly, clz, mdp.x);
+  out.b = make_float4(clx == px ? vx : 0.0f, cly == py ? vy : 0.0f, clz == pz ? vz : 0.0f, mdp.y);
+  out.c = make_float4(nvx, nvy, nvz, 0.0f);
+  S.parts[S.sorted_id[k]] = out;
+}
+
+#ifndef CLAY_ONLY_NEIGHBOUR_PASSES
+// ---------------------------------------------------------------------------------------
+// SplatField bake (splat.ts:200-276).
+//
+// One warp takes 32 consecutive particles of the cloud (in cell order for the fluid) and
+// the union U of their voxel boxes (splat.ts:238-243). When U is compact it walks U with
+// one voxel per lane and takes, per voxel, the minimum of every particle's contribution
+// before a single atomicMin; otherwise it walks each particle's own box. Both give the
+// reference's result exactly: the key is a monotone function of the distance, so the
+// atomicMin of keys equals the key of the minimum distance, and a voxel outside a
+// particle's box is at least half a voxel beyond its reach, so it can never pass
+// `sd < bandWorld` (splat.ts:246). For spheres the minimum is taken over squared lengths:
+// sqrt and the subtraction of the radius are both monotone in f32.
+
+__device__ __forceinline__ uint32_t enc_key(float sd, float bw) {
+  float v = clampf(__fdiv_rn(sd, bw), -1.0f, 1.0f);
+  return static_cast<uint32_t>((v + 1.0f) * 32767.5f);
+}
+
+__device__ __forceinline__ bool cloud_live(const SplatDev& D, uint32_t idx, uint32_t& i) {
+  if (D.order) {
+    uint32_t n = min(*D.live_count, D.capacity);
+    if (idx >= n) return false;
+    i = D.order[idx];
+    return i < D.capacity;
+  }
+  if (idx >= D.capacity) return false;
+  i = idx;
+  if (D.live_mode == 1) return idx < *D.live_count;
+  if (D.live_mode == 2) {
+    uint32_t f = *D.live_first;
+    return idx >= f && idx < f + *D.live_range_count;
+  }
+  return true;
+}
+
+__global__ void __launch_bounds__(32 * kSplatWarps) k_splat(const SplatDev* __restrict__ splats, const Work* __restrict__ work) {
+  Work w = get_work(work);
+  const SplatDev& D = splats[w.obj];
+  const int m = static_cast<int>(w.sub);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __shared__ float4 s_p[kSplatWarps][32];
+  __shared__ float4 s_n[kSplatWarps][32];
+  __shared__ int4 s_lo[kSplatWarps][32];
+  __shared__ int4 s_hi[kSplatWarps][32];
+  const uint32_t idx = w.first + threadIdx.x;
+  const bool has_n = D.nrm != nullptr;
+  const float voxel = D.voxel[m], bw = D.bw[m], reach = D.reach[m], inv_voxel = D.inv_voxel[m], radius = D.radius;
+  const int R = D.r[m];
+  const int last = R - 1;
+  const long long off = D.off[m];
+  uint32_t i = 0;
+  bool live = (threadIdx.x < w.n) && cloud_live(D, idx, i);
+  float px = 0, py = 0, pz = 0, nx = 0, ny = 0, nz = 0;
+  int lx = 0, ly = 0, lz = 0, hx = -1, hy = -1, hz = -1;
+  if (live) {
+    const float* pp = reinterpret_cast<const float*>(D.pos + static_cast<size_t>(i) * D.pos_stride);
+    px = pp[0] - D.vp->origin[0];
+    py = pp[1] - D.vp->origin[1];
+    pz = pp[2] - D.vp->origin[2];
+    if (has_n) {
+      const float* nn = reinterpret_cast<const float*>(D.nrm + static_cast<size_t>(i) * D.nrm_stride);
+      nx = nn[0];
+      ny = nn[1];
+      nz = nn[2];
+      if (D.quat) {  // quatRotate (math/gpu.ts:21-25)
+        float qx = D.quat[0], qy = D.quat[1], qz = D.quat[2], qw = D.quat[3];
+        float tx = (qy * nz - qz * ny) * 2.0f, ty = (qz * nx - qx * nz) * 2.0f, tz = (qx * ny - qy * nx) * 2.0f;
+        float rx = (nx + tx * qw) + (qy * tz - qz * ty);
+        float ry = (ny + ty * qw) + (qz * tx - qx * tz);
+        float rz = (nz + tz * qw) + (qx * ty - qy * tx);
+        nx = rx;
+        ny = ry;
+        nz = rz;
+      }
+    }
+    lx = max(f2i(floorf((px - reach) * inv_voxel)), 0);
+    ly = max(f2i(floorf((py - reach) * inv_voxel)), 0);
+    lz = max(f2i(floorf((pz - reach) * inv_voxel)), 0);
+    hx = min(f2i(floorf((px + reach) * inv_voxel)), last);
+    hy = min(f2i(floorf((py + reach) * inv_voxel)), last);
+    hz = min(f2i(floorf((pz + reach) * inv_voxel)), last);
+    if (lx > hx || ly > hy || lz > hz) live = false;
+  }
+  const uint32_t active = __ballot_sync(0xffffffffu, live);
+  if (active == 0u) return;
+  s_p[wid][lane] = make_float4(px, py, pz, 0.0f);
+  s_n[wid][lane] = make_float4(nx, ny, nz, 0.0f);
+  s_lo[wid][lane] = make_int4(lx, ly, lz, 0);
+  s_hi[wid][lane] = make_int4(hx, hy, hz, 0);
+  // union box and the two cost estimates
+  int ulx = __reduce_min_sync(0xffffffffu, live ? lx : 0x7fffffff);
+  int uly = __reduce_min_sync(0xffffffffu, live ? ly : 0x7fffffff);
+  int ulz = __reduce_min_sync(0xffffffffu, live ? lz : 0x7fffffff);
+  int uhx = __reduce_max_sync(0xffffffffu, live ? hx : -1);
+  int uhy = __reduce_max_sync(0xffffffffu, live ? hy : -1);
+  int uhz = __reduce_max_sync(0xffffffffu, live ? hz : -1);
+  uint32_t own = live ? static_cast<uint32_t>((hx - lx + 1) * (hy - ly + 1) * (hz - lz + 1)) : 0u;
+  uint32_t cost_ind = __reduce_add_sync(0xffffffffu, (own + 31u) >> 5);
+  const uint32_t nux = static_cast<uint32_t>(uhx - ulx + 1), nuy = static_cast<uint32_t>(uhy - uly + 1),
+                 nuz = static_cast<uint32_t>(uhz - ulz + 1);
+  const uint64_t nu64 = static_cast<uint64_t>(nux) * nuy * nuz;
+  const uint32_t nact = __popc(active);
+  __syncwarp();
+  uint32_t* __restrict__ keys = D.keys + off;
+  if (nu64 < (1ull << 31) && ((nu64 + 31) >> 5) * nact <= 2ull * cost_ind) {
+    const uint32_t nu = static_cast<uint32_t>(nu64);
+    const uint32_t nxy = nux * nuy;
+    for (uint32_t v0 = 0; v0 < nu; v0 += 32) {
+      uint32_t v = v0 + lane;
+      uint32_t vv = v < nu ? v : nu - 1;
+      int x = ulx + static_cast<int>(vv % nux);
+      int y = uly + static_cast<int>((vv / nux) % nuy);
+      int z = ulz + static_cast<int>(vv / nxy);
+      float cxf = (static_cast<float>(x) + 0.5f) * voxel;
+      float cyf = (static_cast<float>(y) + 0.5f) * voxel;
+      float czf = (static_cast<float>(z) + 0.5f) * voxel;
+      float best = __int_as_float(0x7f800000);
+      uint32_t rem = active;
+      if (!has_n) {
+        while (rem) {
+          int j = __ffs(rem) - 1;
+          rem &= rem - 1;
+          float4 q = s_p[wid][j];
+          float dx = cxf - q.x, dy = cyf - q.y, dz = czf - q.z;
+          float d2 = (dx * dx + dy * dy) + dz * dz;
+          best = fminf(best, d2);
+        }
+        best = __fsqrt_rn(best) - radius;
+      } else {
+        while (rem) {
+          int j = __ffs(rem) - 1;
+          rem &= rem - 1;
+          float4 q = s_p[wid][j];
+          float4 nn = s_n[wid][j];
+          float dx = cxf - q.x, dy = cyf - q.y, dz = czf - q.z;
+          float sd = fmaxf(dot3(dx, dy, dz, nn.x, nn.y, nn.z), __fsqrt_rn((dx * dx + dy * dy) + dz * dz) - radius);
+          best = fminf(best, sd);
+        }
+      }
+      if (v < nu && best < bw) {
+        atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
+                  enc_key(best, bw));
+      }
+    }
+  } else {
+    uint32_t rem = active;
+    while (rem) {
+      int j = __ffs(rem) - 1;
+      rem &= rem - 1;
+      float4 q = s_p[wid][j];
+      float4 nn = s_n[wid][j];
+      int4 lo = s_lo[wid][j], hi = s_hi[wid][j];
+      uint32_t bxn = static_cast<uint32_t>(hi.x - lo.x + 1), byn = static_cast<uint32_t>(hi.y - lo.y + 1),
+               bzn = static_cast<uint32_t>(hi.z - lo.z + 1);
+      uint32_t nb = bxn * byn * bzn, nbxy = bxn * byn;
+      for (uint32_t v = lane; v < nb; v += 32) {
+        int x = lo.x + static_cast<int>(v % bxn);
+        int y = lo.y + static_cast<int>((v / bxn) % byn);
+        int z = lo.z + static_cast<int>(v / nbxy);
+        float dx = (static_cast<float>(x) + 0.5f) * voxel - q.x;
+        float dy = (static_cast<float>(y) + 0.5f) * voxel - q.y;
+        float dz = (static_cast<float>(z) + 0.5f) * voxel - q.z;
+        float l = __fsqrt_rn((dx * dx + dy * dy) + dz * dz) - radius;
+        float sd = has_n ? fmaxf(dot3(dx, dy, dz, nn.x, nn.y, nn.z), l) : l;
+        if (sd < bw)
+          atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
+                    enc_key(sd, bw));
+      }
+    }
+  }
+}
+
+// resolve[m] (splat.ts:258-276): v = f32(key) * (1/32767.5) - 1 stored as f16 (round to
+// nearest even). The key is reset to 65535 behind the read, which is the clear of the
+// next bake (splat.ts:200-210): the grid holds 65535 everywhere between bakes.
+__global__ void k_resolve(const SplatDev* __restrict__ splats, const Work* __restrict__ work) {
+  Work w = get_work(work);
+  const SplatDev& D = splats[w.obj];
+  const long long base = static_cast<long long>(w.first) * 4;
+  const long long v0 = base + static_cast<long long>(threadIdx.x) * 4;
+  const float inv = 3.0518043793392844e-05f;  // f32(1/32767.5)
+  if (v0 + 3 < D.total) {
+    uint4 k4 = *reinterpret_cast<const uint4*>(D.keys + v0);
+    if (D.key_capture) *reinterpret_cast<uint4*>(D.key_capture + v0) = k4;
+    *reinterpret_cast<uint4*>(D.keys + v0) = make_uint4(65535u, 65535u, 65535u, 65535u);
+    __half2 a = __halves2half2(__float2half_rn(static_cast<float>(k4.x) * inv - 1.0f),
+                               __float2half_rn(static_cast<float>(k4.y) * inv - 1.0f));
+    __half2 b = __halves2half2(__float2half_rn(static_cast<float>(k4.z) * inv - 1.0f),
+                               __float2half_rn(static_cast<float>(k4.w) * inv - 1.0f));
+    __half2* out = reinterpret_cast<__half2*>(D.dist_out + v0);
+    out[0] = a;
+    out[1] = b;
+  } else {
+    for (long long v = v0; v < D.total && v < v0 + 4; v++) {
+      uint32_t key = D.keys[v];
+      if (D.key_capture) D.key_capture[v] = key;
+      D.keys[v] = 65535u;
+      D.dist_out[v] = __float2half_rn(static_cast<float>(key) * inv - 1.0f);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// SdfBuilder.rebuild (builder.ts:87-142) with the brush fold of brush.ts:239-372.
+__device__ __forceinline__ float sd_box3(float px, float py, float pz, float bx, float by, float bz) {
+  float qx = fabsf(px) - bx, qy = fabsf(py) - by, qz = fabsf(pz) - bz;
+  float mx = fmaxf(qx, 0.0f), my = fmaxf(qy, 0.0f), mz = fmaxf(qz, 0.0f);
+  return len3(mx, my, mz) + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.0f);
+}
+
+__device__ float eval_local(uint32_t kind, float px, float py, float pz, float sx, float sy, float sz, float radius) {
+  switch (kind) {
+    case 0:
+      return len3(px, py, pz) - sx;
+    case 1:
+      return sd_box3(px, py, pz, sx, sy, sz);
+    case 2: {
+      float qx = fabsf(px) - (sx - radius), qy = fabsf(py) - (sy - radius), qz = fabsf(pz) - (sz - radius);
+      float mx = fmaxf(qx, 0.0f), my = fmaxf(qy, 0.0f), mz = fmaxf(qz, 0.0f);
+      return len3(mx, my, mz) + fminf(fmaxf(qx, fmaxf(qy, qz)), 0.0f) - radius;
+    }
+    case 3: {
+      float pax = px, pay = py - (-sy), paz = pz;
+      float bay = sy - (-sy);
+      float h = clampf(__fdiv_rn(dot3(pax, pay, paz, 0.0f, bay, 0.0f), dot3(0.0f, bay, 0.0f, 0.0f, bay, 0.0f)), 0.0f, 1.0f);
+      return len3(pax - 0.0f * h, pay - bay * h, paz - 0.0f * h) - radius;
+    }
+    case 4: {
+      float qx = sqrtf(px * px + pz * pz) - sx;
+      return sqrtf(qx * qx + py * py) - radius;
+    }
+    case 5: {
+      float dx = sqrtf(px * px + pz * pz) - sx;
+      float dy = fabsf(py) - sy;
+      float mx = fmaxf(dx, 0.0f), my = fmaxf(dy, 0.0f);
+      return fminf(fmaxf(dx, dy), 0.0f) + sqrtf(mx * mx + my * my);
+    }
+    case 6:
+      return py - radius;
+    case 7: {
+      float ax = fabsf(px) - sx, ay = fabsf(py) - sy, az = fabsf(pz) - sz;
+      float qx = fabsf(ax + radius) - radius, qy = fabsf(ay + radius) - radius, qz = fabsf(az + radius) - radius;
+      auto term = [](float a, float b, float c) {
+        return len3(fmaxf(a, 0.0f), fmaxf(b, 0.0f), fmaxf(c, 0.0f)) + fminf(fmaxf(a, fmaxf(b, c)), 0.0f);
+      };
+      return fminf(fminf(term(ax, qy, qz), term(qx, ay, qz)), term(qx, qy, az));
+    }
+    case 9: {
+      float qx = sqrtf(px * px + pz * pz), qy = py;
+      float k1x = sz, k1y = sy, k2x = sz - sx, k2y = 2.0f * sy;
+      float cax = qx - fminf(qx, qy < 0.0f ? sx : sz);
+      float cay = fabsf(qy) - sy;
+      float num = (k1x - qx) * k2x + (k1y - qy) * k2y;
+      float den = fmaxf(k2x * k2x + k2y * k2y, 1e-20f);
+      float t = clampf(__fdiv_rn(num, den), 0.0f, 1.0f);
+      float cbx = qx - k1x + k2x * t, cby = qy - k1y + k2y * t;
+      float sg = (cbx < 0.0f && cay < 0.0f) ? -1.0f : 1.0f;
+      return sg * sqrtf(fminf(cax * cax + cay * cay, cbx * cbx + cby * cby));
+    }
+    case 10: {
+      float ax = fabsf(px), ay = fabsf(py), az = fabsf(pz);
+      float m = ax + ay + az - sx;
+      float qx, qy, qz;
+      if (3.0f * ax < m) {
+        qx = ax; qy = ay; qz = az;
+      } else if (3.0f * ay < m) {
+        qx = ay; qy = az; qz = ax;
+      } else if (3.0f * az < m) {
+        qx = az; qy = ax; qz = ay;
+      } else {
+        return m * 0.57735026918962584f;
+      }
+      float k = clampf(0.5f * (qz - qy + sx), 0.0f, sx);
+      return len3(qx, qy - sx + k, qz - k);
+    }
+    case 11: {
+      float m = fmaxf(fmaxf(-px - py - pz, -px + py + pz), fmaxf(px - py + pz, px + py - pz)) * 0.57735026918962584f;
+      return m - __fdiv_rn(sx, 3.0f);
+    }
+    case 12: {
+      const float phi = 1.6180339887498949f;
+      float qx = fabsf(px), qy = fabsf(py), qz = fabsf(pz);
+      float m = fmaxf(fmaxf(phi * qy + qz, qx + phi * qz), phi * qx + qy) * 0.52573111211913359f;
+      return m - sx * 0.79465447229176612f;
+    }
+    case 13: {
+      const float phi = 1.6180339887498949f, iphi = 0.61803398874989485f;
+      float qx = fabsf(px), qy = fabsf(py), qz = fabsf(pz);
+      float m = fmaxf(fmaxf(qx + qy + qz, qy * phi + qz * iphi), fmaxf(qx * iphi + qz * phi, qx * phi + qy * iphi)) *
+                0.57735026918962584f;
+      return m - sx * 0.79465447229176612f;
+    }
+    default:
+      return 1e9f;
+  }
+}
+
+__device__ __forceinline__ float smoothstepf(float e0, float e1, float x) {
+  float t = clampf(__fdiv_rn(x - e0, e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+
+__device__ __forceinline__ void apply_brush(float& ax, float& ay, const BrushDev& b, float px, float py, float pz) {
+  float inv_scale = __frcp_rn(fmaxf(b.scale, 1e-5f));
+  float qx = -b.rot[0], qy = -b.rot[1], qz = -b.rot[2], qw = b.rot[3];
+  float vx = px - b.pos[0], vy = py - b.pos[1], vz = pz - b.pos[2];
+  float tx = (qy * vz - qz * vy) * 2.0f, ty = (qz * vx - qx * vz) * 2.0f, tz = (qx * vy - qy * vx) * 2.0f;
+  float lx = ((vx + tx * qw) + (qy * tz - qz * ty)) * inv_scale;
+  float ly = ((vy + ty * qw) + (qz * tx - qx * tz)) * inv_scale;
+  float lz = ((vz + tz * qw) + (qx * ty - qy * tx)) * inv_scale;
+  float dist = eval_local(b.kind, lx, ly, lz, b.size[0], b.size[1], b.size[2], b.radius) * b.scale;
+  float keep = b.mask >= 0.0f ? 1.0f - smoothstepf(0.25f, 0.75f, fabsf(ay - b.mask)) : 1.0f;
+  if (b.op == 0u) {
+    float kk = fmaxf(b.blend, 1e-6f);
+    float h = clampf(0.5f + __fdiv_rn(0.5f * (ax - dist), kk), 0.0f, 1.0f);
+    float rx = (ax * (1.0f - h) + dist * h) - kk * h * (1.0f - h);
+    float ny = ay * (1.0f - h) + b.material * h;
+    float nax = ax * (1.0f - keep) + rx * keep;
+    float nay = ay * (1.0f - keep) + ny * keep;
+    ax = nax;
+    ay = nay;
+  } else if (b.op == 1u) {
+    float a = -dist;
+    float kk = fmaxf(b.blend, 1e-6f);
+    float h = clampf(0.5f - __fdiv_rn(0.5f * (ax - a), kk), 0.0f, 1.0f);
+    float rx = (ax * (1.0f - h) + a * h) + kk * h * (1.0f - h);
+    float hh = h * 0.85f;
+    float ny = ay * (1.0f - hh) + b.material * hh;
+    float nax = ax * (1.0f - keep) + rx * keep;
+    float nay = ay * (1.0f - keep) + ny * keep;
+    ax = nax;
+    ay = nay;
+  } else {
+    float wv = 1.0f - smoothstepf(-fmaxf(b.blend, 1e-4f), 0.0f, dist);
+    float t = wv * keep;
+    ay = ay * (1.0f - t) + b.material * t;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_build(const BuildLevelDev L, const BrushDev* __restrict__ brushes, int nbrush) {
+  __shared__ int s_ids[64];
+  __shared__ int s_n;
+  const int wx = blockIdx.x, wy = blockIdx.y, wz = blockIdx.z;
+  const float tminx = L.ox + static_cast<float>(wx) * L.tile_size;
+  const float tminy = L.oy + static_cast<float>(wy) * L.tile_size;
+  const float tminz = L.oz + static_cast<float>(wz) * L.tile_size;
+  if (threadIdx.x == 0) {
+    float tcx = tminx + L.tile_half, tcy = tminy + L.tile_half, tcz = tminz + L.tile_half;
+    int n = 0;
+    for (int b = 0; b < nbrush; b++) {
+      const BrushDev& B = brushes[b];
+      float nx = fmaxf(fabsf(B.pos[0] - tcx) - L.tile_half, 0.0f);
+      float ny = fmaxf(fabsf(B.pos[1] - tcy) - L.tile_half, 0.0f);
+      float nz = fmaxf(fabsf(B.pos[2] - tcz) - L.tile_half, 0.0f);
+      if (len3(nx, ny, nz) < B.bound + L.bw && n < 64) s_ids[n++] = b;
+    }
+    s_n = n;
+  }
+  __syncthreads();
+  const int n = s_n;
+  const int lx = threadIdx.x & 7, ly = (threadIdx.x >> 3) & 7, lz2 = threadIdx.x >> 6;
+  for (int half = 0; half < 2; half++) {
+    int lz = lz2 * 2 + half;
+    float px = tminx + (static_cast<float>(lx) + 0.5f) * L.voxel;
+    float py = tminy + (static_cast<float>(ly) + 0.5f) * L.voxel;
+    float pz = tminz + (static_cast<float>(lz) + 0.5f) * L.voxel;
+    float ax = L.empty, ay = 0.0f;
+    for (int q = 0; q < n; q++) apply_brush(ax, ay, brushes[s_ids[q]], px, py, pz);
+    int x = wx * 8 + lx, y = wy * 8 + ly, z = wz * 8 + lz;
+    size_t idx = static_cast<size_t>(x) + static_cast<size_t>(L.R) * (static_cast<size_t>(y) + static_cast<size_t>(L.R) * z);
+    L.dist[idx] = __float2half_rn(clampf(__fdiv_rn(ax, L.bw), -1.0f, 1.0f));
+    L.mat[idx] = __float2half_rn(ay);
+  }
+}
+
+// Test hook: the reference's cellIndex (fluid.ts:258-262) of every live particle, or
+// 0xffffffff when the particle is outside the grid (fluid.ts:319-321).
+__global__ void k_cell_index(const SceneDev* __restrict__ scenes, uint32_t* __restrict__ out) {
+  const SceneDev& S = scenes[0];
+  uint32_t count = work_count(S);
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  float4 p = S.parts[i].a;
+  int cx, cy, cz;
+  cell_of(S, p.x, p.y, p.z, cx, cy, cz);
+  bool in = cx >= 0 && cy >= 0 && cz >= 0 && cx < S.G && cy < S.G && cz < S.G;
+  uint32_t g = static_cast<uint32_t>(S.G);
+  out[i] = in ? static_cast<uint32_t>(cx) + g * (static_cast<uint32_t>(cy) + g * static_cast<uint32_t>(cz)) : kSentinel;
+}
+
+// Gathers the ContactList of every scene of a batch into one array (one readback).
+__global__ void k_gather_contacts(const SceneDev* __restrict__ scenes, int n, ContactsDev* __restrict__ out) {
+  int s = blockIdx.x;
+  if (s >= n) return;
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(scenes[s].contacts);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(out + s);
+  for (int i = threadIdx.x; i < static_cast<int>(sizeof(ContactsDev) / 4); i += blockDim.x) dst[i] = src[i];
+}
+
+// Collider query (test hook): sample(p, 0) and normal(p) at n points.
+__global__ void k_field_query(const FieldDev* __restrict__ f, const float* __restrict__ pts, int n, float* __restrict__ sxy,
+                              float* __restrict__ nrm) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float px = pts[3 * i], py = pts[3 * i + 1], pz = pts[3 * i + 2];
+  float sx = 0.0f, sy = 0.0f, nx = 0.0f, ny = 1.0f, nz = 0.0f;
+  if (f->n > 0) {
+    int c = field_pick(f, px, py, pz, sx, sy);
+    field_normal(f, c, px, py, pz, nx, ny, nz);
+  }
+  sxy[2 * i] = sx;
+  sxy[2 * i + 1] = sy;
+  nrm[3 * i] = nx;
+  nrm[3 * i + 1] = ny;
+  nrm[3 * i + 2] = nz;
+}
+
+#endif  // CLAY_ONLY_NEIGHBOUR_PASSES
+
+}  // namespace clay
+#endif  // CLAY_DEFINE_KERNELS

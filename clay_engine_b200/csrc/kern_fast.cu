@@ -1,0 +1,20 @@
+// kern_fast.cu - fast-mode neighbour passes: multiply-adds may be contracted into FMA and
+// the density sum is compensated. Compiled with -fmad=true.
+#define CLAY_DEFINE_KERNELS
+#define CLAY_ONLY_NEIGHBOUR_PASSES
+#include "launch.h"
+
+namespace clay {
+
+cudaError_t L_density_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  k_density<true><<<blocks, threads, 0, st>>>(s, w, sub);
+  count_launch();
+  return cudaPeekAtLastError();
+}
+cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  k_forces_integrate<true><<<blocks, threads, 0, st>>>(s, w, sub);
+  count_launch();
+  return cudaPeekAtLastError();
+}
+
+}  // namespace clay

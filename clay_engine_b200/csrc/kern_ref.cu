@@ -1,0 +1,74 @@
+// kern_ref.cu - kernels whose f32 arithmetic must round exactly as written: emission, the
+// cell build, the bake, the collider build and the reference-mode neighbour passes.
+// Compiled with -fmad=false (no multiply-add contraction); division and square root are
+// IEEE round-to-nearest (-prec-div=true -prec-sqrt=true, the nvcc defaults).
+#define CLAY_DEFINE_KERNELS
+#include <atomic>
+
+#include "launch.h"
+
+namespace clay {
+
+static std::atomic<uint64_t> g_launches{0};
+uint64_t launch_count() { return g_launches.load(); }
+void count_launch() { g_launches.fetch_add(1); }
+void count_launches(uint64_t n) { g_launches.fetch_add(n); }
+
+#define CLAY_LAUNCH(kern, grid, block, st, ...)         \
+  do {                                                  \
+    kern<<<grid, block, 0, st>>>(__VA_ARGS__);          \
+    count_launch();                                     \
+    return cudaPeekAtLastError();                       \
+  } while (0)
+
+cudaError_t L_emit(const SceneDev* s, const Work* w, int blocks, int threads, cudaStream_t st) {
+  CLAY_LAUNCH(k_emit, blocks, threads, st, s, w);
+}
+cudaError_t L_cell_key(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  CLAY_LAUNCH(k_cell_key, blocks, threads, st, s, w, sub);
+}
+cudaError_t L_cell_count(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  CLAY_LAUNCH(k_cell_count, blocks, threads, st, s, w, sub);
+}
+cudaError_t L_scan_partial(const SceneDev* s, const Work* w, int blocks, int sub, cudaStream_t st) {
+  dim3 g(w ? blocks : 1, w ? 1 : blocks);
+  CLAY_LAUNCH(k_scan_partial, g, kScanThreads, st, s, w, sub);
+}
+cudaError_t L_scan_final(const SceneDev* s, const Work* w, int blocks, int sub, cudaStream_t st) {
+  dim3 g(w ? blocks : 1, w ? 1 : blocks);
+  CLAY_LAUNCH(k_scan_final, g, kScanThreads, st, s, w, sub);
+}
+cudaError_t L_cell_scatter(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  CLAY_LAUNCH(k_cell_scatter, blocks, threads, st, s, w, sub);
+}
+cudaError_t L_cell_order(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  CLAY_LAUNCH(k_cell_order, blocks, threads, st, s, w, sub);
+}
+cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  CLAY_LAUNCH(k_density<false>, blocks, threads, st, s, w, sub);
+}
+cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  CLAY_LAUNCH(k_forces_integrate<false>, blocks, threads, st, s, w, sub);
+}
+cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, cudaStream_t st) {
+  dim3 g(blocks, w ? 1 : blocks_y);
+  CLAY_LAUNCH(k_splat, g, kSplatThreads, st, d, w);
+}
+cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t st) {
+  CLAY_LAUNCH(k_resolve, blocks, kResolveThreads, st, d, w);
+}
+cudaError_t L_build(const BuildLevelDev& lv, const BrushDev* brushes, int n, cudaStream_t st) {
+  dim3 g(lv.tiles, lv.tiles, lv.tiles);
+  CLAY_LAUNCH(k_build, g, 256, st, lv, brushes, n);
+}
+cudaError_t L_cell_index(const SceneDev* s, uint32_t* out, int n, cudaStream_t st) {
+  CLAY_LAUNCH(k_cell_index, (n + 255) / 256, 256, st, s, out);
+}
+cudaError_t L_gather_contacts(const SceneDev* s, int n, ContactsDev* out, cudaStream_t st) {
+  CLAY_LAUNCH(k_gather_contacts, n, 128, st, s, n, out);
+}
+cudaError_t L_field_query(const FieldDev* f, const float* pts, int n, float* sxy, float* nrm, cudaStream_t st) {
+  CLAY_LAUNCH(k_field_query, (n + 127) / 128, 128, st, f, pts, n, sxy, nrm);
+}
+
+}  // namespace clay

@@ -1,0 +1,45 @@
+// launch.h - host-side launchers of the kernels in clay_device.cuh.
+//
+// Every launcher takes either a work table (batched: one launch covers every scene) or
+// nullptr plus a block count (one object, blocks tiling [0, n)). Each call counts one
+// kernel launch in a process-wide counter.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "clay_device.cuh"
+
+namespace clay {
+
+uint64_t launch_count();
+void count_launch();
+void count_launches(uint64_t n);  // kernels replayed by a graph launch
+
+// Threads per block of the particle passes when no tuning overrides it.
+constexpr int kBlock = 256;
+
+cudaError_t L_emit(const SceneDev* s, const Work* w, int blocks, int threads, cudaStream_t st);
+cudaError_t L_cell_key(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+cudaError_t L_cell_count(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+cudaError_t L_scan_partial(const SceneDev* s, const Work* w, int blocks, int sub, cudaStream_t st);
+cudaError_t L_scan_final(const SceneDev* s, const Work* w, int blocks, int sub, cudaStream_t st);
+cudaError_t L_cell_scatter(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+cudaError_t L_cell_order(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+// Reference mode (kern_ref.cu) and fast mode (kern_fast.cu) of the neighbour passes.
+cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+cudaError_t L_density_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+// `blocks_y` = mip levels when w == nullptr.
+cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, cudaStream_t st);
+cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t st);
+cudaError_t L_build(const BuildLevelDev& lv, const BrushDev* brushes, int n, cudaStream_t st);
+cudaError_t L_cell_index(const SceneDev* s, uint32_t* out, int n, cudaStream_t st);
+cudaError_t L_gather_contacts(const SceneDev* s, int n, ContactsDev* out, cudaStream_t st);
+cudaError_t L_field_query(const FieldDev* f, const float* pts, int n, float* sxy, float* nrm, cudaStream_t st);
+
+constexpr int kScanThreads = 1024;
+constexpr int kSplatThreads = 32 * kSplatWarps;
+constexpr int kResolveThreads = 256;
+
+}  // namespace clay

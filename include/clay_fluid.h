@@ -1,0 +1,428 @@
+/*
+ * clay_fluid.h - C ABI of the B200-native fluid hot path of clay-engine.
+ *
+ * The path is one frame of `FluidSim.step` (lib/src/sim/fluid.ts:536-558): emission,
+ * `substeps` x (grid build, density/pressure, XSPH + pressure forces, integrate with
+ * collision against a `TracedField`), followed by `SplatField.bake`
+ * (lib/src/sim/splat.ts:296-304). Every entry point below replaces one member of the
+ * reference's `FluidSim` / `SplatField` / `SdfVolume` / `ParticleCloud` surface; the
+ * comment on each names the reference interface (file:line) it stands in for.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a negative CLAY_E* code; the message of the
+ *    last failure on the calling thread is `clay_last_error()`. Where the reference throws
+ *    an `Error`, the same condition returns CLAY_EINVAL with the reference's message text.
+ *  - Real-valued options are `double`: the reference's options are JavaScript numbers
+ *    (binary64) and its host-side derivations (voxel size, rest density, wall box) are done
+ *    in binary64 before they are rounded once to f32 for the device.
+ *  - Work is enqueued on the caller's CUDA stream (`void* stream` is a `cudaStream_t`,
+ *    NULL = the legacy default stream) and never blocks, which is what "records into a
+ *    caller-owned compute pass" means in the reference. Readbacks are asynchronous copies
+ *    into caller memory; synchronise the stream before reading them.
+ *  - The library owns all device memory it allocates; `*_destroy` frees it. The caller owns
+ *    streams and host buffers.
+ */
+#ifndef CLAY_FLUID_H
+#define CLAY_FLUID_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLAY_OK 0
+#define CLAY_EINVAL (-1)   /* bad argument / option (reference: constructor throws) */
+#define CLAY_ECUDA (-2)    /* a CUDA runtime call failed */
+#define CLAY_ENOMEM (-3)   /* device allocation failed or the HBM budget is exceeded */
+#define CLAY_ESTATE (-4)   /* call not valid in the object's current state */
+#define CLAY_ETIMEOUT (-5) /* a bounded device-side wait gave up */
+
+/* Thread-local message of the last failing call on this thread ("" if none). */
+const char* clay_last_error(void);
+/* Library version string. */
+const char* clay_version(void);
+
+/* ------------------------------------------------------------------------------------
+ * Context: binds a CUDA device. Replaces the `TgpuRoot` every reference constructor takes
+ * (fluid.ts:140, splat.ts:147, volume.ts:139).
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_ctx clay_ctx;
+int clay_ctx_create(int device, clay_ctx** out);
+void clay_ctx_destroy(clay_ctx* ctx);
+/* Bytes of device memory currently allocated by objects of this context. */
+int clay_ctx_bytes_in_use(const clay_ctx* ctx, uint64_t* out);
+
+/* ------------------------------------------------------------------------------------
+ * SdfVolume (lib/src/field/volume.ts:36-62 options, :139-314 class).
+ *
+ * Device layout: per mip level m (resolution R_m = resolution >> m) one f16 plane of
+ * band-normalised distance (`.r` of the reference's rgba16float texel) and one f16 plane of
+ * material (`.g`), each x-fastest then y then z, levels concatenated. The constant `.b`/`.a`
+ * channels (0, 1) are not stored.
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_volume clay_volume;
+
+enum {
+  CLAY_VOL_RESOLUTION = 1u << 0,
+  CLAY_VOL_WORLD_SIZE = 1u << 1,
+  CLAY_VOL_ORIGIN = 1u << 2,
+  CLAY_VOL_MIP_LEVELS = 1u << 3,
+  CLAY_VOL_BAND = 1u << 4,
+  CLAY_VOL_GRADIENT_VOXELS = 1u << 5,
+};
+
+/* `SdfVolumeOptions` (volume.ts:36-62). A field whose bit is clear in `set` takes the
+ * reference default (`??` at volume.ts:140-154,299). */
+typedef struct clay_volume_opts {
+  uint32_t set;
+  int32_t resolution;      /* ?? 128 */
+  double world_size;       /* ?? 16 */
+  double origin[3];        /* ?? [0,0,0] */
+  int32_t mip_levels;      /* ?? derived from resolution (volume.ts:148-151) */
+  double band;             /* ?? 4 */
+  double gradient_voxels;  /* ?? 1 */
+} clay_volume_opts;
+
+/* Read-only description of a volume (the reference's public fields). */
+typedef struct clay_volume_info {
+  int32_t resolution;
+  int32_t mip_levels;
+  double world_size;
+  double voxel_size;       /* mip 0 */
+  double band;
+  double origin[3];
+  int32_t tile_res_per_mip[16];
+  int64_t level_offset[16]; /* voxel offset of each level inside the concatenated planes */
+  int64_t total_voxels;
+  int32_t total_cells;      /* tile records, volume.ts:172-179 */
+} clay_volume_info;
+
+/* new SdfVolume(root, options) (volume.ts:139). Errors with the reference's message when
+ * the resolution cannot carry the mip chain (volume.ts:156-160). */
+int clay_volume_create(clay_ctx* ctx, const clay_volume_opts* opts, clay_volume** out);
+void clay_volume_destroy(clay_volume* vol);
+int clay_volume_get_info(const clay_volume* vol, clay_volume_info* out);
+/* SdfVolume.setOrigin (volume.ts:327-334). */
+int clay_volume_set_origin(clay_volume* vol, double x, double y, double z);
+/* voxelSizeAt (volume.ts:336-338). */
+double clay_volume_voxel_size_at(const clay_volume* vol, int mip);
+/* Device views of the f16 distance and material planes (all levels). */
+int clay_volume_device_planes(clay_volume* vol, void** dist_f16, void** material_f16);
+/* Host <-> device copies of whole planes (all levels, `total_voxels` halves each). Either
+ * pointer may be NULL to skip that plane. Asynchronous on `stream`. */
+int clay_volume_upload(clay_volume* vol, const uint16_t* dist_f16, const uint16_t* material_f16,
+                       void* stream);
+int clay_volume_download(const clay_volume* vol, uint16_t* dist_f16, uint16_t* material_f16,
+                         void* stream);
+/* The reference's texel layout: one level as interleaved rgba16float (r=dist, g=material,
+ * b=0, a=1), 4 halves per voxel, written into host memory. */
+int clay_volume_download_rgba16f(const clay_volume* vol, int mip, uint16_t* rgba, void* stream);
+
+/* One brush record, laid out exactly as the reference's `Brush` struct (brush.ts:52-78,
+ * 80 bytes). Produced on the host by the reference's `BrushSet.make` rule. */
+typedef struct clay_brush {
+  float pos[3];
+  float scale;
+  float rot[4];   /* xyzw */
+  float size[3];
+  float radius;
+  float material;
+  float blend;
+  float bound;
+  float mask;
+  uint32_t kind;
+  uint32_t op;
+  uint32_t slot;
+  uint32_t pad;
+} clay_brush;
+
+/* SdfBuilder.setBrushes + rebuild (lib/src/field/builder.ts:147-172): folds the brush list,
+ * in order, into every mip level of the volume on the device. Brushes beyond 256 are
+ * dropped as in builder.ts:148-153. */
+int clay_volume_build_brushes(clay_volume* vol, const clay_brush* brushes, int count, void* stream);
+
+/* ------------------------------------------------------------------------------------
+ * TracedField as a collider (lib/src/trace/field.ts:20-73). Only what the fluid reads:
+ * `sample(p, 0).x` and `normal(p)`.
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_field clay_field;
+/* volumeField(volume) (trace/field.ts:102-180). */
+int clay_field_from_volume(clay_volume* vol, clay_field** out);
+/* unionField(a, b) (trace/field.ts:246-315). At most 8 volume leaves in total. */
+int clay_field_union(const clay_field* a, const clay_field* b, clay_field** out);
+/* offsetField(field, offset) (trace/field.ts:396-429) with a host-set translation. */
+int clay_field_offset(const clay_field* f, double dx, double dy, double dz, clay_field** out);
+int clay_field_set_offset(clay_field* f, double dx, double dy, double dz);
+void clay_field_destroy(clay_field* f);
+/* Evaluates the collider at `n` points on the device (test/debug hook): writes
+ * `sample(p,0)` as (x,y) pairs into `sample_xy` and `normal(p)` as xyz triples into `nrm`.
+ * All pointers are host memory; the call synchronises `stream`. */
+int clay_field_query(const clay_field* f, const float* points_xyz, int n, float* sample_xy,
+                     float* nrm, void* stream);
+
+/* ------------------------------------------------------------------------------------
+ * ParticleCloud (lib/src/sim/splat.ts:15-38) and bodyCloud (splat.ts:47-72).
+ * ---------------------------------------------------------------------------------- */
+enum {
+  CLAY_LIVE_ALL = 0,    /* liveAt(i) = true */
+  CLAY_LIVE_COUNT = 1,  /* liveAt(i) = i < *live_count                 (fluid.ts:221-224) */
+  CLAY_LIVE_RANGE = 2,  /* liveAt(i) = first <= i < first + count       (splat.ts:56-60) */
+};
+
+typedef struct clay_cloud_desc {
+  uint32_t capacity;            /* the dispatch bound */
+  const void* positions;        /* device: float[3] at the start of each record */
+  uint32_t position_stride;     /* bytes between records */
+  uint32_t live_mode;           /* CLAY_LIVE_* */
+  const uint32_t* live_count;   /* device u32, CLAY_LIVE_COUNT */
+  const uint32_t* live_first;   /* device u32, CLAY_LIVE_RANGE */
+  const uint32_t* live_range_count; /* device u32, CLAY_LIVE_RANGE */
+  const void* normals;          /* device float[3] per record, or NULL: no normalAt */
+  uint32_t normal_stride;       /* bytes */
+  const float* rotation;        /* device xyzw quaternion applied to normals, or NULL */
+} clay_cloud_desc;
+
+/* ------------------------------------------------------------------------------------
+ * SplatField (lib/src/sim/splat.ts:74-106 options, :136-309 class).
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_splat clay_splat;
+
+enum {
+  CLAY_SPLAT_MATERIAL = 1u << 0,
+  CLAY_SPLAT_RESOLUTION = 1u << 1,
+  CLAY_SPLAT_MIP_LEVELS = 1u << 2,
+  CLAY_SPLAT_BAND = 1u << 3,
+  CLAY_SPLAT_ORIGIN = 1u << 4,
+  CLAY_SPLAT_WORLD_SIZE = 1u << 5,
+};
+
+typedef struct clay_splat_opts {
+  uint32_t set;
+  double radius;          /* required */
+  double material;        /* ?? 0 */
+  int32_t resolution;     /* ?? 64 */
+  int32_t mip_levels;     /* ?? max(1, log2(res / 8) | 0) (splat.ts:149) */
+  double band;            /* ?? 2 */
+  double origin[3];       /* ?? [-12,-4,-12] */
+  double world_size;      /* ?? 24 */
+} clay_splat_opts;
+
+/* new SplatField(root, cloud, options) (splat.ts:147). */
+int clay_splat_create(clay_ctx* ctx, const clay_cloud_desc* cloud, const clay_splat_opts* opts,
+                      clay_splat** out);
+void clay_splat_destroy(clay_splat* s);
+/* SplatField.setCenter (splat.ts:284-287). */
+int clay_splat_set_center(clay_splat* s, double x, double y, double z);
+/* SplatField.bake (splat.ts:296-304). */
+int clay_splat_bake(clay_splat* s, void* stream);
+/* SplatField.volume / .field. The returned objects are owned by the splat. */
+clay_volume* clay_splat_volume(clay_splat* s);
+clay_field* clay_splat_field(clay_splat* s);
+/* Test hook: during the next bakes, copy each voxel's 16-bit key (the u32 the reference
+ * `atomicMin`s, splat.ts:247-249) into `keys_device` (total_voxels u32) before resolving.
+ * NULL turns it off. */
+int clay_splat_capture_keys(clay_splat* s, uint32_t* keys_device);
+
+/* ------------------------------------------------------------------------------------
+ * FluidSim (lib/src/sim/fluid.ts:60-91 options, :111-582 class).
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_fluid clay_fluid;
+
+enum {
+  CLAY_FLUID_CAPACITY = 1u << 0,
+  CLAY_FLUID_SPACING = 1u << 1,
+  CLAY_FLUID_SMOOTHING = 1u << 2,
+  CLAY_FLUID_BUCKET = 1u << 3,
+  CLAY_FLUID_RADIUS = 1u << 4,
+  CLAY_FLUID_SURFACE_RADIUS = 1u << 5,
+  CLAY_FLUID_MATERIAL = 1u << 6,
+  CLAY_FLUID_BAKE_RESOLUTION = 1u << 7,
+  CLAY_FLUID_BAKE_MIP_LEVELS = 1u << 8,
+  CLAY_FLUID_BAKE_BAND = 1u << 9,
+  CLAY_FLUID_ORIGIN = 1u << 10,
+  CLAY_FLUID_WORLD_SIZE = 1u << 11,
+  CLAY_FLUID_SUBSTEPS = 1u << 12,
+  CLAY_FLUID_GRAVITY = 1u << 13,
+  CLAY_FLUID_STIFFNESS = 1u << 14,
+  CLAY_FLUID_VISCOSITY = 1u << 15,
+  CLAY_FLUID_DAMPING = 1u << 16,
+  CLAY_FLUID_MAX_SPEED = 1u << 17,
+};
+
+/* `FluidSimOptions` (fluid.ts:60-91); unset fields take the `??` defaults of
+ * fluid.ts:141-160,184-203. */
+typedef struct clay_fluid_opts {
+  uint32_t set;
+  int64_t capacity;        /* ?? 8192 */
+  double spacing;          /* ?? 0.45 */
+  double smoothing;        /* ?? spacing * 2.2 */
+  int32_t bucket;          /* ?? 64 */
+  double radius;           /* ?? spacing * 0.5 */
+  double surface_radius;   /* ?? spacing * 1.1 */
+  double material;         /* ?? 0 */
+  int32_t bake_resolution; /* ?? 64 */
+  int32_t bake_mip_levels; /* ?? max(1, log2(bakeRes / 8) | 0) */
+  double bake_band;        /* ?? 2 */
+  double origin[3];        /* ?? [-12,-4,-12] */
+  double world_size;       /* ?? 24 */
+  int32_t substeps;        /* ?? 3 */
+  double gravity[3];       /* ?? [0,-9.81,0] */
+  double stiffness;        /* ?? 220 */
+  double viscosity;        /* ?? 0.4 */
+  double damping;          /* ?? 0.995 */
+  double max_speed;        /* ?? 15 */
+} clay_fluid_opts;
+
+/* `FluidParams` (fluid.ts:28-51): the 80-byte per-frame uniform, WGSL layout. */
+typedef struct clay_fluid_params {
+  float gravity[3];
+  float dt;
+  float emit_pos[3];
+  float emit_radius;
+  float emit_vel[3];
+  float max_speed;
+  float stiffness;
+  float viscosity;
+  float damping;
+  uint32_t count;
+  uint32_t emit_base;
+  uint32_t emit_count;
+  uint32_t emit_seed;
+  float contact_depth;
+} clay_fluid_params;
+
+/* Fields `configure` may patch (fluid.ts:528: everything except the emission cursor). */
+enum {
+  CLAY_P_GRAVITY = 1u << 0,
+  CLAY_P_DT = 1u << 1,
+  CLAY_P_EMIT_POS = 1u << 2,
+  CLAY_P_EMIT_RADIUS = 1u << 3,
+  CLAY_P_EMIT_VEL = 1u << 4,
+  CLAY_P_MAX_SPEED = 1u << 5,
+  CLAY_P_STIFFNESS = 1u << 6,
+  CLAY_P_VISCOSITY = 1u << 7,
+  CLAY_P_DAMPING = 1u << 8,
+  CLAY_P_CONTACT_DEPTH = 1u << 9,
+};
+
+/* One `FluidParticle` record (fluid.ts:20-26): WGSL layout, 48-byte stride. */
+typedef struct clay_fluid_particle {
+  float pos[3];
+  float density;
+  float vel[3];
+  float pressure;
+  float nvel[3];
+  float pad;
+} clay_fluid_particle;
+
+/* `ContactList` (fluid.ts:55-58): WGSL layout (points start at byte 16). */
+typedef struct clay_contact_list {
+  uint32_t count;
+  uint32_t pad[3];
+  float points[32][4];
+} clay_contact_list;
+
+/* Arithmetic of the SPH passes. REFERENCE follows the reference's operation order with no
+ * fused multiply-add and plain f32 sums, and reproduces the f32 CPU restatement bit for
+ * bit. FAST (the default) lets the compiler contract multiply-adds and accumulates density
+ * with compensated (Kahan-Neumaier) summation. The bake is exact in both modes. */
+enum { CLAY_MODE_FAST = 0, CLAY_MODE_REFERENCE = 1 };
+
+/* new FluidSim(root, world, options) (fluid.ts:140). `world` may be NULL (no collider). */
+int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_opts* opts,
+                      clay_fluid** out);
+void clay_fluid_destroy(clay_fluid* sim);
+int clay_fluid_set_mode(clay_fluid* sim, int mode);
+/* FluidSim.spawn (fluid.ts:511-525). `spread` NULL = the reference default
+ * `spacing * cbrt(max(n,1)) * 0.62`. */
+int clay_fluid_spawn(clay_fluid* sim, int64_t n, const double pos[3], const double vel[3],
+                     const double* spread);
+/* FluidSim.configure (fluid.ts:528-530). `mask` = CLAY_P_* bits naming patched fields. */
+int clay_fluid_configure(clay_fluid* sim, const clay_fluid_params* patch, uint32_t mask);
+/* FluidSim.step (fluid.ts:536-558): emit, substeps, bake, enqueued on `stream`. */
+int clay_fluid_step(clay_fluid* sim, void* stream);
+/* FluidSim.particleCount (fluid.ts:496-498). */
+int64_t clay_fluid_particle_count(const clay_fluid* sim);
+/* The host copy of the uniform as the next step will write it (`frozen`, fluid.ts:185-203). */
+int clay_fluid_get_params(const clay_fluid* sim, clay_fluid_params* out);
+/* FluidSim.readContacts (fluid.ts:565-569): copies the raw ContactList into `host_out`
+ * asynchronously; n = min(count, 32) once the stream has completed. */
+int clay_fluid_read_contacts_async(clay_fluid* sim, clay_contact_list* host_out, void* stream);
+/* FluidSim.particles (fluid.ts:116): device pointer to `capacity` FluidParticle records. */
+int clay_fluid_particles_device(clay_fluid* sim, clay_fluid_particle** ptr, uint32_t* stride);
+/* Test hook: writes `count` records into slots [0, count) and sets the live count and the
+ * emission cursor to `count` (the reference can only emit jittered balls). Asynchronous. */
+int clay_fluid_upload(clay_fluid* sim, const clay_fluid_particle* host, int64_t count, void* stream);
+int clay_fluid_download(const clay_fluid* sim, clay_fluid_particle* host, int64_t count, void* stream);
+/* Test hook: the reference's `cellIndex` (fluid.ts:258-262) of each of the first
+ * particleCount particles, or 0xffffffff for a particle outside the grid (fluid.ts:319-321).
+ * Host output; synchronises `stream`. */
+int clay_fluid_cell_indices(clay_fluid* sim, uint32_t* host_out, void* stream);
+/* FluidSim.surface / .field (fluid.ts:119-120); owned by the sim. */
+clay_splat* clay_fluid_surface(clay_fluid* sim);
+clay_field* clay_fluid_field(clay_fluid* sim);
+/* Derived constants, for tests: h, rest density, grid resolution, grid origin. */
+typedef struct clay_fluid_info {
+  int64_t capacity;
+  int32_t substeps;
+  int32_t bucket;
+  int32_t grid_res;
+  double smoothing;
+  double rest_density;
+  double grid_origin[3];
+  double spacing;
+  double radius;
+  uint64_t device_bytes;
+} clay_fluid_info;
+int clay_fluid_get_info(const clay_fluid* sim, clay_fluid_info* out);
+
+/* ------------------------------------------------------------------------------------
+ * Batched stepping (no reference counterpart: the reference steps one FluidSim per
+ * `FluidSim.step`). Independent scenes of uneven size advance one frame each per launch:
+ * every pass of the frame runs once for all scenes, and the whole frame is captured into
+ * one CUDA graph.
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_batch clay_batch;
+int clay_batch_create(clay_ctx* ctx, clay_fluid* const* sims, int n, clay_batch** out);
+void clay_batch_destroy(clay_batch* b);
+/* Extra clouds baked in the same launch (e.g. clay-body shells), before the fluid steps. */
+int clay_batch_add_splat(clay_batch* b, clay_splat* s);
+/* Tile shapes: threads per block of the particle passes and particles per block. */
+typedef struct clay_batch_tuning {
+  int32_t sph_block;     /* threads per block of the neighbour passes: 64..512 */
+  int32_t splat_block;   /* threads per block of the splat pass: 64..512 */
+  int32_t use_graph;     /* 1: capture the frame into a CUDA graph */
+} clay_batch_tuning;
+int clay_batch_set_tuning(clay_batch* b, const clay_batch_tuning* t);
+int clay_batch_get_tuning(const clay_batch* b, clay_batch_tuning* t);
+/* One frame for every scene: host bookkeeping of each sim (as clay_fluid_step), then the
+ * batched passes (or the captured graph) on `stream`. */
+int clay_batch_step(clay_batch* b, void* stream);
+/* Frame with a subset of the scenes (indices into the batch), used by the server. */
+int clay_batch_step_subset(clay_batch* b, const int32_t* scenes, int n, void* stream);
+/* The ContactList of every scene, in batch order, copied into `host_out` (n records)
+ * asynchronously: one gather launch and one device-to-host copy. */
+int clay_batch_read_contacts_async(clay_batch* b, clay_contact_list* host_out, void* stream);
+/* One frame of the batch without the graph, each kernel bracketed by CUDA events on
+ * `stream`; per kernel (summed over substeps) its total milliseconds and launch count. */
+typedef struct clay_phase_time {
+  char name[32];
+  float ms;
+  int32_t launches;
+} clay_phase_time;
+int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int cap, int* n_out);
+/* Kernel launches one clay_batch_step enqueues (graph nodes count as launches). */
+int clay_batch_launches_per_step(const clay_batch* b, int64_t* out);
+
+/* ------------------------------------------------------------------------------------
+ * Number of library kernel launches enqueued by this process so far (all objects).
+ * ---------------------------------------------------------------------------------- */
+uint64_t clay_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CLAY_FLUID_H */

@@ -1,0 +1,379 @@
+"""ctypes wrapper of the CPU restatement in ``oracle/clay_oracle.cpp``.
+
+TEST INFRASTRUCTURE. Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg
+of ``bench.py`` import this module; the product path never does. Every function here
+forwards to the C++ restatement of the reference WGSL (see the header of
+``clay_oracle.h`` for the rounding rules and the reference lines each function follows).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libclay_oracle.so")
+
+
+def build() -> str:
+    """Compiles the restatement with its Makefile (g++, -ffp-contract=off)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = C.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+u16p = np.ctypeslib.ndpointer(dtype=np.uint16, flags="C_CONTIGUOUS")
+
+
+class Volume(C.Structure):
+    _fields_ = [
+        ("res", C.c_int32), ("mips", C.c_int32), ("origin", C.c_double * 3),
+        ("world_size", C.c_double), ("band", C.c_double), ("gradient_voxels", C.c_double),
+        ("dist", C.c_void_p), ("mat", C.c_void_p),
+    ]
+
+
+class Field(C.Structure):
+    _fields_ = [("n", C.c_int32), ("pad", C.c_int32), ("vol", Volume * 8),
+                ("offset", (C.c_double * 3) * 8)]
+
+
+class FluidCfg(C.Structure):
+    _fields_ = [
+        ("capacity", C.c_uint32), ("bucket", C.c_uint32), ("spacing", C.c_double),
+        ("h", C.c_double), ("radius", C.c_double), ("surface_radius", C.c_double),
+        ("material", C.c_double), ("bake_res", C.c_int32), ("bake_mips", C.c_int32),
+        ("bake_band", C.c_double), ("origin", C.c_double * 3), ("world_size", C.c_double),
+        ("substeps", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("gravity", C.c_float * 3), ("dt", C.c_float), ("emit_pos", C.c_float * 3),
+        ("emit_radius", C.c_float), ("emit_vel", C.c_float * 3), ("max_speed", C.c_float),
+        ("stiffness", C.c_float), ("viscosity", C.c_float), ("damping", C.c_float),
+        ("count", C.c_uint32), ("emit_base", C.c_uint32), ("emit_count", C.c_uint32),
+        ("emit_seed", C.c_uint32), ("contact_depth", C.c_float),
+    ]
+
+
+class FluidDerived(C.Structure):
+    _fields_ = [
+        ("h", C.c_double), ("poly6", C.c_double), ("spiky_grad", C.c_double),
+        ("mass", C.c_double), ("rest_density", C.c_double), ("grid_res", C.c_int32),
+        ("pad", C.c_int32), ("grid_origin", C.c_double * 3), ("wall_lo", C.c_double * 3),
+        ("wall_hi", C.c_double * 3),
+    ]
+
+
+class Cloud(C.Structure):
+    _fields_ = [
+        ("capacity", C.c_uint32), ("pos_stride", C.c_uint32), ("pos", C.c_void_p),
+        ("live_mode", C.c_uint32), ("live_a", C.c_uint32), ("live_b", C.c_uint32),
+        ("nrm_stride", C.c_uint32), ("nrm", C.c_void_p), ("quat", C.c_void_p),
+    ]
+
+
+class SplatCfg(C.Structure):
+    _fields_ = [
+        ("res", C.c_int32), ("mips", C.c_int32), ("band", C.c_double), ("radius", C.c_double),
+        ("world_size", C.c_double), ("material", C.c_double), ("origin", C.c_double * 3),
+    ]
+
+
+BRUSH_DTYPE = np.dtype([
+    ("pos", np.float32, 3), ("scale", np.float32), ("rot", np.float32, 4),
+    ("size", np.float32, 3), ("radius", np.float32), ("material", np.float32),
+    ("blend", np.float32), ("bound", np.float32), ("mask", np.float32),
+    ("kind", np.uint32), ("op", np.uint32), ("slot", np.uint32), ("pad", np.uint32),
+])
+assert BRUSH_DTYPE.itemsize == 80
+
+PARTICLE_DTYPE = np.dtype([
+    ("pos", np.float32, 3), ("density", np.float32), ("vel", np.float32, 3),
+    ("pressure", np.float32), ("nvel", np.float32, 3), ("pad", np.float32),
+])
+assert PARTICLE_DTYPE.itemsize == 48
+PARTICLE_DTYPE_F64 = np.dtype([
+    ("pos", np.float64, 3), ("density", np.float64), ("vel", np.float64, 3),
+    ("pressure", np.float64), ("nvel", np.float64, 3), ("pad", np.float64),
+])
+
+
+def _declare(L):
+    L.orc_hash1.argtypes = [C.c_uint32]
+    L.orc_hash1.restype = C.c_float
+    L.orc_hash3.argtypes = [C.c_uint32, f32p]
+    L.orc_f32_to_f16.argtypes = [C.c_float]
+    L.orc_f32_to_f16.restype = C.c_uint16
+    L.orc_f16_to_f32.argtypes = [C.c_uint16]
+    L.orc_f16_to_f32.restype = C.c_float
+    L.orc_volume_mip_levels.argtypes = [C.c_int32, C.c_int32, C.c_char_p, C.c_int32]
+    L.orc_volume_mip_levels.restype = C.c_int32
+    L.orc_volume_total_voxels.argtypes = [C.c_int32, C.c_int32]
+    L.orc_volume_total_voxels.restype = C.c_int64
+    L.orc_field_query_f32.argtypes = [C.POINTER(Field), f32p, f32p, f32p]
+    L.orc_field_query_f64.argtypes = [C.POINTER(Field), f64p, f64p, f64p]
+    L.orc_rest_density.argtypes = [C.c_double, C.c_double]
+    L.orc_rest_density.restype = C.c_double
+    L.orc_fluid_derive.argtypes = [C.POINTER(FluidCfg), C.POINTER(FluidDerived)]
+    L.orc_fluid_cells.argtypes = [C.POINTER(FluidCfg), C.c_void_p, C.c_uint32, u32p]
+    L.orc_fluid_emit.argtypes = [C.POINTER(FluidCfg), C.POINTER(Params), C.c_void_p]
+    L.orc_fluid_substep_f32.argtypes = [
+        C.POINTER(FluidCfg), C.POINTER(Params), C.POINTER(Field), C.c_void_p,
+        C.POINTER(C.c_uint32), f32p, u32p, C.c_uint32, C.c_int32]
+    L.orc_fluid_substep_f64.argtypes = [
+        C.POINTER(FluidCfg), C.POINTER(Params), C.POINTER(Field), C.c_void_p, C.c_int32]
+    L.orc_fluid_density_f64.argtypes = [
+        C.POINTER(FluidCfg), C.POINTER(Params), C.c_void_p, f64p, C.c_int32]
+    L.orc_splat_encode.argtypes = [C.c_float, C.c_float]
+    L.orc_splat_encode.restype = C.c_uint32
+    L.orc_splat_decode.argtypes = [C.c_uint32]
+    L.orc_splat_decode.restype = C.c_float
+    L.orc_splat_keys.argtypes = [C.POINTER(SplatCfg), C.POINTER(Cloud), u32p, C.c_int32]
+    L.orc_splat_resolve.argtypes = [C.POINTER(SplatCfg), u32p, u16p, u16p]
+    L.orc_splat_values_f64.argtypes = [C.POINTER(SplatCfg), C.POINTER(Cloud), f64p, C.c_int32]
+    L.orc_build_brushes.argtypes = [C.POINTER(Volume), C.c_void_p, C.c_int32, u16p, u16p, C.c_int32]
+    L.orc_eval_brush.argtypes = [C.c_void_p, f32p, C.c_int32, f32p]
+
+
+# ---------------------------------------------------------------------------------------
+# Thin Python helpers over the C entry points.
+
+def hash1(seed: int) -> float:
+    return float(lib().orc_hash1(seed & 0xFFFFFFFF))
+
+
+def hash3(seed: int) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    lib().orc_hash3(seed & 0xFFFFFFFF, out)
+    return out
+
+
+def f32_to_f16(a: np.ndarray) -> np.ndarray:
+    a = np.asarray(a, np.float32).ravel()
+    return np.array([lib().orc_f32_to_f16(float(x)) for x in a], np.uint16)
+
+
+def mip_levels(resolution: int, requested: int | None = None):
+    err = C.create_string_buffer(256)
+    m = lib().orc_volume_mip_levels(resolution, -1 if requested is None else requested, err, 256)
+    if m < 0:
+        raise ValueError(err.value.decode())
+    return m
+
+
+def total_voxels(res: int, mips: int) -> int:
+    return int(lib().orc_volume_total_voxels(res, mips))
+
+
+class VolumeData:
+    """A volume as f16 planes plus its geometry, the oracle's view of an SdfVolume."""
+
+    def __init__(self, res, mips, origin, world_size, band=4.0, gradient_voxels=1.0,
+                 dist=None, mat=None):
+        self.res, self.mips = int(res), int(mips)
+        self.origin = tuple(float(x) for x in origin)
+        self.world_size, self.band = float(world_size), float(band)
+        self.gradient_voxels = float(gradient_voxels)
+        n = total_voxels(self.res, self.mips)
+        self.dist = np.ascontiguousarray(dist if dist is not None else np.full(n, 0x3C00, np.uint16), np.uint16)
+        self.mat = np.ascontiguousarray(mat if mat is not None else np.zeros(n, np.uint16), np.uint16)
+
+    def c(self) -> Volume:
+        v = Volume()
+        v.res, v.mips = self.res, self.mips
+        v.origin[:] = self.origin
+        v.world_size, v.band, v.gradient_voxels = self.world_size, self.band, self.gradient_voxels
+        v.dist = self.dist.ctypes.data
+        v.mat = self.mat.ctypes.data
+        return v
+
+
+def make_field(volumes, offsets=None) -> Field:
+    f = Field()
+    f.n = len(volumes)
+    for i, v in enumerate(volumes):
+        f.vol[i] = v.c()
+        off = offsets[i] if offsets is not None else (0.0, 0.0, 0.0)
+        f.offset[i][:] = off
+    return f
+
+
+def field_query_f32(field: Field, pts: np.ndarray):
+    pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+    s = np.zeros((len(pts), 2), np.float32)
+    n = np.zeros((len(pts), 3), np.float32)
+    o2, o3 = np.zeros(2, np.float32), np.zeros(3, np.float32)
+    for i, p in enumerate(pts):
+        lib().orc_field_query_f32(C.byref(field), np.ascontiguousarray(p), o2, o3)
+        s[i], n[i] = o2, o3
+    return s, n
+
+
+def fluid_cfg(**kw) -> FluidCfg:
+    c = FluidCfg()
+    for k, v in kw.items():
+        if k == "origin":
+            c.origin[:] = v
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def derive(cfg: FluidCfg) -> FluidDerived:
+    d = FluidDerived()
+    lib().orc_fluid_derive(C.byref(cfg), C.byref(d))
+    return d
+
+
+def params_from(d: dict) -> Params:
+    p = Params()
+    for k, v in d.items():
+        if isinstance(v, (list, tuple, np.ndarray)):
+            getattr(p, k)[:] = [float(x) for x in v]
+        else:
+            setattr(p, k, v)
+    return p
+
+
+def fluid_cells(cfg: FluidCfg, parts: np.ndarray) -> np.ndarray:
+    parts = np.ascontiguousarray(parts, PARTICLE_DTYPE)
+    keys = np.zeros(len(parts), np.uint32)
+    lib().orc_fluid_cells(C.byref(cfg), parts.ctypes.data, len(parts), keys)
+    return keys
+
+
+def fluid_emit(cfg: FluidCfg, prm: Params, parts: np.ndarray) -> None:
+    assert parts.dtype == PARTICLE_DTYPE and parts.flags["C_CONTIGUOUS"]
+    lib().orc_fluid_emit(C.byref(cfg), C.byref(prm), parts.ctypes.data)
+
+
+def fluid_substep_f32(cfg, prm, field, parts, threads=1, max_ids=1 << 20):
+    """One substep in place on an f32 particle array. Returns (count, points[32,4], ids)."""
+    assert parts.dtype == PARTICLE_DTYPE and parts.flags["C_CONTIGUOUS"]
+    cnt = C.c_uint32(0)
+    pts = np.zeros(32 * 4, np.float32)
+    ids = np.zeros(max(max_ids, 1), np.uint32)
+    lib().orc_fluid_substep_f32(C.byref(cfg), C.byref(prm), C.byref(field) if field else None,
+                                parts.ctypes.data, C.byref(cnt), pts, ids, max_ids, threads)
+    n = cnt.value
+    return n, pts.reshape(32, 4), ids[: min(n, max_ids)].copy()
+
+
+def fluid_substep_f64(cfg, prm, field, parts_d, threads=1):
+    assert parts_d.dtype == PARTICLE_DTYPE_F64 and parts_d.flags["C_CONTIGUOUS"]
+    lib().orc_fluid_substep_f64(C.byref(cfg), C.byref(prm), C.byref(field) if field else None,
+                                parts_d.ctypes.data, threads)
+
+
+def fluid_density_f64(cfg, prm, parts, threads=1) -> np.ndarray:
+    parts = np.ascontiguousarray(parts, PARTICLE_DTYPE)
+    out = np.zeros(2 * len(parts), np.float64)
+    lib().orc_fluid_density_f64(C.byref(cfg), C.byref(prm), parts.ctypes.data, out, threads)
+    return out.reshape(-1, 2)
+
+
+def to_f64(parts: np.ndarray) -> np.ndarray:
+    out = np.zeros(len(parts), PARTICLE_DTYPE_F64)
+    for name in PARTICLE_DTYPE.names:
+        out[name] = parts[name]
+    return out
+
+
+def splat_cfg(res, mips, band, radius, world_size=24.0, material=0.0, origin=(-12.0, -4.0, -12.0)):
+    c = SplatCfg()
+    c.res, c.mips, c.band, c.radius = res, mips, band, radius
+    c.world_size, c.material = world_size, material
+    c.origin[:] = origin
+    return c
+
+
+class CloudData:
+    """A ParticleCloud as arrays (positions, optional normals, liveness rule)."""
+
+    def __init__(self, pos, normals=None, quat=None, live_mode=0, live_a=0, live_b=0):
+        self.pos = np.ascontiguousarray(pos, np.float32)
+        self.pos_stride = self.pos.shape[1] if self.pos.ndim == 2 else 3
+        self.normals = None if normals is None else np.ascontiguousarray(normals, np.float32)
+        self.quat = None if quat is None else np.ascontiguousarray(quat, np.float32)
+        self.live_mode, self.live_a, self.live_b = live_mode, live_a, live_b
+
+    def c(self) -> Cloud:
+        c = Cloud()
+        c.capacity = self.pos.shape[0]
+        c.pos_stride = self.pos_stride
+        c.pos = self.pos.ctypes.data
+        c.live_mode, c.live_a, c.live_b = self.live_mode, self.live_a, self.live_b
+        if self.normals is not None:
+            c.nrm = self.normals.ctypes.data
+            c.nrm_stride = self.normals.shape[1]
+        if self.quat is not None:
+            c.quat = self.quat.ctypes.data
+        return c
+
+
+def enc(sd: float, bw: float = 1.0) -> int:
+    return int(lib().orc_splat_encode(sd, bw))
+
+
+def dec(key: int) -> float:
+    return float(lib().orc_splat_decode(key))
+
+
+def splat_keys(cfg: SplatCfg, cloud: CloudData, threads=1) -> np.ndarray:
+    keys = np.zeros(total_voxels(cfg.res, cfg.mips), np.uint32)
+    cc = cloud.c()
+    lib().orc_splat_keys(C.byref(cfg), C.byref(cc), keys, threads)
+    return keys
+
+
+def splat_resolve(cfg: SplatCfg, keys: np.ndarray):
+    n = total_voxels(cfg.res, cfg.mips)
+    d = np.zeros(n, np.uint16)
+    m = np.zeros(n, np.uint16)
+    lib().orc_splat_resolve(C.byref(cfg), np.ascontiguousarray(keys, np.uint32), d, m)
+    return d, m
+
+
+def splat_values_f64(cfg: SplatCfg, cloud: CloudData, threads=1) -> np.ndarray:
+    vals = np.zeros(total_voxels(cfg.res, cfg.mips), np.float64)
+    cc = cloud.c()
+    lib().orc_splat_values_f64(C.byref(cfg), C.byref(cc), vals, threads)
+    return vals
+
+
+def build_brushes(vol: VolumeData, brushes: np.ndarray, threads=1):
+    brushes = np.ascontiguousarray(brushes, BRUSH_DTYPE)
+    n = total_voxels(vol.res, vol.mips)
+    d = np.zeros(n, np.uint16)
+    m = np.zeros(n, np.uint16)
+    v = vol.c()
+    lib().orc_build_brushes(C.byref(v), brushes.ctypes.data, len(brushes), d, m, threads)
+    return d, m
+
+
+def eval_brush(brush: np.ndarray, pts) -> np.ndarray:
+    b = np.ascontiguousarray(np.asarray(brush, BRUSH_DTYPE).reshape(1))
+    pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+    out = np.zeros(len(pts), np.float32)
+    lib().orc_eval_brush(b.ctypes.data, pts.ravel(), len(pts), out)
+    return out

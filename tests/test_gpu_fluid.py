@@ -1,0 +1,230 @@
+"""FluidSim on the GPU against the oracle.
+
+Reference mode reproduces the f32 restatement bit for bit, frame after frame: the cell build,
+emission, density/pressure, forces, integration with collision, the contact counter and the
+bake. Fast mode (FMA contraction, compensated density) is held to a stated tolerance against
+the same restatement, and its density error against the f64 twin must be at most 1e-4.
+"""
+import numpy as np
+import pytest
+
+from oracle.fluid_frame import OracleFluid
+
+pytestmark = pytest.mark.gpu
+
+ORIGIN = (-12.0, -4.0, -12.0)
+# Fast mode vs the f32 restatement, one frame from the same state: contraction and
+# compensated summation change the last bits of each sum; the state is relative to its scale.
+FAST_REL_TOL = 2e-5
+
+
+def make_collider(root, oracle, res=96):
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    v = ce.SdfVolume(root, resolution=res, worldSize=24.0, origin=ORIGIN)
+    v.build(scenes.config1_collider_brushes())
+    d, m = v.download()
+    ov = oracle.VolumeData(res, v.mipLevels, ORIGIN, 24.0, 4.0, dist=d, mat=m)
+    return v, ce.volumeField(v), ov
+
+
+CFG1 = dict(capacity=4096, spacing=0.1, radius=0.05, substeps=2, gravity=(0, -9.8, 0), bakeResolution=64,
+            bakeMipLevels=3, bakeBand=4.0, worldSize=24.0, origin=ORIGIN)
+
+
+def blob(n_side=16, spacing=0.1, center=(0.0, 3.0, 0.0), seed=1, vel=(0, 0, 0)):
+    from clay_engine_b200 import scenes
+
+    p = scenes.jittered_lattice(n_side, spacing, center, seed)
+    p["vel"] = vel
+    return p
+
+
+def make_pair(root, oracle, opts, parts=None, mode="reference", with_collider=True):
+    import clay_engine_b200 as ce
+
+    vol = field = ov = None
+    if with_collider:
+        vol, field, ov = make_collider(root, oracle)
+    sim = ce.FluidSim(root, field, opts)
+    sim.set_mode(mode)
+    ref = OracleFluid(oracle, [ov] if ov else [], **opts)
+    if parts is not None:
+        sim.upload(parts)
+        ref.upload(parts)
+    return sim, ref, (vol, field)
+
+
+def gpu_keys(sim):
+    import torch
+
+    keys = torch.zeros(sim.surface.volume.totalVoxels, dtype=torch.int32).cuda()
+    sim.surface.capture_keys(keys)
+    return keys
+
+
+def assert_state_equal(g, r, n, what=""):
+    for name in ("pos", "vel", "density", "pressure", "nvel"):
+        a = np.ascontiguousarray(g[name][:n]).view(np.uint32)
+        b = np.ascontiguousarray(r[name][:n]).view(np.uint32)
+        bad = np.nonzero((a != b).reshape(n, -1).any(1))[0]
+        assert bad.size == 0, f"{what}{name}: {bad.size} particles differ, first {bad[:4]}: " \
+                              f"gpu {g[name][bad[:2]]} oracle {r[name][bad[:2]]}"
+
+
+def test_cell_indices_are_bit_exact(root, oracle):
+    """cellIndex (fluid.ts:253-262) including particles outside the grid (:319-321)."""
+    p = blob()
+    rng = np.random.default_rng(2)
+    p["pos"][:200] = rng.uniform(-20, 30, (200, 3)).astype(np.float32)  # some outside the grid
+    sim, ref, keep = make_pair(root, oracle, CFG1, p)
+    g = sim.cell_indices()
+    o = oracle.fluid_cells(ref.cfg, p)
+    assert (g == o).all()
+    assert (o == 0xFFFFFFFF).any() and (o != 0xFFFFFFFF).any()
+    sim.destroy()
+
+
+def test_reference_mode_frames_are_bit_exact(root, oracle):
+    """Config 1 (4096 particles, 2 substeps, 96^3 collider, 64^3 x 3 bake) for 6 frames."""
+    sim, ref, keep = make_pair(root, oracle, CFG1, blob(vel=(0.5, -1.0, 0.2)))
+    keys = gpu_keys(sim)
+    import torch
+
+    for frame in range(6):
+        sim.step()
+        ok = ref.step()
+        g = sim.download()
+        assert_state_equal(g, ref.parts, sim.particleCount, f"frame {frame}: ")
+        gk = keys.cpu().numpy().view(np.uint32)
+        assert (gk == ok).all(), f"frame {frame}: {(gk != ok).sum()} bake keys differ"
+        pts, count = sim.readContacts()
+        assert count == ref.contacts[0]
+    torch.cuda.synchronize()
+    sim.destroy()
+
+
+def test_reference_mode_falling_onto_the_collider(root, oracle):
+    """A blob dropped onto the plate: collision, normals and contacts all engage."""
+    opts = dict(CFG1, capacity=2048)
+    p = blob(12, 0.1, center=(2.5, 0.2, 0.0), vel=(0.0, -4.0, 0.0))
+    sim, ref, keep = make_pair(root, oracle, opts, p)
+    hits = 0
+    for frame in range(5):
+        sim.step()
+        ref.step()
+        assert_state_equal(sim.download(), ref.parts, sim.particleCount, f"frame {frame}: ")
+        pts, count = sim.readContacts()
+        assert count == ref.contacts[0]
+        hits += count
+        # every recorded point is one of the oracle's contacts (atomic order differs)
+        if count:
+            ids = ref.contacts[2]
+            cand = ref.parts["pos"][ids]
+            for q in pts:
+                assert np.min(np.abs(cand - np.asarray(q[:3], np.float32)).sum(1)) == 0
+    assert hits > 0, "vacuous: nothing touched the collider"
+    sim.destroy()
+
+
+def test_emission_and_ring_wrap_are_bit_exact(root, oracle):
+    """spawn (fluid.ts:511-525) + emit (:268-291) with the ring buffer wrapping (:540-544)."""
+    opts = dict(CFG1, capacity=1000)
+    sim, ref, keep = make_pair(root, oracle, opts)
+    for frame in range(5):
+        sim.spawn(300, (0.5, 4.0, -0.5), (0.0, -2.0 - 0.1 * frame, 0.3))
+        ref.spawn(300, (0.5, 4.0, -0.5), (0.0, -2.0 - 0.1 * frame, 0.3))
+        sim.step()
+        ref.step()
+        assert sim.particleCount == ref.live
+        assert_state_equal(sim.download(), ref.parts, sim.particleCount, f"frame {frame}: ")
+    assert sim.particleCount == 1000
+    sim.destroy()
+
+
+def test_bucket_overflow_keeps_the_lowest_indices(root, oracle):
+    """A pile denser than `bucket` per cell: full cells keep their `bucket` lowest indices."""
+    opts = dict(CFG1, capacity=3000, bucket=8)
+    p = blob(14, 0.05, center=(0.0, 3.0, 0.0))
+    sim, ref, keep = make_pair(root, oracle, opts, p[:2744])
+    for frame in range(3):
+        sim.step()
+        ref.step()
+        assert_state_equal(sim.download(), ref.parts, sim.particleCount, f"frame {frame}: ")
+    sim.destroy()
+
+
+def test_no_collider_and_walls(root, oracle):
+    """world = none; particles pushed against the bake box walls (fluid.ts:484-489)."""
+    opts = dict(CFG1, capacity=1000)
+    p = blob(10, 0.1, center=(11.9, -3.9, 0.0), vel=(3.0, -3.0, 0.0))
+    sim, ref, keep = make_pair(root, oracle, opts, p, with_collider=False)
+    for frame in range(3):
+        sim.step()
+        ref.step()
+        assert_state_equal(sim.download(), ref.parts, sim.particleCount, f"frame {frame}: ")
+    g = sim.download()
+    assert (g["pos"][:, 0] <= np.float32(12.0 - 0.05)).all()
+    sim.destroy()
+
+
+def test_nothing_alive_still_clears_the_bake(root, oracle):
+    import clay_engine_b200 as ce
+
+    sim = ce.FluidSim(root, None, dict(CFG1, capacity=64))
+    sim.step()
+    d, _ = sim.surface.volume.download()
+    assert (d == 0x3C00).all()
+    assert sim.particleCount == 0
+    sim.destroy()
+
+
+def test_configure_and_params(root, oracle):
+    import clay_engine_b200 as ce
+
+    sim = ce.FluidSim(root, None, dict(CFG1, capacity=64))
+    p = sim.params
+    assert p["dt"] == pytest.approx(1 / 120) and p["maxSpeed"] == 15 and p["stiffness"] == 220
+    assert p["contactDepth"] == pytest.approx(0.075)
+    sim.configure({"viscosity": 0.8, "gravity": (0, -1, 0)})
+    assert sim.params["viscosity"] == pytest.approx(0.8) and sim.params["gravity"][1] == -1
+    with pytest.raises(ce.ClayError):
+        sim.configure({"count": 5})
+    sim.destroy()
+
+
+def test_fast_mode_within_tolerance(root, oracle):
+    """Fast mode from the same state as the oracle (teacher forcing each frame): every field
+    within FAST_REL_TOL of its scale."""
+    sim, ref, keep = make_pair(root, oracle, CFG1, blob(vel=(0.5, -1.0, 0.2)), mode="fast")
+    for frame in range(3):
+        state = sim.download()
+        ref.upload(state)  # teacher forcing: both start the frame from the GPU's state
+        sim.step()
+        ref.step()
+        g = sim.download()
+        n = sim.particleCount
+        for name in ("pos", "vel", "nvel", "density", "pressure"):
+            a = g[name][:n].astype(np.float64)
+            b = ref.parts[name][:n].astype(np.float64)
+            scale = max(np.abs(b).max(), 1e-6)
+            err = np.abs(a - b).max() / scale
+            assert err <= FAST_REL_TOL, f"frame {frame} {name}: rel err {err:.3g}"
+    sim.destroy()
+
+
+def test_density_error_against_f64(root, oracle):
+    """Precision target: per-particle density of the GPU within 1e-4 relative of the f64 twin,
+    from the same input state (one substep)."""
+    opts = dict(CFG1, substeps=1)
+    for mode in ("fast", "reference"):
+        sim, ref, keep = make_pair(root, oracle, opts, blob(vel=(0.1, 0.0, 0.0)), mode=mode)
+        state = sim.download()
+        sim.step()
+        g = sim.download()
+        prm = oracle.params_from(dict(ref.frozen, count=sim.particleCount, emit_base=0, emit_count=0))
+        d64 = oracle.fluid_density_f64(ref.cfg, prm, state, threads=8)
+        rel = np.abs(g["density"].astype(np.float64) - d64[:, 0]) / np.abs(d64[:, 0])
+        assert rel.max() <= 1e-4, f"{mode}: density rel err {rel.max():.3g}"
+        sim.destroy()
