@@ -14,8 +14,12 @@ pytestmark = pytest.mark.gpu
 
 ORIGIN = (-12.0, -4.0, -12.0)
 # Fast mode vs the f32 restatement, one frame from the same state: contraction and
-# compensated summation change the last bits of each sum; the state is relative to its scale.
+# compensated summation change the last bits of each sum. Errors are relative to the field's
+# largest magnitude. Pressure = stiffness * (rho - rho0) subtracts two nearly equal numbers,
+# so a density difference of a few ulps becomes a larger relative pressure difference: it
+# gets its own bound.
 FAST_REL_TOL = 2e-5
+FAST_REL_TOL_PRESSURE = 2e-4
 
 
 def make_collider(root, oracle, res=96):
@@ -108,7 +112,8 @@ def test_reference_mode_frames_are_bit_exact(root, oracle):
 def test_reference_mode_falling_onto_the_collider(root, oracle):
     """A blob dropped onto the plate: collision, normals and contacts all engage."""
     opts = dict(CFG1, capacity=2048)
-    p = blob(12, 0.1, center=(2.5, 0.2, 0.0), vel=(0.0, -4.0, 0.0))
+    # on top of the 9.5 x 1.4 x 0.9 box (top face y = 1.4), clear of the sphere cut
+    p = blob(12, 0.1, center=(6.0, 2.05, 0.0), vel=(0.0, -6.0, 0.0))
     sim, ref, keep = make_pair(root, oracle, opts, p)
     hits = 0
     for frame in range(5):
@@ -210,7 +215,8 @@ def test_fast_mode_within_tolerance(root, oracle):
             b = ref.parts[name][:n].astype(np.float64)
             scale = max(np.abs(b).max(), 1e-6)
             err = np.abs(a - b).max() / scale
-            assert err <= FAST_REL_TOL, f"frame {frame} {name}: rel err {err:.3g}"
+            tol = FAST_REL_TOL_PRESSURE if name == "pressure" else FAST_REL_TOL
+            assert err <= tol, f"frame {frame} {name}: rel err {err:.3g}"
     sim.destroy()
 
 
