@@ -117,9 +117,20 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # nvidia-smi's start-up holds the driver for a moment: let it finish before timing
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 15:
+                time.sleep(0.05)
         except OSError:
             self.proc = None
         return self
+
+    def mark(self):
+        """Starts the sample window of the timed region."""
+        self.start = len(self.lines)
+
+    def stop(self):
+        self.end = len(self.lines)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -136,7 +147,8 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        lines = self.lines[getattr(self, "start", 0):getattr(self, "end", len(self.lines)) + 1]
+        for ln in lines:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -311,6 +323,7 @@ def main():
     batch = ce.Batch(root, sims, extra_splats=bodies, use_graph=True)
     stream = torch.cuda.Stream()
     torch.cuda.synchronize()
+    clocks = ClockSampler(local).__enter__()
 
     # warm-up (also captures the graph)
     for _ in range(max(args.warmup, 1)):
@@ -322,12 +335,13 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier(ws)
     torch.cuda.synchronize()
-    with ClockSampler(local) as clocks:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            batch.step(stream)
-        ev1.record(stream)
-        ev1.synchronize()
+    clocks.mark()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        batch.step(stream)
+    ev1.record(stream)
+    ev1.synchronize()
+    clocks.stop()
     torch.cuda.synchronize()
     barrier(ws)
     launches = ce.kernel_launch_count() - l0
@@ -388,6 +402,7 @@ def main():
         plain_ms = max_over_ranks(ws, p0.elapsed_time(p1))
         plain_value = total_particles * args.plain_steps / (plain_ms / 1000)
 
+    clocks.__exit__(None, None, None)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, total, dt, desc = cpu_sample(n_scenes, seed, 20000, os.cpu_count() or 1)
