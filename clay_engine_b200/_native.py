@@ -142,6 +142,7 @@ SIGNATURES = {
     "clay_splat_volume": (P, [P]),
     "clay_splat_field": (P, [P]),
     "clay_splat_capture_keys": (I, [P, P]),
+    "clay_splat_bake_static": (I, [C.POINTER(CloudDesc), C.POINTER(SplatOpts), P, P, P]),
     "clay_fluid_create": (I, [P, P, C.POINTER(FluidOpts), C.POINTER(P)]),
     "clay_fluid_destroy": (None, [P]),
     "clay_fluid_set_mode": (I, [P, I]),

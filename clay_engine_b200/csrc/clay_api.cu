@@ -49,6 +49,8 @@ constexpr int TILE = 8;
 
 }  // namespace
 
+int clay::report_error(int code, const char* msg) { return fail(code, "%s", msg); }
+
 // ------------------------------------------------------------------------------------------
 // Context and staging ring.
 struct clay_ctx {

@@ -827,7 +827,6 @@ __global__ void k_forces_integrate(const SceneDev* __restrict__ scenes, const Wo
   S.parts[S.sorted_id[k]] = out;
 }
 
-#ifndef CLAY_ONLY_NEIGHBOUR_PASSES
 // ---------------------------------------------------------------------------------------
 // SplatField bake (splat.ts:200-276).
 //
@@ -863,9 +862,9 @@ __device__ __forceinline__ bool cloud_live(const SplatDev& D, uint32_t idx, uint
   return true;
 }
 
-__global__ void __launch_bounds__(32 * kSplatWarps) k_splat(const SplatDev* __restrict__ splats, const Work* __restrict__ work) {
-  Work w = get_work(work);
-  const SplatDev& D = splats[w.obj];
+// One block of the splat pass: level w.sub, cloud indices [w.first, w.first + w.n). The
+// volume origin (ox, oy, oz) is the f32 uniform of the baked volume.
+__device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, float ox, float oy, float oz) {
   const int m = static_cast<int>(w.sub);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   __shared__ float4 s_p[kSplatWarps][32];
@@ -884,9 +883,9 @@ __global__ void __launch_bounds__(32 * kSplatWarps) k_splat(const SplatDev* __re
   int lx = 0, ly = 0, lz = 0, hx = -1, hy = -1, hz = -1;
   if (live) {
     const float* pp = reinterpret_cast<const float*>(D.pos + static_cast<size_t>(i) * D.pos_stride);
-    px = pp[0] - D.vp->origin[0];
-    py = pp[1] - D.vp->origin[1];
-    pz = pp[2] - D.vp->origin[2];
+    px = pp[0] - ox;
+    py = pp[1] - oy;
+    pz = pp[2] - oz;
     if (has_n) {
       const float* nn = reinterpret_cast<const float*>(D.nrm + static_cast<size_t>(i) * D.nrm_stride);
       nx = nn[0];
@@ -1003,9 +1002,7 @@ __global__ void __launch_bounds__(32 * kSplatWarps) k_splat(const SplatDev* __re
 // resolve[m] (splat.ts:258-276): v = f32(key) * (1/32767.5) - 1 stored as f16 (round to
 // nearest even). The key is reset to 65535 behind the read, which is the clear of the
 // next bake (splat.ts:200-210): the grid holds 65535 everywhere between bakes.
-__global__ void k_resolve(const SplatDev* __restrict__ splats, const Work* __restrict__ work) {
-  Work w = get_work(work);
-  const SplatDev& D = splats[w.obj];
+__device__ __forceinline__ void resolve_block(const SplatDev& D, const Work w) {
   const long long base = static_cast<long long>(w.first) * 4;
   const long long v0 = base + static_cast<long long>(threadIdx.x) * 4;
   const float inv = 3.0518043793392844e-05f;  // f32(1/32767.5)
@@ -1028,6 +1025,18 @@ __global__ void k_resolve(const SplatDev* __restrict__ splats, const Work* __res
       D.dist_out[v] = __float2half_rn(static_cast<float>(key) * inv - 1.0f);
     }
   }
+}
+
+#ifndef CLAY_ONLY_NEIGHBOUR_PASSES
+__global__ void __launch_bounds__(32 * kSplatWarps) k_splat(const SplatDev* __restrict__ splats, const Work* __restrict__ work) {
+  const Work w = get_work(work);
+  const SplatDev& D = splats[w.obj];
+  splat_block(D, w, D.vp->origin[0], D.vp->origin[1], D.vp->origin[2]);
+}
+
+__global__ void k_resolve(const SplatDev* __restrict__ splats, const Work* __restrict__ work) {
+  const Work w = get_work(work);
+  resolve_block(splats[w.obj], w);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -11,6 +11,9 @@
 
 namespace clay {
 
+// Records `msg` as the calling thread's clay_last_error() and returns `code`.
+int report_error(int code, const char* msg);
+
 uint64_t launch_count();
 void count_launch();
 void count_launches(uint64_t n);  // kernels replayed by a graph launch

@@ -217,6 +217,22 @@ void clay_splat_destroy(clay_splat* s);
 int clay_splat_set_center(clay_splat* s, double x, double y, double z);
 /* SplatField.bake (splat.ts:296-304). */
 int clay_splat_bake(clay_splat* s, void* stream);
+/* A SplatField bake that allocates no device memory. No counterpart in the reference: it
+ * is for callers that may not allocate once running - a per-frame tick where cudaMalloc or
+ * cudaFree would synchronise the device and stall the frame, or a plugin host that gives
+ * the library only buffers allocated up front. The caller passes the cloud and the output
+ * planes (`dist_out_f16`, and `material_out_f16` or NULL; total-voxel halves each, levels
+ * concatenated as in an SdfVolume); options as clay_splat_create, origin taken from
+ * `opts` (default [-12,-4,-12]). Output is bit for bit that of clay_splat_bake.
+ * Limit: at most CLAY_STATIC_BAKE_MAX_VOXELS voxels over all levels (e.g. 96^3 with 3
+ * levels); larger bakes are refused with CLAY_EINVAL. The key scratch is one fixed
+ * file-scope device array (4 MiB, held by every GPU that loads the library until exit)
+ * shared by every call: each call clears it before use, and calls that overlap on the GPU
+ * race on it, so order them. The first call on each device also looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream capture. */
+#define CLAY_STATIC_BAKE_MAX_VOXELS 1048576
+int clay_splat_bake_static(const clay_cloud_desc* cloud, const clay_splat_opts* opts, void* dist_out_f16,
+                           void* material_out_f16, void* stream);
 /* SplatField.volume / .field. The returned objects are owned by the splat. */
 clay_volume* clay_splat_volume(clay_splat* s);
 clay_field* clay_splat_field(clay_splat* s);
