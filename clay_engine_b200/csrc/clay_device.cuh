@@ -864,6 +864,15 @@ __device__ __forceinline__ bool cloud_live(const SplatDev& D, uint32_t idx, uint
 
 // One block of the splat pass: level w.sub, cloud indices [w.first, w.first + w.n). The
 // volume origin (ox, oy, oz) is the f32 uniform of the baked volume.
+//
+// Two strategies, chosen per block from the particles' voxel boxes:
+//  - block walk: when the union U of the block's boxes is compact (a cell-ordered fluid),
+//    each thread owns 4 voxels of U along x and takes the minimum over every live particle
+//    of the block, read as broadcasts from shared memory; one atomicMin per voxel per block.
+//    dy*dy and dz*dz are computed once per particle and row, so the squared length keeps the
+//    reference's rounding order (dx*dx + dy*dy) + dz*dz.
+//  - warp walk: otherwise each warp works on its 32 particles, walking their union box with a
+//    voxel per lane when that is compact, or each particle's own box.
 __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, float ox, float oy, float oz) {
   const int m = static_cast<int>(w.sub);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -871,6 +880,12 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   __shared__ float4 s_n[kSplatWarps][32];
   __shared__ int4 s_lo[kSplatWarps][32];
   __shared__ int4 s_hi[kSplatWarps][32];
+  __shared__ float4 s_cp[32 * kSplatWarps];
+  __shared__ float4 s_cn[32 * kSplatWarps];
+  __shared__ int s_box[6];
+  __shared__ unsigned long long s_cost;
+  __shared__ uint32_t s_woff[kSplatWarps];
+  __shared__ uint32_t s_nlive;
   const uint32_t idx = w.first + threadIdx.x;
   const bool has_n = D.nrm != nullptr;
   const float voxel = D.voxel[m], bw = D.bw[m], reach = D.reach[m], inv_voxel = D.inv_voxel[m], radius = D.radius;
@@ -910,27 +925,134 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     hz = min(f2i(floorf((pz + reach) * inv_voxel)), last);
     if (lx > hx || ly > hy || lz > hz) live = false;
   }
-  const uint32_t active = __ballot_sync(0xffffffffu, live);
-  if (active == 0u) return;
   s_p[wid][lane] = make_float4(px, py, pz, 0.0f);
   s_n[wid][lane] = make_float4(nx, ny, nz, 0.0f);
   s_lo[wid][lane] = make_int4(lx, ly, lz, 0);
   s_hi[wid][lane] = make_int4(hx, hy, hz, 0);
-  // union box and the two cost estimates
+  if (threadIdx.x < 6) s_box[threadIdx.x] = threadIdx.x < 3 ? 0x7fffffff : -1;
+  if (threadIdx.x == 0) s_cost = 0ull;
+  __syncthreads();
+  // warp then block union box, live counts and the sum of the particles' own box sizes
+  const uint32_t active = __ballot_sync(0xffffffffu, live);
   int ulx = __reduce_min_sync(0xffffffffu, live ? lx : 0x7fffffff);
   int uly = __reduce_min_sync(0xffffffffu, live ? ly : 0x7fffffff);
   int ulz = __reduce_min_sync(0xffffffffu, live ? lz : 0x7fffffff);
   int uhx = __reduce_max_sync(0xffffffffu, live ? hx : -1);
   int uhy = __reduce_max_sync(0xffffffffu, live ? hy : -1);
   int uhz = __reduce_max_sync(0xffffffffu, live ? hz : -1);
-  uint32_t own = live ? static_cast<uint32_t>((hx - lx + 1) * (hy - ly + 1) * (hz - lz + 1)) : 0u;
-  uint32_t cost_ind = __reduce_add_sync(0xffffffffu, (own + 31u) >> 5);
+  const uint32_t own = live ? static_cast<uint32_t>((hx - lx + 1) * (hy - ly + 1) * (hz - lz + 1)) : 0u;
+  const uint32_t cost_ind = __reduce_add_sync(0xffffffffu, (own + 31u) >> 5);
+  const uint32_t wsum = __reduce_add_sync(0xffffffffu, own);
+  if (lane == 0) {
+    if (active) {
+      atomicMin(&s_box[0], ulx);
+      atomicMin(&s_box[1], uly);
+      atomicMin(&s_box[2], ulz);
+      atomicMax(&s_box[3], uhx);
+      atomicMax(&s_box[4], uhy);
+      atomicMax(&s_box[5], uhz);
+    }
+    atomicAdd(&s_cost, static_cast<unsigned long long>(wsum));
+    s_woff[wid] = __popc(active);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t o = 0;
+    for (int k = 0; k < kSplatWarps; k++) {
+      uint32_t c = s_woff[k];
+      s_woff[k] = o;
+      o += c;
+    }
+    s_nlive = o;
+  }
+  __syncthreads();
+  if (live) {
+    uint32_t slot = s_woff[wid] + __popc(active & ((1u << lane) - 1u));
+    s_cp[slot] = make_float4(px, py, pz, 0.0f);
+    s_cn[slot] = make_float4(nx, ny, nz, 0.0f);
+  }
+  __syncthreads();
+  const uint32_t nlive = s_nlive;
+  if (nlive == 0) return;
+  uint32_t* __restrict__ keys = D.keys + off;
+  {
+    const int bx0 = s_box[0], by0 = s_box[1], bz0 = s_box[2];
+    const uint64_t bnx = static_cast<uint64_t>(s_box[3] - bx0 + 1), bny = static_cast<uint64_t>(s_box[4] - by0 + 1),
+                   bnz = static_cast<uint64_t>(s_box[5] - bz0 + 1);
+    const uint64_t bnu = bnx * bny * bnz;
+    // pair evaluations of the block walk against those of each particle's own box, weighted by
+    // their relative cost (the block walk's pair is ~3x cheaper for spheres, ~1.5x for discs)
+    const uint64_t lhs = bnu * nlive * (has_n ? 2ull : 1ull);
+    const uint64_t rhs = s_cost * 3ull;
+    if (bnu < (1ull << 30) && lhs <= rhs) {
+      const uint32_t ngx = static_cast<uint32_t>((bnx + 3) >> 2);
+      const uint32_t ngroups = ngx * static_cast<uint32_t>(bny * bnz);
+      const int bhx = s_box[3];
+      for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
+        const uint32_t gx = g % ngx, rest = g / ngx;
+        const int y = by0 + static_cast<int>(rest % static_cast<uint32_t>(bny));
+        const int z = bz0 + static_cast<int>(rest / static_cast<uint32_t>(bny));
+        const int x0 = bx0 + static_cast<int>(gx * 4);
+        float cx[4], b[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          cx[k] = (static_cast<float>(x0 + k) + 0.5f) * voxel;
+          b[k] = __int_as_float(0x7f800000);
+        }
+        const float cy = (static_cast<float>(y) + 0.5f) * voxel;
+        const float cz = (static_cast<float>(z) + 0.5f) * voxel;
+        if (!has_n) {
+#pragma unroll 4
+          for (uint32_t j = 0; j < nlive; j++) {
+            const float4 q = s_cp[j];
+            const float dy = cy - q.y, dz = cz - q.z;
+            const float dy2 = dy * dy, dz2 = dz * dz;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const float dx = cx[k] - q.x;
+              float t = dx * dx;
+              t = t + dy2;
+              t = t + dz2;
+              b[k] = fminf(b[k], t);
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < 4; k++) b[k] = __fsqrt_rn(b[k]) - radius;
+        } else {
+          for (uint32_t j = 0; j < nlive; j++) {
+            const float4 q = s_cp[j];
+            const float4 nn = s_cn[j];
+            const float dy = cy - q.y, dz = cz - q.z;
+            const float dy2 = dy * dy, dz2 = dz * dz;
+            const float dyn = dy * nn.y, dzn = dz * nn.z;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const float dx = cx[k] - q.x;
+              float t = dx * dx;
+              t = t + dy2;
+              t = t + dz2;
+              float pl = dx * nn.x;
+              pl = pl + dyn;
+              pl = pl + dzn;
+              b[k] = fminf(b[k], fmaxf(pl, __fsqrt_rn(t) - radius));
+            }
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+          if (x0 + k <= bhx && b[k] < bw)
+            atomicMin(keys + (static_cast<long long>(x0 + k) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
+                      enc_key(b[k], bw));
+        }
+      }
+      return;
+    }
+  }
+  if (active == 0u) return;
   const uint32_t nux = static_cast<uint32_t>(uhx - ulx + 1), nuy = static_cast<uint32_t>(uhy - uly + 1),
                  nuz = static_cast<uint32_t>(uhz - ulz + 1);
   const uint64_t nu64 = static_cast<uint64_t>(nux) * nuy * nuz;
   const uint32_t nact = __popc(active);
-  __syncwarp();
-  uint32_t* __restrict__ keys = D.keys + off;
   if (nu64 < (1ull << 31) && ((nu64 + 31) >> 5) * nact <= 2ull * cost_ind) {
     const uint32_t nu = static_cast<uint32_t>(nu64);
     const uint32_t nxy = nux * nuy;
