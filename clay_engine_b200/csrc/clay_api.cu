@@ -1362,8 +1362,8 @@ int clay_batch_add_splat(clay_batch* b, clay_splat* s) {
 
 int clay_batch_set_tuning(clay_batch* b, const clay_batch_tuning* t) {
   if (!b || !t) return fail(CLAY_EINVAL, "clay_batch_set_tuning: NULL argument");
-  if (t->sph_block < 64 || t->sph_block > 512 || (t->sph_block & 31))
-    return fail(CLAY_EINVAL, "sph_block %d must be a multiple of 32 in 64..512", t->sph_block);
+  if (t->sph_block < 64 || t->sph_block > 256 || (t->sph_block & 31))
+    return fail(CLAY_EINVAL, "sph_block %d must be a multiple of 32 in 64..256", t->sph_block);
   b->tune = *t;
   b->tune.splat_block = kSplatThreads;
   b->release();

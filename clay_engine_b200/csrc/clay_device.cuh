@@ -18,6 +18,7 @@ constexpr int kMaxLeaves = 8;
 constexpr int kMaxParts = 64;
 constexpr int kMaxMips = 8;
 constexpr int kSplatWarps = 8;  // warps per block of the splat pass
+constexpr int kSplatAccVoxels = 4096;  // shared-memory minimum tile of the splat pass
 
 // FluidParticle (fluid.ts:20-26): (pos, density), (vel, pressure), (nvel, pad).
 struct __align__(16) ParticleDev {
@@ -103,7 +104,7 @@ struct __align__(16) SceneDev {
   uint32_t* sorted_id;
   float4* spos;
   float4* svel;
-  float2* sdp;
+  float4* sdp;  // density, pressure, 1/density (the reference's per-pair `1 / other.density`)
   uint32_t* counts;
   uint32_t* cell_start;
   const FieldDev* world;
@@ -687,7 +688,7 @@ __device__ __forceinline__ void for_neighbours(const SceneDev& S, const BoxInfo&
 
 // density (fluid.ts:333-368). kFast accumulates with Kahan-Neumaier compensation.
 template <bool kFast>
-__global__ void k_density(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+__global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
   if (substep >= S.substeps) return;
@@ -722,14 +723,15 @@ __global__ void k_density(const SceneDev* __restrict__ scenes, const Work* __res
   });
   if (kFast) rho = __fadd_rn(rho, comp);
   const float stiff = S.prm->stiffness;
-  S.sdp[k] = make_float2(fmaxf(rho, S.rest_floor), fmaxf(stiff * (rho - S.rest), 0.0f));
+  const float dens = fmaxf(rho, S.rest_floor);
+  S.sdp[k] = make_float4(dens, fmaxf(stiff * (rho - S.rest), 0.0f), __frcp_rn(dens), 0.0f);
 }
 
 // forces (fluid.ts:370-439) fused with integrate (fluid.ts:449-491). The neighbour pass
 // reads only the cell-ordered copies made by the cell build, and writes only the particle
 // records, so no neighbour can observe a half-updated particle.
 template <bool kFast>
-__global__ void k_forces_integrate(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+__global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
   if (substep >= S.substeps) return;
@@ -741,7 +743,7 @@ __global__ void k_forces_integrate(const SceneDev* __restrict__ scenes, const Wo
   const ParamsDev& P = *S.prm;
   const float4 me = S.spos[k];
   const float4 mv = S.svel[k];
-  const float2 mdp = S.sdp[k];
+  const float4 mdp = S.sdp[k];
   int cx, cy, cz;
   cell_of(S, me.x, me.y, me.z, cx, cy, cz);
   const float h2 = S.h2, h = S.h, mass = S.mass, spiky = S.spiky;
@@ -751,15 +753,15 @@ __global__ void k_forces_integrate(const SceneDev* __restrict__ scenes, const Wo
   float wsum = S.h6;
   const float4* __restrict__ spos = S.spos;
   const float4* __restrict__ svel = S.svel;
-  const float2* __restrict__ sdp = S.sdp;
+  const float4* __restrict__ sdp = S.sdp;
   for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
     if (q == k) return;
     float4 o = __ldg(spos + q);
     float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
     float r2 = (dx * dx + dy * dy) + dz * dz;
     if (r2 >= h2) return;
-    float2 odp = __ldg(sdp + q);
-    float inv = __frcp_rn(odp.x);
+    const float4 odp = __ldg(sdp + q);
+    const float inv = odp.z;
     float w0 = h2 - r2;
     float wv = (w0 * w0) * w0;
     float4 ov = __ldg(svel + q);
@@ -767,17 +769,19 @@ __global__ void k_forces_integrate(const SceneDev* __restrict__ scenes, const Wo
     vsy = vsy + ov.y * wv;
     vsz = vsz + ov.z * wv;
     wsum = wsum + wv;
-    float r = __fsqrt_rn(r2);
+    // fast mode: hardware reciprocal square root; reference mode: IEEE sqrt and 1/r
+    const float irs = kFast ? rsqrtf(r2) : 0.0f;
+    const float r = kFast ? r2 * irs : __fsqrt_rn(r2);
     if (r > 1e-6f) {
       float hr = h - r;
       float s = mass * (mp + odp.y) * 0.5f * inv * spiky * (hr * hr);
-      float ir = __frcp_rn(r);
+      float ir = kFast ? irs : __frcp_rn(r);
       fx = fx - (dx * ir) * s;
       fy = fy - (dy * ir) * s;
       fz = fz - (dz * ir) * s;
     }
   });
-  float id = __frcp_rn(mdp.x);
+  float id = mdp.z;
   float ax = fx * id + P.gravity[0], ay = fy * id + P.gravity[1], az = fz * id + P.gravity[2];
   float t = clampf(P.viscosity, 0.0f, 1.0f);
   float iw = __frcp_rn(wsum);
@@ -1019,6 +1023,11 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
 #pragma unroll
           for (int k = 0; k < 4; k++) b[k] = __fsqrt_rn(b[k]) - radius;
         } else {
+          // b starts at bandWorld: only values below it are ever written. A pair is skipped
+          // when it provably cannot lower b: its plane term is already >= b, or its squared
+          // length is beyond (b + radius)^2 (with a 1e-5 margin over f32 rounding).
+#pragma unroll
+          for (int k = 0; k < 4; k++) b[k] = bw;
           for (uint32_t j = 0; j < nlive; j++) {
             const float4 q = s_cp[j];
             const float4 nn = s_cn[j];
@@ -1028,13 +1037,16 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
 #pragma unroll
             for (int k = 0; k < 4; k++) {
               const float dx = cx[k] - q.x;
-              float t = dx * dx;
-              t = t + dy2;
-              t = t + dz2;
               float pl = dx * nn.x;
               pl = pl + dyn;
               pl = pl + dzn;
-              b[k] = fminf(b[k], fmaxf(pl, __fsqrt_rn(t) - radius));
+              if (pl < b[k]) {
+                float t = dx * dx;
+                t = t + dy2;
+                t = t + dz2;
+                const float thr = b[k] + radius;
+                if (thr > 0.0f && t < thr * thr * 1.00001f) b[k] = fminf(b[k], fmaxf(pl, __fsqrt_rn(t) - radius));
+              }
             }
           }
         }
@@ -1048,74 +1060,114 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       return;
     }
   }
-  if (active == 0u) return;
-  const uint32_t nux = static_cast<uint32_t>(uhx - ulx + 1), nuy = static_cast<uint32_t>(uhy - uly + 1),
-                 nuz = static_cast<uint32_t>(uhz - ulz + 1);
-  const uint64_t nu64 = static_cast<uint64_t>(nux) * nuy * nuz;
-  const uint32_t nact = __popc(active);
-  if (nu64 < (1ull << 31) && ((nu64 + 31) >> 5) * nact <= 2ull * cost_ind) {
-    const uint32_t nu = static_cast<uint32_t>(nu64);
-    const uint32_t nxy = nux * nuy;
-    for (uint32_t v0 = 0; v0 < nu; v0 += 32) {
-      uint32_t v = v0 + lane;
-      uint32_t vv = v < nu ? v : nu - 1;
-      int x = ulx + static_cast<int>(vv % nux);
-      int y = uly + static_cast<int>((vv / nux) % nuy);
-      int z = ulz + static_cast<int>(vv / nxy);
-      float cxf = (static_cast<float>(x) + 0.5f) * voxel;
-      float cyf = (static_cast<float>(y) + 0.5f) * voxel;
-      float czf = (static_cast<float>(z) + 0.5f) * voxel;
-      float best = __int_as_float(0x7f800000);
-      uint32_t rem = active;
-      if (!has_n) {
-        while (rem) {
-          int j = __ffs(rem) - 1;
-          rem &= rem - 1;
-          float4 q = s_p[wid][j];
-          float dx = cxf - q.x, dy = cyf - q.y, dz = czf - q.z;
-          float d2 = (dx * dx + dy * dy) + dz * dz;
-          best = fminf(best, d2);
+  // Warp walks. When the block's union box fits in shared memory the minima are taken there
+  // first (shared-memory atomicMin) and written out with one global atomicMin per touched voxel;
+  // otherwise every hit goes to the key grid directly.
+  __shared__ uint32_t s_acc[kSplatAccVoxels];
+  const int ax0 = s_box[0], ay0 = s_box[1], az0 = s_box[2];
+  const uint32_t anx = static_cast<uint32_t>(s_box[3] - ax0 + 1), any = static_cast<uint32_t>(s_box[4] - ay0 + 1),
+                 anz = static_cast<uint32_t>(s_box[5] - az0 + 1);
+  const uint64_t an = static_cast<uint64_t>(anx) * any * anz;
+  const bool use_acc = an <= static_cast<uint64_t>(kSplatAccVoxels);
+  if (use_acc) {
+    for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) s_acc[v] = 65535u;
+    __syncthreads();
+  }
+  auto emit = [&](int x, int y, int z, uint32_t key) {
+    if (use_acc) {
+      uint32_t a = static_cast<uint32_t>(x - ax0) + anx * (static_cast<uint32_t>(y - ay0) + any * static_cast<uint32_t>(z - az0));
+      atomicMin(&s_acc[a], key);
+    } else {
+      atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)), key);
+    }
+  };
+  const float reach2_hi = (bw + radius) * (bw + radius) * 1.00001f;
+  if (active != 0u) {
+    const uint32_t nux = static_cast<uint32_t>(uhx - ulx + 1), nuy = static_cast<uint32_t>(uhy - uly + 1),
+                   nuz = static_cast<uint32_t>(uhz - ulz + 1);
+    const uint64_t nu64 = static_cast<uint64_t>(nux) * nuy * nuz;
+    const uint32_t nact = __popc(active);
+    if (nu64 < (1ull << 31) && ((nu64 + 31) >> 5) * nact <= 2ull * cost_ind) {
+      const uint32_t nu = static_cast<uint32_t>(nu64);
+      const uint32_t nxy = nux * nuy;
+      for (uint32_t v0 = 0; v0 < nu; v0 += 32) {
+        uint32_t v = v0 + lane;
+        uint32_t vv = v < nu ? v : nu - 1;
+        int x = ulx + static_cast<int>(vv % nux);
+        int y = uly + static_cast<int>((vv / nux) % nuy);
+        int z = ulz + static_cast<int>(vv / nxy);
+        float cxf = (static_cast<float>(x) + 0.5f) * voxel;
+        float cyf = (static_cast<float>(y) + 0.5f) * voxel;
+        float czf = (static_cast<float>(z) + 0.5f) * voxel;
+        float best = __int_as_float(0x7f800000);
+        uint32_t rem = active;
+        if (!has_n) {
+          while (rem) {
+            int j = __ffs(rem) - 1;
+            rem &= rem - 1;
+            float4 q = s_p[wid][j];
+            float dx = cxf - q.x, dy = cyf - q.y, dz = czf - q.z;
+            float d2 = (dx * dx + dy * dy) + dz * dz;
+            best = fminf(best, d2);
+          }
+          best = __fsqrt_rn(best) - radius;
+        } else {
+          best = bw;  // as in the block walk: skip pairs that cannot lower best
+          while (rem) {
+            int j = __ffs(rem) - 1;
+            rem &= rem - 1;
+            float4 q = s_p[wid][j];
+            float4 nn = s_n[wid][j];
+            float dx = cxf - q.x, dy = cyf - q.y, dz = czf - q.z;
+            float pl = dot3(dx, dy, dz, nn.x, nn.y, nn.z);
+            if (pl < best) {
+              float t = (dx * dx + dy * dy) + dz * dz;
+              const float thr = best + radius;
+              if (thr > 0.0f && t < thr * thr * 1.00001f) best = fminf(best, fmaxf(pl, __fsqrt_rn(t) - radius));
+            }
+          }
         }
-        best = __fsqrt_rn(best) - radius;
-      } else {
-        while (rem) {
-          int j = __ffs(rem) - 1;
-          rem &= rem - 1;
-          float4 q = s_p[wid][j];
-          float4 nn = s_n[wid][j];
-          float dx = cxf - q.x, dy = cyf - q.y, dz = czf - q.z;
-          float sd = fmaxf(dot3(dx, dy, dz, nn.x, nn.y, nn.z), __fsqrt_rn((dx * dx + dy * dy) + dz * dz) - radius);
-          best = fminf(best, sd);
-        }
+        if (v < nu && best < bw) emit(x, y, z, enc_key(best, bw));
       }
-      if (v < nu && best < bw) {
-        atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
-                  enc_key(best, bw));
+    } else {
+      uint32_t rem = active;
+      while (rem) {
+        int j = __ffs(rem) - 1;
+        rem &= rem - 1;
+        float4 q = s_p[wid][j];
+        float4 nn = s_n[wid][j];
+        int4 lo = s_lo[wid][j], hi = s_hi[wid][j];
+        uint32_t bxn = static_cast<uint32_t>(hi.x - lo.x + 1), byn = static_cast<uint32_t>(hi.y - lo.y + 1),
+                 bzn = static_cast<uint32_t>(hi.z - lo.z + 1);
+        uint32_t nb = bxn * byn * bzn, nbxy = bxn * byn;
+        for (uint32_t v = lane; v < nb; v += 32) {
+          int x = lo.x + static_cast<int>(v % bxn);
+          int y = lo.y + static_cast<int>((v / bxn) % byn);
+          int z = lo.z + static_cast<int>(v / nbxy);
+          float dx = (static_cast<float>(x) + 0.5f) * voxel - q.x;
+          float dy = (static_cast<float>(y) + 0.5f) * voxel - q.y;
+          float dz = (static_cast<float>(z) + 0.5f) * voxel - q.z;
+          // a voxel whose plane term or squared length already puts it at or beyond the band
+          // cannot pass sd < bandWorld: skip its square root
+          float pl = has_n ? dot3(dx, dy, dz, nn.x, nn.y, nn.z) : -__int_as_float(0x7f800000);
+          if (pl >= bw) continue;
+          float t = (dx * dx + dy * dy) + dz * dz;
+          if (t >= reach2_hi) continue;
+          float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
+          if (sd < bw) emit(x, y, z, enc_key(sd, bw));
+        }
       }
     }
-  } else {
-    uint32_t rem = active;
-    while (rem) {
-      int j = __ffs(rem) - 1;
-      rem &= rem - 1;
-      float4 q = s_p[wid][j];
-      float4 nn = s_n[wid][j];
-      int4 lo = s_lo[wid][j], hi = s_hi[wid][j];
-      uint32_t bxn = static_cast<uint32_t>(hi.x - lo.x + 1), byn = static_cast<uint32_t>(hi.y - lo.y + 1),
-               bzn = static_cast<uint32_t>(hi.z - lo.z + 1);
-      uint32_t nb = bxn * byn * bzn, nbxy = bxn * byn;
-      for (uint32_t v = lane; v < nb; v += 32) {
-        int x = lo.x + static_cast<int>(v % bxn);
-        int y = lo.y + static_cast<int>((v / bxn) % byn);
-        int z = lo.z + static_cast<int>(v / nbxy);
-        float dx = (static_cast<float>(x) + 0.5f) * voxel - q.x;
-        float dy = (static_cast<float>(y) + 0.5f) * voxel - q.y;
-        float dz = (static_cast<float>(z) + 0.5f) * voxel - q.z;
-        float l = __fsqrt_rn((dx * dx + dy * dy) + dz * dz) - radius;
-        float sd = has_n ? fmaxf(dot3(dx, dy, dz, nn.x, nn.y, nn.z), l) : l;
-        if (sd < bw)
-          atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
-                    enc_key(sd, bw));
+  }
+  if (use_acc) {
+    __syncthreads();
+    for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) {
+      uint32_t key = s_acc[v];
+      if (key < 65535u) {
+        int x = ax0 + static_cast<int>(v % anx);
+        int y = ay0 + static_cast<int>((v / anx) % any);
+        int z = az0 + static_cast<int>(v / (anx * any));
+        atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)), key);
       }
     }
   }

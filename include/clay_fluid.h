@@ -407,7 +407,7 @@ void clay_batch_destroy(clay_batch* b);
 int clay_batch_add_splat(clay_batch* b, clay_splat* s);
 /* Tile shapes: threads per block of the particle passes and particles per block. */
 typedef struct clay_batch_tuning {
-  int32_t sph_block;     /* threads per block of the neighbour passes: 64..512 */
+  int32_t sph_block;     /* threads per block of the particle passes: 64..256, multiple of 32 */
   int32_t splat_block;   /* threads per block of the splat pass: 64..512 */
   int32_t use_graph;     /* 1: capture the frame into a CUDA graph */
 } clay_batch_tuning;
