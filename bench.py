@@ -45,6 +45,10 @@ def parse():
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--small", action="store_true", help="a small case for profiling (16 scenes)")
+    ap.add_argument("--serve-window", type=float, default=2.0, help="seconds of Poisson arrivals served")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="requests per second")
+    ap.add_argument("--serve-pool", type=int, default=1024, help="resident scenes of the serving pool")
+    ap.add_argument("--no-serve", action="store_true")
     return ap.parse_args()
 
 
@@ -95,6 +99,66 @@ def build_scenes(root, n_scenes, seed, with_bodies=True):
         sim.upload(p)
         sims.append(sim)
     return sims, bodies, keep
+
+
+def serve_pool(root, n_scenes, seed):
+    """The serving configuration: `n_scenes` resident scenes, particle counts log-uniform over
+    2k-256k, bake volumes 32^3 / 64^3 / 128^3 (seeded choice), a 64^3 collider of 8 brushes each.
+    Returns (factory, estimate)."""
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes, serve
+
+    cfg = scenes.CONFIG5
+    counts = scenes.log_uniform_counts(n_scenes, cfg["n_lo"], cfg["n_hi"], seed)
+    rng = np.random.default_rng(seed + 1)
+    bakes = [int(cfg["bakes"][int(b)]) for b in rng.integers(0, len(cfg["bakes"]), n_scenes)]
+    G = serve.grid_res_for(24.0, 0.22)
+
+    def opts(i):
+        o = dict(scenes.CONFIG3["fluid"])
+        o.update(capacity=int(counts[i]), bakeResolution=bakes[i], bakeMipLevels=max(1, int(math.log2(bakes[i] / 8))))
+        return o
+
+    def factory(i):
+        vol = ce.SdfVolume(root, resolution=64, worldSize=24.0, origin=scenes.WORLD_ORIGIN)
+        vol.build(scenes.random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10), hi=(10, 1.0, 10)))
+        field = ce.volumeField(vol)
+        sim = ce.FluidSim(root, field, opts(i))
+        n = int(counts[i])
+        side = math.ceil(n ** (1 / 3)) * 0.1
+        sim.upload(scenes.lattice_block(n, 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i))
+        return sim, [field, vol]
+
+    def estimate(i):
+        return serve.scene_bytes_estimate(int(counts[i]), bakes[i], max(1, int(math.log2(bakes[i] / 8))), G)
+
+    return factory, estimate, counts
+
+
+def run_serving(root, args, seed, stream):
+    from clay_engine_b200 import scenes, serve
+
+    cfg = scenes.CONFIG5
+    factory, estimate, counts = serve_pool(root, args.serve_pool, seed)
+    srv = serve.Server(root, factory, estimate, args.serve_pool, cfg["budget_bytes"])
+    t0 = time.perf_counter()
+    for i in range(args.serve_pool):
+        if not srv.admit(i):
+            break
+    setup_s = time.perf_counter() - t0
+    # warm the kernels on a few scenes, then reset the statistics
+    srv.serve([(0.0, i, 1) for i in range(min(8, args.serve_pool))], stream)
+    srv.stats = serve.ServeStats()
+    arrivals = serve.poisson_arrivals(args.serve_rate, args.serve_window, args.serve_pool, cfg["k_lo"], cfg["k_hi"],
+                                      seed + 2)
+    srv.serve(arrivals, stream, timeout_s=600)
+    out = srv.stats.summary()
+    out.update(rate_req_s=args.serve_rate, window_s_arrivals=args.serve_window, requests=len(arrivals),
+               resident_scenes=len(srv.resident), resident_gb=srv.used_bytes() / 1e9, setup_s=setup_s,
+               budget_gb=cfg["budget_bytes"] / 1e9, demand_particle_steps_s=float(
+                   args.serve_rate * (cfg["k_lo"] + cfg["k_hi"]) / 2 * np.mean(counts)))
+    srv.close()
+    return out
 
 
 # ---------------------------------------------------------------------------------------
@@ -215,7 +279,7 @@ def sum_over_ranks(ws, x):
 # ---------------------------------------------------------------------------------------
 # CPU baseline: the oracle (the f32 restatement of the reference WGSL) on host cores.
 
-def cpu_sample(n_scenes, seed, max_particles, threads):
+def cpu_sample(n_scenes, seed, max_particles, threads, frames=1):
     """Runs the oracle on a bounded sample of the batched scenes, one frame each, and returns
     (particle-steps/s, particles, seconds, sample description)."""
     from clay_engine_b200 import brushes as _b  # noqa: F401  (brush records for the colliders)
@@ -233,7 +297,7 @@ def cpu_sample(n_scenes, seed, max_particles, threads):
             break
         chosen.append(int(i))
         total += int(counts[i])
-    frames = []
+    sims = []
     for i in chosen:
         vd = oracle.VolumeData(64, 3, scenes.WORLD_ORIGIN, 24.0, 4.0)
         d, m = oracle.build_brushes(vd, scenes.random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10),
@@ -243,13 +307,15 @@ def cpu_sample(n_scenes, seed, max_particles, threads):
         ref = OracleFluid(oracle, [vd], threads=threads, **o)
         side = math.ceil(counts[i] ** (1 / 3)) * 0.1
         ref.upload(scenes.lattice_block(int(counts[i]), 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i))
-        frames.append(ref)
+        sims.append(ref)
     t0 = time.perf_counter()
-    for ref in frames:
-        ref.step()
+    for _ in range(frames):
+        for ref in sims:
+            ref.step()
     dt = time.perf_counter() - t0
-    desc = f"{len(chosen)} of the {n_scenes} batched scenes nearest the median size, {total} particles, 1 frame each"
-    return total / dt, total, dt, desc
+    desc = (f"{len(chosen)} of the {n_scenes} batched scenes nearest the median size, {total} particles, "
+            f"{frames} frame(s) each, f32 oracle with OpenMP")
+    return total * frames / dt, total * frames, dt, desc
 
 
 def reference_arm(args, ws, rank):
@@ -260,7 +326,7 @@ def reference_arm(args, ws, rank):
     threads = os.cpu_count() or 1
     vals = []
     for s in range(args.warmup + args.steps):
-        v, total, dt, desc = cpu_sample(args.scenes, 3, 20000, threads)
+        v, total, dt, desc = cpu_sample(args.scenes, 3, 150_000, threads)
         if s >= args.warmup:
             vals.append((total, dt))
     tot = sum(t for t, _ in vals)
@@ -367,22 +433,8 @@ def main():
     e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
     e2e_value = total_particles * e2e_steps / (e2e_ms / 1000)
 
-    # ---- per-kernel times of one frame (events around each launch) for the roofline
     prof = batch.profile(stream)
     frame_ms = sum(v[0] for v in prof.values())
-    top = max(prof.items(), key=lambda kv: kv[1][0])
-    peak, peak_kind = load_peaks()
-    roof = None
-    if top[0] in BYTES_PER_PARTICLE:
-        per_launch_bytes = BYTES_PER_PARTICLE[top[0]] * particles
-        avg_ms = top[1][0] / top[1][1]
-        achieved = per_launch_bytes / (avg_ms / 1000) / 1e9
-        roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_ms}
-    else:
-        roof = {"bound": "hbm", "kernel": top[0], "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
-                "traffic": None, "peak_source": peak_kind}
 
     # ---- plain path: the same scenes, one scene per launch sequence, no graph
     plain_value = None
@@ -403,9 +455,43 @@ def main():
         plain_value = total_particles * args.plain_steps / (plain_ms / 1000)
 
     clocks.__exit__(None, None, None)
+    # algorithmic bytes of the bake: each (particle, level) reads its 16-byte position once; each
+    # voxel the bake lowers is read and written once in the key grid (8 B)
+    touched = 0
+    for s in sims:
+        d, _ = s.surface.volume.download()
+        touched += int((d != 0x3C00).sum())
+    mips = sims[0].surface.volume.mipLevels if sims else 0
+    n_sims = len(sims)
+    splat_bytes = 16 * particles * mips + 8 * touched
+    # ---- per-kernel times of one frame (events around each launch) for the roofline
+    top = max(prof.items(), key=lambda kv: kv[1][0])
+    peak, peak_kind = load_peaks()
+    roof = None
+    if top[0] in BYTES_PER_PARTICLE or top[0] == "splat":
+        per_launch_bytes = BYTES_PER_PARTICLE[top[0]] * particles if top[0] != "splat" else splat_bytes
+        avg_ms = top[1][0] / top[1][1]
+        achieved = per_launch_bytes / (avg_ms / 1000) / 1e9
+        roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_ms}
+    else:
+        roof = {"bound": "hbm", "kernel": top[0], "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                "traffic": None, "peak_source": peak_kind}
+
+    # ---- serving: free the batched scenes first, then a resident pool under Poisson arrivals
+    batch.destroy()
+    for s in sims:
+        s.destroy()
+    for x in bodies:
+        x.destroy()
+    sims, bodies, keep = [], [], []
+    served = None
+    if not args.no_serve and not args.small:
+        served = run_serving(root, args, seed + 50, stream)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        v, total, dt, desc = cpu_sample(n_scenes, seed, 20000, os.cpu_count() or 1)
+        v, total, dt, desc = cpu_sample(n_scenes, seed, 1_500_000, os.cpu_count() or 1, frames=2)
         cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port", "sample": desc}
 
     if rank == 0:
@@ -420,8 +506,9 @@ def main():
                        "l2": "working set larger than L2 (no flush needed)"},
             "plain": {"value": plain_value, "unit": UNIT, "ratio_batched_over_plain":
                       (value / plain_value) if plain_value else None},
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 80 * len(sims) * ws,
-                    "d2h_bytes_per_step": 528 * len(sims) * ws},
+            "served": served,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 80 * n_sims * ws,
+                    "d2h_bytes_per_step": 528 * n_sims * ws},
             "gpu_launches": int(launches),
             "roofline": roof,
             "kernels_ms_per_frame": {k: round(v[0], 4) for k, v in prof.items()},
@@ -431,9 +518,6 @@ def main():
         }
         print(json.dumps(line), flush=True)
 
-    batch.destroy()
-    for s in sims:
-        s.destroy()
     root.destroy()
     if ws > 1:
         import torch.distributed as dist

@@ -482,6 +482,11 @@ class Batch:
     def step(self, pass_=None):
         check(lib().clay_batch_step(self.handle, stream_handle(pass_)))
 
+    def step_subset(self, scenes, pass_=None):
+        """One frame for the listed scenes only (indices into this batch, each at most once)."""
+        arr = (C.c_int32 * len(scenes))(*[int(i) for i in scenes])
+        check(lib().clay_batch_step_subset(self.handle, arr, len(scenes), stream_handle(pass_)))
+
     def read_contacts_async(self, host_ptr: int, pass_=None):
         """Every scene's ContactList into pinned host memory at `host_ptr` (528 B each)."""
         check(lib().clay_batch_read_contacts_async(self.handle, host_ptr, stream_handle(pass_)))

@@ -1182,13 +1182,26 @@ struct clay_batch {
   bool params_used[2] = {false, false};
   int params_slot = 0;
   ContactsDev* d_contacts = nullptr;
+  // Subset stepping (continuous batching): per-frame work tables built on the host for the
+  // scenes of that frame, double-buffered in pinned memory, one upload per frame.
+  std::vector<ParamsDev> all_params;
+  Work* h_sub[2] = {nullptr, nullptr};
+  size_t h_sub_cap[2] = {0, 0};
+  cudaEvent_t sub_ev[2] = {nullptr, nullptr};
+  bool sub_used[2] = {false, false};
+  int sub_slot = 0;
+  Work* d_sub = nullptr;
+  size_t d_sub_cap = 0;
 
   ~clay_batch() {
     release();
     for (int k = 0; k < 2; k++) {
       if (h_params[k]) cudaFreeHost(h_params[k]);
       if (params_ev[k]) cudaEventDestroy(params_ev[k]);
+      if (h_sub[k]) cudaFreeHost(h_sub[k]);
+      if (sub_ev[k]) cudaEventDestroy(sub_ev[k]);
     }
+    if (d_sub) ctx->dev_free(d_sub, d_sub_cap * sizeof(Work));
   }
   void release() {
     if (graph) {
@@ -1390,6 +1403,7 @@ int clay_batch_step(clay_batch* b, void* stream) {
       clay_fluid* f = b->sims[i];
       clay_fluid_params p = fluid_frame_params(f);
       std::memcpy(&b->h_params[k][i], &p, sizeof(ParamsDev));
+      if (b->all_params.size() == b->sims.size()) std::memcpy(&b->all_params[i], &p, sizeof(ParamsDev));
       if (f->world && (rc = const_cast<clay_field*>(f->world)->flush(s))) return rc;
     }
     if (!b->sims.empty()) {
@@ -1537,7 +1551,130 @@ int clay_batch_read_contacts_async(clay_batch* b, clay_contact_list* host, void*
 }
 
 int clay_batch_step_subset(clay_batch* b, const int32_t* scenes, int n, void* stream) {
-  return fail(CLAY_ESTATE, "clay_batch_step_subset: not available in this build");
+  if (!b || n < 0 || (n > 0 && !scenes)) return fail(CLAY_EINVAL, "clay_batch_step_subset: bad argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc;
+  if (!b->built && (rc = batch_build(b))) return rc;
+  const int ns = static_cast<int>(b->sims.size());
+  if (b->all_params.size() != static_cast<size_t>(ns)) {
+    b->all_params.resize(ns);
+    for (int i = 0; i < ns; i++) std::memcpy(&b->all_params[i], &b->sims[i]->frozen, sizeof(ParamsDev));
+    for (int i = 0; i < ns; i++) b->all_params[i].count = static_cast<uint32_t>(b->sims[i]->live);
+  }
+  std::vector<char> seen(ns, 0);
+  for (int q = 0; q < n; q++) {
+    int i = scenes[q];
+    if (i < 0 || i >= ns) return fail(CLAY_EINVAL, "clay_batch_step_subset: scene %d outside 0..%d", i, ns - 1);
+    if (seen[i]) return fail(CLAY_EINVAL, "clay_batch_step_subset: scene %d listed twice", i);
+    seen[i] = 1;
+  }
+  if (n == 0) return CLAY_OK;
+  // The frame's uniforms (fluid.ts:537-545) for the listed scenes; the others keep theirs.
+  const int T = b->tune.sph_block;
+  int max_sub = 0;
+  for (int q = 0; q < n; q++) {
+    clay_fluid* f = b->sims[scenes[q]];
+    clay_fluid_params p = fluid_frame_params(f);
+    std::memcpy(&b->all_params[scenes[q]], &p, sizeof(ParamsDev));
+    if (f->world && (rc = const_cast<clay_field*>(f->world)->flush(s))) return rc;
+    if ((rc = f->surface->flush(s))) return rc;
+    if (f->live > 0) max_sub = std::max(max_sub, f->substeps);
+  }
+  // Work tables sized by the live counts (known on the host): no idle blocks.
+  std::vector<Work> tab;
+  auto mark = [&]() { return static_cast<int>(tab.size()); };
+  const int o_emit = mark();
+  for (int q = 0; q < n; q++) {
+    const ParamsDev& p = b->all_params[scenes[q]];
+    uint32_t ec = p.emit_count;
+    if (ec == 0) continue;
+    int eb = static_cast<int>(std::min<int64_t>(8, (ec + T - 1) / T));
+    for (int e = 0; e < eb; e++)
+      tab.push_back({static_cast<uint32_t>(scenes[q]), 0u, static_cast<uint32_t>(e * T), static_cast<uint32_t>(eb * T)});
+  }
+  const int n_emit = mark() - o_emit;
+  const int o_part = mark();
+  for (int q = 0; q < n; q++) {
+    clay_fluid* f = b->sims[scenes[q]];
+    for (int64_t x = 0; x < f->live; x += T)
+      tab.push_back({static_cast<uint32_t>(scenes[q]), 0u, static_cast<uint32_t>(x), static_cast<uint32_t>(std::min<int64_t>(T, f->live - x))});
+  }
+  const int n_part = mark() - o_part;
+  const int o_scan = mark();
+  for (int q = 0; q < n; q++) {
+    clay_fluid* f = b->sims[scenes[q]];
+    if (f->live == 0) continue;
+    for (uint32_t p = 0; p < f->parts_scan; p++) tab.push_back({static_cast<uint32_t>(scenes[q]), p, 0u, 0u});
+  }
+  const int n_scan = mark() - o_scan;
+  const int o_splat = mark();
+  for (int q = 0; q < n; q++) {
+    clay_fluid* f = b->sims[scenes[q]];
+    int64_t it = (f->substeps > 0 && f->live > 0) ? f->live : 0;
+    for (int m = 0; m < f->surface->mips; m++)
+      for (int64_t x = 0; x < it; x += kSplatThreads)
+        tab.push_back({static_cast<uint32_t>(scenes[q]), static_cast<uint32_t>(m), static_cast<uint32_t>(x),
+                       static_cast<uint32_t>(std::min<int64_t>(kSplatThreads, it - x))});
+  }
+  const int n_splat = mark() - o_splat;
+  const int o_res = mark();
+  for (int q = 0; q < n; q++) {
+    int64_t quads = (b->sims[scenes[q]]->surface->vol->total + 3) / 4;
+    for (int64_t x = 0; x < quads; x += kResolveThreads)
+      tab.push_back({static_cast<uint32_t>(scenes[q]), 0u, static_cast<uint32_t>(x), kResolveThreads});
+  }
+  const int n_res = mark() - o_res;
+  // upload params + tables through double-buffered pinned memory
+  int k = b->sub_slot;
+  b->sub_slot ^= 1;
+  if (b->sub_used[k]) CK(cudaEventSynchronize(b->sub_ev[k]));
+  if (!b->sub_ev[k]) CK(cudaEventCreateWithFlags(&b->sub_ev[k], cudaEventDisableTiming));
+  const size_t need = tab.size() + (sizeof(ParamsDev) * ns + sizeof(Work) - 1) / sizeof(Work);
+  if (b->h_sub_cap[k] < need) {
+    if (b->h_sub[k]) cudaFreeHost(b->h_sub[k]);
+    b->h_sub_cap[k] = need * 2;
+    CK(cudaMallocHost(&b->h_sub[k], b->h_sub_cap[k] * sizeof(Work)));
+  }
+  if (b->d_sub_cap < tab.size()) {
+    // the previous frame's kernels may still read the old table: order the free behind them
+    if (b->d_sub) {
+      CK(cudaStreamSynchronize(s));
+      b->ctx->dev_free(b->d_sub, b->d_sub_cap * sizeof(Work));
+    }
+    b->d_sub_cap = tab.size() * 2;
+    void* p = nullptr;
+    if ((rc = b->ctx->dev_alloc(&p, b->d_sub_cap * sizeof(Work)))) return rc;
+    b->d_sub = static_cast<Work*>(p);
+  }
+  std::memcpy(b->h_sub[k], tab.data(), tab.size() * sizeof(Work));
+  char* hp = reinterpret_cast<char*>(b->h_sub[k] + tab.size());
+  std::memcpy(hp, b->all_params.data(), sizeof(ParamsDev) * ns);
+  CK(cudaMemcpyAsync(b->d_sub, b->h_sub[k], tab.size() * sizeof(Work), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(b->d_params, hp, sizeof(ParamsDev) * ns, cudaMemcpyHostToDevice, s));
+  CK(cudaEventRecord(b->sub_ev[k], s));
+  b->sub_used[k] = true;
+  const SceneDev* d = b->d_scenes;
+  Work* W = b->d_sub;
+  const bool ref = b->mode == CLAY_MODE_REFERENCE;
+  if (n_emit) CK(L_emit(d, W + o_emit, n_emit, T, s));
+  for (int sub = 0; sub < max_sub && n_part > 0; sub++) {
+    CK(L_cell_key(d, W + o_part, n_part, T, sub, s));
+    CK(L_cell_count(d, W + o_part, n_part, T, sub, s));
+    CK(L_scan_partial(d, W + o_scan, n_scan, sub, s));
+    CK(L_scan_final(d, W + o_scan, n_scan, sub, s));
+    CK(L_cell_scatter(d, W + o_part, n_part, T, sub, s));
+    CK(L_cell_order(d, W + o_part, n_part, T, sub, s));
+    if (ref) {
+      CK(L_density_ref(d, W + o_part, n_part, T, sub, s));
+      CK(L_forces_ref(d, W + o_part, n_part, T, sub, s));
+    } else {
+      CK(L_density_fast(d, W + o_part, n_part, T, sub, s));
+      CK(L_forces_fast(d, W + o_part, n_part, T, sub, s));
+    }
+  }
+  if (n_splat) CK(L_splat(b->d_surf, W + o_splat, n_splat, 1, s));
+  if (n_res) CK(L_resolve(b->d_surf, W + o_res, n_res, s));
+  return CLAY_OK;
 }
 
 }  // extern "C"

@@ -416,7 +416,10 @@ int clay_batch_get_tuning(const clay_batch* b, clay_batch_tuning* t);
 /* One frame for every scene: host bookkeeping of each sim (as clay_fluid_step), then the
  * batched passes (or the captured graph) on `stream`. */
 int clay_batch_step(clay_batch* b, void* stream);
-/* Frame with a subset of the scenes (indices into the batch), used by the server. */
+/* One frame for a subset of the batch's scenes (indices, each at most once): the other
+ * scenes keep their state. Work tables are sized from the listed scenes' live counts and
+ * uploaded with their uniforms in one copy; no graph. The batch's extra clouds are not baked.
+ * This is the launch of the continuous-batching server. */
 int clay_batch_step_subset(clay_batch* b, const int32_t* scenes, int n, void* stream);
 /* The ContactList of every scene, in batch order, copied into `host_out` (n records)
  * asynchronously: one gather launch and one device-to-host copy. */
