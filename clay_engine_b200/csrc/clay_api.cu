@@ -499,7 +499,7 @@ int splat_bake(clay_splat* s, cudaStream_t st, bool ordered, int64_t iter_n) {
   int64_t n = iter_n;
   if (n > 0) {
     int blocks = static_cast<int>((n + kSplatThreads - 1) / kSplatThreads);
-    CK(L_splat(d, nullptr, blocks, s->mips, st));
+    CK(L_splat(d, nullptr, blocks, s->mips, s->cloud.normals ? kSplatAccVoxelsDiscs : kSplatAccVoxels, st));
   }
   int64_t quads = (s->vol->total + 3) / 4;
   int rblocks = static_cast<int>((quads + kResolveThreads - 1) / kResolveThreads);
@@ -1312,7 +1312,7 @@ int batch_build(clay_batch* b) {
 int batch_enqueue(clay_batch* b, cudaStream_t s) {
   const int T = b->tune.sph_block;
   const SceneDev* d = b->d_scenes;
-  if (b->n_xsplat) CK(L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, s));
+  if (b->n_xsplat) CK(L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, kSplatAccVoxelsDiscs, s));
   if (b->n_xres) CK(L_resolve(b->d_extra, b->w_xres, b->n_xres, s));
   if (b->n_part) {
     CK(L_emit(d, b->w_emit, b->n_emit, T, s));
@@ -1332,7 +1332,7 @@ int batch_enqueue(clay_batch* b, cudaStream_t s) {
       }
     }
   }
-  if (b->n_ssplat) CK(L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, s));
+  if (b->n_ssplat) CK(L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, kSplatAccVoxels, s));
   if (b->n_sres) CK(L_resolve(b->d_surf, b->w_sres, b->n_sres, s));
   return CLAY_OK;
 }
@@ -1488,7 +1488,7 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
   const int T = b->tune.sph_block;
   const SceneDev* d = b->d_scenes;
   const bool ref = b->mode == CLAY_MODE_REFERENCE;
-  if (b->n_xsplat && (rc = timed("body_splat", [&] { return L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, s); }))) return rc;
+  if (b->n_xsplat && (rc = timed("body_splat", [&] { return L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, kSplatAccVoxelsDiscs, s); }))) return rc;
   if (b->n_xres && (rc = timed("body_resolve", [&] { return L_resolve(b->d_extra, b->w_xres, b->n_xres, s); }))) return rc;
   if (b->n_part) {
     if ((rc = timed("emit", [&] { return L_emit(d, b->w_emit, b->n_emit, T, s); }))) return rc;
@@ -1509,7 +1509,7 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
         return rc;
     }
   }
-  if (b->n_ssplat && (rc = timed("splat", [&] { return L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, s); }))) return rc;
+  if (b->n_ssplat && (rc = timed("splat", [&] { return L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, kSplatAccVoxels, s); }))) return rc;
   if (b->n_sres && (rc = timed("resolve", [&] { return L_resolve(b->d_surf, b->w_sres, b->n_sres, s); }))) return rc;
   CK(cudaStreamSynchronize(s));
   std::vector<clay_phase_time> agg;
@@ -1672,7 +1672,7 @@ int clay_batch_step_subset(clay_batch* b, const int32_t* scenes, int n, void* st
       CK(L_forces_fast(d, W + o_part, n_part, T, sub, s));
     }
   }
-  if (n_splat) CK(L_splat(b->d_surf, W + o_splat, n_splat, 1, s));
+  if (n_splat) CK(L_splat(b->d_surf, W + o_splat, n_splat, 1, kSplatAccVoxels, s));
   if (n_res) CK(L_resolve(b->d_surf, W + o_res, n_res, s));
   return CLAY_OK;
 }

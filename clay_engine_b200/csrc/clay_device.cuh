@@ -18,7 +18,8 @@ constexpr int kMaxLeaves = 8;
 constexpr int kMaxParts = 64;
 constexpr int kMaxMips = 8;
 constexpr int kSplatWarps = 8;  // warps per block of the splat pass
-constexpr int kSplatAccVoxels = 4096;  // shared-memory minimum tile of the splat pass
+constexpr int kSplatAccVoxels = 4096;   // shared-memory minimum tile of the splat pass (spheres)
+constexpr int kSplatAccVoxelsDiscs = 4096;  // the same for oriented-disc clouds
 
 // FluidParticle (fluid.ts:20-26): (pos, density), (vel, pressure), (nvel, pad).
 struct __align__(16) ParticleDev {
@@ -866,6 +867,39 @@ __device__ __forceinline__ bool cloud_live(const SplatDev& D, uint32_t idx, uint
   return true;
 }
 
+
+// Walks a bx*by*bz box in x-fastest order with one voxel per lane, 32 at a time, keeping the
+// lane's (x, y, z) incrementally: the integer divisions happen once per box, not per voxel.
+struct BoxWalk {
+  int x, y, z;       // current voxel (relative to the box corner)
+  int sx, sy, sz;    // the step of 32 voxels decomposed in the box
+  int bx, by;
+  __device__ __forceinline__ void init(uint32_t lane, uint32_t bxn, uint32_t byn) {
+    bx = static_cast<int>(bxn);
+    by = static_cast<int>(byn);
+    const uint32_t bxy = bxn * byn;
+    x = static_cast<int>(lane % bxn);
+    y = static_cast<int>((lane / bxn) % byn);
+    z = static_cast<int>(lane / bxy);
+    sx = static_cast<int>(32u % bxn);
+    sy = static_cast<int>((32u / bxn) % byn);
+    sz = static_cast<int>(32u / bxy);
+  }
+  __device__ __forceinline__ void next() {
+    x += sx;
+    y += sy;
+    z += sz;
+    if (x >= bx) {
+      x -= bx;
+      y++;
+    }
+    if (y >= by) {
+      y -= by;
+      z++;
+    }
+  }
+};
+
 // One block of the splat pass: level w.sub, cloud indices [w.first, w.first + w.n). The
 // volume origin (ox, oy, oz) is the f32 uniform of the baked volume.
 //
@@ -877,7 +911,8 @@ __device__ __forceinline__ bool cloud_live(const SplatDev& D, uint32_t idx, uint
 //    reference's rounding order (dx*dx + dy*dy) + dz*dz.
 //  - warp walk: otherwise each warp works on its 32 particles, walking their union box with a
 //    voxel per lane when that is compact, or each particle's own box.
-__device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, float ox, float oy, float oz) {
+__device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, float ox, float oy, float oz,
+                                            uint32_t acc_cap) {
   const int m = static_cast<int>(w.sub);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   __shared__ float4 s_p[kSplatWarps][32];
@@ -887,6 +922,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   __shared__ float4 s_cp[32 * kSplatWarps];
   __shared__ float4 s_cn[32 * kSplatWarps];
   __shared__ int s_box[6];
+  __shared__ float s_pb[6];  // bounding box of the block's live particle positions
   __shared__ unsigned long long s_cost;
   __shared__ uint32_t s_woff[kSplatWarps];
   __shared__ uint32_t s_nlive;
@@ -934,6 +970,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   s_lo[wid][lane] = make_int4(lx, ly, lz, 0);
   s_hi[wid][lane] = make_int4(hx, hy, hz, 0);
   if (threadIdx.x < 6) s_box[threadIdx.x] = threadIdx.x < 3 ? 0x7fffffff : -1;
+  if (threadIdx.x < 6) reinterpret_cast<int*>(s_pb)[threadIdx.x] = threadIdx.x < 3 ? 0x7fffffff : (-0x7fffffff - 1);
   if (threadIdx.x == 0) s_cost = 0ull;
   __syncthreads();
   // warp then block union box, live counts and the sum of the particles' own box sizes
@@ -947,6 +984,32 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   const uint32_t own = live ? static_cast<uint32_t>((hx - lx + 1) * (hy - ly + 1) * (hz - lz + 1)) : 0u;
   const uint32_t cost_ind = __reduce_add_sync(0xffffffffu, (own + 31u) >> 5);
   const uint32_t wsum = __reduce_add_sync(0xffffffffu, own);
+  {
+    // particle bounding box: warp reduction, then one float min/max per warp in shared memory
+    float a0 = live ? px : __int_as_float(0x7f800000), a1 = live ? py : __int_as_float(0x7f800000),
+          a2 = live ? pz : __int_as_float(0x7f800000);
+    float b0 = live ? px : -__int_as_float(0x7f800000), b1 = live ? py : -__int_as_float(0x7f800000),
+          b2 = live ? pz : -__int_as_float(0x7f800000);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a0 = fminf(a0, __shfl_xor_sync(0xffffffffu, a0, o));
+      a1 = fminf(a1, __shfl_xor_sync(0xffffffffu, a1, o));
+      a2 = fminf(a2, __shfl_xor_sync(0xffffffffu, a2, o));
+      b0 = fmaxf(b0, __shfl_xor_sync(0xffffffffu, b0, o));
+      b1 = fmaxf(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+      b2 = fmaxf(b2, __shfl_xor_sync(0xffffffffu, b2, o));
+    }
+    if (lane == 0 && active) {
+      // positions are finite for live particles; order-preserving integer min/max of floats
+      auto okey = [](float f) { int i = __float_as_int(f); return i >= 0 ? i : i ^ 0x7fffffff; };
+      atomicMin(reinterpret_cast<int*>(&s_pb[0]), okey(a0));
+      atomicMin(reinterpret_cast<int*>(&s_pb[1]), okey(a1));
+      atomicMin(reinterpret_cast<int*>(&s_pb[2]), okey(a2));
+      atomicMax(reinterpret_cast<int*>(&s_pb[3]), okey(b0));
+      atomicMax(reinterpret_cast<int*>(&s_pb[4]), okey(b1));
+      atomicMax(reinterpret_cast<int*>(&s_pb[5]), okey(b2));
+    }
+  }
   if (lane == 0) {
     if (active) {
       atomicMin(&s_box[0], ulx);
@@ -992,11 +1055,27 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       const uint32_t ngx = static_cast<uint32_t>((bnx + 3) >> 2);
       const uint32_t ngroups = ngx * static_cast<uint32_t>(bny * bnz);
       const int bhx = s_box[3];
+      auto ofloat = [](int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff); };
+      const int* pbk = reinterpret_cast<const int*>(s_pb);
+      const float pbx0 = ofloat(pbk[0]), pby0 = ofloat(pbk[1]), pbz0 = ofloat(pbk[2]);
+      const float pbx1 = ofloat(pbk[3]), pby1 = ofloat(pbk[4]), pbz1 = ofloat(pbk[5]);
+      // A group of voxels farther than the reach from the particles' bounding box cannot be
+      // lowered by any of them (sd >= bandWorld): skipped. The 1e-4 margin covers f32 rounding.
+      const float cull = reach * 1.0001f + 1e-5f;
+      const float cull2 = cull * cull;
       for (uint32_t g = threadIdx.x; g < ngroups; g += blockDim.x) {
         const uint32_t gx = g % ngx, rest = g / ngx;
         const int y = by0 + static_cast<int>(rest % static_cast<uint32_t>(bny));
         const int z = bz0 + static_cast<int>(rest / static_cast<uint32_t>(bny));
         const int x0 = bx0 + static_cast<int>(gx * 4);
+        {
+          const float gx0 = (static_cast<float>(x0) + 0.5f) * voxel, gx1 = (static_cast<float>(x0 + 3) + 0.5f) * voxel;
+          const float gy = (static_cast<float>(y) + 0.5f) * voxel, gz = (static_cast<float>(z) + 0.5f) * voxel;
+          const float ex = fmaxf(fmaxf(pbx0 - gx1, gx0 - pbx1), 0.0f);
+          const float ey = fmaxf(fmaxf(pby0 - gy, gy - pby1), 0.0f);
+          const float ez = fmaxf(fmaxf(pbz0 - gz, gz - pbz1), 0.0f);
+          if (ex * ex + ey * ey + ez * ez > cull2) continue;
+        }
         float cx[4], b[4];
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -1063,12 +1142,12 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   // Warp walks. When the block's union box fits in shared memory the minima are taken there
   // first (shared-memory atomicMin) and written out with one global atomicMin per touched voxel;
   // otherwise every hit goes to the key grid directly.
-  __shared__ uint32_t s_acc[kSplatAccVoxels];
+  extern __shared__ uint32_t s_acc[];  // acc_cap voxels of dynamic shared memory
   const int ax0 = s_box[0], ay0 = s_box[1], az0 = s_box[2];
   const uint32_t anx = static_cast<uint32_t>(s_box[3] - ax0 + 1), any = static_cast<uint32_t>(s_box[4] - ay0 + 1),
                  anz = static_cast<uint32_t>(s_box[5] - az0 + 1);
   const uint64_t an = static_cast<uint64_t>(anx) * any * anz;
-  const bool use_acc = an <= static_cast<uint64_t>(kSplatAccVoxels);
+  const bool use_acc = an <= static_cast<uint64_t>(acc_cap);
   if (use_acc) {
     for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) s_acc[v] = 65535u;
     __syncthreads();
@@ -1089,13 +1168,13 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     const uint32_t nact = __popc(active);
     if (nu64 < (1ull << 31) && ((nu64 + 31) >> 5) * nact <= 2ull * cost_ind) {
       const uint32_t nu = static_cast<uint32_t>(nu64);
-      const uint32_t nxy = nux * nuy;
-      for (uint32_t v0 = 0; v0 < nu; v0 += 32) {
+      BoxWalk bw_;
+      bw_.init(lane, nux, nuy);
+      for (uint32_t v0 = 0; v0 < nu; v0 += 32, bw_.next()) {
         uint32_t v = v0 + lane;
-        uint32_t vv = v < nu ? v : nu - 1;
-        int x = ulx + static_cast<int>(vv % nux);
-        int y = uly + static_cast<int>((vv / nux) % nuy);
-        int z = ulz + static_cast<int>(vv / nxy);
+        int x = ulx + bw_.x;
+        int y = uly + bw_.y;
+        int z = ulz + (v < nu ? bw_.z : 0);
         float cxf = (static_cast<float>(x) + 0.5f) * voxel;
         float cyf = (static_cast<float>(y) + 0.5f) * voxel;
         float czf = (static_cast<float>(z) + 0.5f) * voxel;
@@ -1139,11 +1218,13 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
         int4 lo = s_lo[wid][j], hi = s_hi[wid][j];
         uint32_t bxn = static_cast<uint32_t>(hi.x - lo.x + 1), byn = static_cast<uint32_t>(hi.y - lo.y + 1),
                  bzn = static_cast<uint32_t>(hi.z - lo.z + 1);
-        uint32_t nb = bxn * byn * bzn, nbxy = bxn * byn;
-        for (uint32_t v = lane; v < nb; v += 32) {
-          int x = lo.x + static_cast<int>(v % bxn);
-          int y = lo.y + static_cast<int>((v / bxn) % byn);
-          int z = lo.z + static_cast<int>(v / nbxy);
+        uint32_t nb = bxn * byn * bzn;
+        BoxWalk bw_;
+        bw_.init(lane, bxn, byn);
+        for (uint32_t v = lane; v < nb; v += 32, bw_.next()) {
+          int x = lo.x + bw_.x;
+          int y = lo.y + bw_.y;
+          int z = lo.z + bw_.z;
           float dx = (static_cast<float>(x) + 0.5f) * voxel - q.x;
           float dy = (static_cast<float>(y) + 0.5f) * voxel - q.y;
           float dz = (static_cast<float>(z) + 0.5f) * voxel - q.z;
@@ -1202,10 +1283,11 @@ __device__ __forceinline__ void resolve_block(const SplatDev& D, const Work w) {
 }
 
 #ifndef CLAY_ONLY_NEIGHBOUR_PASSES
-__global__ void __launch_bounds__(32 * kSplatWarps) k_splat(const SplatDev* __restrict__ splats, const Work* __restrict__ work) {
+__global__ void __launch_bounds__(32 * kSplatWarps) k_splat(const SplatDev* __restrict__ splats, const Work* __restrict__ work,
+                                                             uint32_t acc_cap) {
   const Work w = get_work(work);
   const SplatDev& D = splats[w.obj];
-  splat_block(D, w, D.vp->origin[0], D.vp->origin[1], D.vp->origin[2]);
+  splat_block(D, w, D.vp->origin[0], D.vp->origin[1], D.vp->origin[2], acc_cap);
 }
 
 __global__ void k_resolve(const SplatDev* __restrict__ splats, const Work* __restrict__ work) {

@@ -50,9 +50,18 @@ cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int thre
 cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
   CLAY_LAUNCH(k_forces_integrate<false>, blocks, threads, st, s, w, sub);
 }
-cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, cudaStream_t st) {
+cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, uint32_t acc_voxels, cudaStream_t st) {
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_splat, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kSplatAccVoxelsDiscs * static_cast<int>(sizeof(uint32_t)));
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
   dim3 g(blocks, w ? 1 : blocks_y);
-  CLAY_LAUNCH(k_splat, g, kSplatThreads, st, d, w);
+  k_splat<<<g, kSplatThreads, acc_voxels * sizeof(uint32_t), st>>>(d, w, acc_voxels);
+  count_launch();
+  return cudaPeekAtLastError();
 }
 cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t st) {
   CLAY_LAUNCH(k_resolve, blocks, kResolveThreads, st, d, w);

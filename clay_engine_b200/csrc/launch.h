@@ -34,7 +34,8 @@ cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threa
 cudaError_t L_density_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
 cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
 // `blocks_y` = mip levels when w == nullptr.
-cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, cudaStream_t st);
+// acc_voxels: size of the shared-memory minimum tile (dynamic shared memory, 4 B per voxel).
+cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, uint32_t acc_voxels, cudaStream_t st);
 cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t st);
 cudaError_t L_build(const BuildLevelDev& lv, const BrushDev* brushes, int n, cudaStream_t st);
 cudaError_t L_cell_index(const SceneDev* s, uint32_t* out, int n, cudaStream_t st);

@@ -50,7 +50,7 @@ __global__ void __launch_bounds__(32 * kSplatWarps) k_static_splat(const __grid_
   w.sub = blockIdx.y;
   w.first = blockIdx.x * blockDim.x;
   w.n = blockDim.x;
-  splat_block(D, w, ox, oy, oz);
+  splat_block(D, w, ox, oy, oz, kSplatAccVoxels);
 }
 
 __global__ void k_static_resolve(const __grid_constant__ SplatDev D) {
@@ -168,7 +168,7 @@ extern "C" int clay_splat_bake_static(const clay_cloud_desc* cloud, const clay_s
   count_launch();
   if (cloud->capacity > 0) {
     dim3 g((cloud->capacity + kSplatThreads - 1) / kSplatThreads, mips);
-    k_static_splat<<<g, kSplatThreads, 0, s>>>(h, static_cast<float>(origin[0]), static_cast<float>(origin[1]),
+    k_static_splat<<<g, kSplatThreads, kSplatAccVoxels * sizeof(uint32_t), s>>>(h, static_cast<float>(origin[0]), static_cast<float>(origin[1]),
                                                static_cast<float>(origin[2]));
     count_launch();
   }
