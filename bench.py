@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="requests per second")
     ap.add_argument("--serve-pool", type=int, default=1024, help="resident scenes of the serving pool")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--workload", default="batched", choices=["batched", "tap"],
+                    help="batched: the 256-scene batch (+plain, served); tap: one 262,144-particle scene fed by a tap")
     return ap.parse_args()
 
 
@@ -229,54 +231,6 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------
-# Distributed plumbing
-
-def dist_init(args):
-    ws = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if ws > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    return ws, rank, local
-
-
-def barrier(ws):
-    if ws > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-
-
-def max_over_ranks(ws, x):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def sum_over_ranks(ws, x):
-    if ws == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
-
-
-# ---------------------------------------------------------------------------------------
 # CPU baseline: the oracle (the f32 restatement of the reference WGSL) on host cores.
 
 def cpu_sample(n_scenes, seed, max_particles, threads, frames=1):
@@ -316,6 +270,50 @@ def cpu_sample(n_scenes, seed, max_particles, threads, frames=1):
     desc = (f"{len(chosen)} of the {n_scenes} batched scenes nearest the median size, {total} particles, "
             f"{frames} frame(s) each, f32 oracle with OpenMP")
     return total * frames / dt, total * frames, dt, desc
+
+
+def run_tap(root, args, stream, seed):
+    """The plain method at scale: one scene of capacity 262,144 over a 192^3 collider of 64
+    seeded brushes, baked into 128^3 x 4 (band 4), fed each frame by spawn(4096) at a tap with
+    a downward speed ~ N(2, 0.3) (one speed per spawn, as the reference emits one velocity per
+    spawn). Every frame is one FluidSim.step on one stream (no graph)."""
+    import torch
+
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    cfg = scenes.CONFIG2
+    vol = ce.SdfVolume(root, resolution=cfg["collider"]["resolution"], worldSize=24.0, origin=scenes.WORLD_ORIGIN)
+    vol.build(scenes.random_brushes(64, seed=seed))
+    world = ce.volumeField(vol)
+    sim = ce.FluidSim(root, world, cfg["fluid"])
+    rng = np.random.default_rng(seed)
+    tap = cfg["tap"]
+    live_sum = 0
+
+    def frame():
+        sim.spawn(tap["n"], tap["pos"], (0.0, -float(rng.normal(*tap["speed"])), 0.0))
+        sim.step(stream)
+        return sim.particleCount
+
+    for _ in range(args.warmup):
+        frame()
+    stream.synchronize()
+    a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    l0 = ce.kernel_launch_count()
+    for _ in range(args.steps):
+        live_sum += frame()
+    z.record(stream)
+    z.synchronize()
+    ms = a.elapsed_time(z)
+    launches = ce.kernel_launch_count() - l0
+    out = {"value": live_sum / (ms / 1000), "ms_per_step": ms / args.steps, "gpu_launches": launches,
+           "live_at_end": sim.particleCount}
+    sim.destroy()
+    world.destroy()
+    vol.destroy()
+    return out
 
 
 def reference_arm(args, ws, rank):
@@ -367,13 +365,12 @@ BYTES_PER_PARTICLE = {
 
 def main():
     args = parse()
-    ws, rank, local = dist_init(args)
+    from clay_engine_b200 import dist as D
+
+    ws, rank, local = D.init("nccl")
     if args.impl == "reference":
         reference_arm(args, ws, rank)
-        if ws > 1:
-            import torch.distributed as dist
-
-            dist.destroy_process_group()
+        D.finalize()
         return
 
     import torch
@@ -382,12 +379,37 @@ def main():
 
     torch.cuda.set_device(local)
     root = ce.init(local)
+    if args.workload == "tap":
+        stream = torch.cuda.Stream()
+        with ClockSampler(local) as clocks:
+            clocks.mark()
+            r = run_tap(root, args, stream, D.rank_seed(11, rank))
+            clocks.stop()
+        value = D.reduce_sum(r["value"])
+        if rank == 0:
+            print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                              "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+                              "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                              "config": {"workload": "plain-scale-262144-tap", "collider": "192^3 from 64 brushes",
+                                         "bake": "128^3 x 4 mips band 4", "tap": "spawn(4096)/frame, speed N(2,0.3)",
+                                         "live_at_end": r["live_at_end"]},
+                              "gpu_launches": r["gpu_launches"], "clocks": clocks.summary()}), flush=True)
+        root.destroy()
+        D.finalize()
+        return
     n_scenes = 16 if args.small else args.scenes
-    seed = 3 + rank
+    seed = D.rank_seed(3, rank)
     sims, bodies, keep = build_scenes(root, n_scenes, seed)
     particles = sum(s.particleCount for s in sims)
-    batch = ce.Batch(root, sims, extra_splats=bodies, use_graph=True)
     stream = torch.cuda.Stream()
+    # autotune (untimed): block size of the particle passes per scene-size bucket
+    from clay_engine_b200 import autotune
+
+    t_tune = time.perf_counter()
+    tuned, tune_report = autotune.tune(root, sims, bodies, stream, frames=3, use_cache=False)
+    t_tune = time.perf_counter() - t_tune
+    batch = ce.Batch(root, sims, extra_splats=bodies, use_graph=True, sph_block=tuned["default"])
+    autotune.apply(batch, tuned)
     torch.cuda.synchronize()
     clocks = ClockSampler(local).__enter__()
 
@@ -399,7 +421,7 @@ def main():
     # ---- device-resident throughput: K batched frames, CUDA events on the launching stream
     l0 = ce.kernel_launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier(ws)
+    D.barrier()
     torch.cuda.synchronize()
     clocks.mark()
     ev0.record(stream)
@@ -409,16 +431,16 @@ def main():
     ev1.synchronize()
     clocks.stop()
     torch.cuda.synchronize()
-    barrier(ws)
+    D.barrier()
     launches = ce.kernel_launch_count() - l0
-    ms = max_over_ranks(ws, ev0.elapsed_time(ev1))
-    total_particles = sum_over_ranks(ws, particles)
+    ms = D.reduce_max(ev0.elapsed_time(ev1))
+    total_particles = D.reduce_sum(particles)
     value = total_particles * args.steps / (ms / 1000)
 
     # ---- end to end through the public API: per frame the inputs (every scene's FluidParams)
     # go up from pinned memory and every scene's ContactList comes back to pinned memory.
     h_contacts = torch.empty(len(sims) * 528, dtype=torch.uint8, pin_memory=True)
-    barrier(ws)
+    D.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e2e_steps = max(2, args.steps // 2)
@@ -429,8 +451,8 @@ def main():
         stream.synchronize()
     e1.record(stream)
     e1.synchronize()
-    barrier(ws)
-    e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
+    D.barrier()
+    e2e_ms = D.reduce_max(e0.elapsed_time(e1))
     e2e_value = total_particles * e2e_steps / (e2e_ms / 1000)
 
     prof = batch.profile(stream)
@@ -451,7 +473,7 @@ def main():
                 s.step(stream)
         p1.record(stream)
         p1.synchronize()
-        plain_ms = max_over_ranks(ws, p0.elapsed_time(p1))
+        plain_ms = D.reduce_max(p0.elapsed_time(p1))
         plain_value = total_particles * args.plain_steps / (plain_ms / 1000)
 
     clocks.__exit__(None, None, None)
@@ -507,6 +529,9 @@ def main():
             "plain": {"value": plain_value, "unit": UNIT, "ratio_batched_over_plain":
                       (value / plain_value) if plain_value else None},
             "served": served,
+            "autotune": {"buckets_capacity_below": tuned["uppers"], "blocks": tuned["blocks"],
+                         "default_block": tuned["default"], "seconds": t_tune,
+                         "trials": len(tune_report.get("trials", []))},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 80 * n_sims * ws,
                     "d2h_bytes_per_step": 528 * n_sims * ws},
             "gpu_launches": int(launches),
@@ -519,10 +544,7 @@ def main():
         print(json.dumps(line), flush=True)
 
     root.destroy()
-    if ws > 1:
-        import torch.distributed as dist
-
-        dist.destroy_process_group()
+    D.finalize()
 
 
 if __name__ == "__main__":

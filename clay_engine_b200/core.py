@@ -479,6 +479,12 @@ class Batch:
         t = N.BatchTuning(int(sph_block), 256, 1 if use_graph else 0)
         check(lib().clay_batch_set_tuning(self.handle, C.byref(t)))
 
+    def set_bucket_blocks(self, uppers, blocks):
+        """Thread-block size of the particle passes per scene-size bucket (capacity < upper)."""
+        u = (C.c_int64 * len(uppers))(*[int(x) for x in uppers])
+        b = (C.c_int32 * len(blocks))(*[int(x) for x in blocks])
+        check(lib().clay_batch_set_bucket_blocks(self.handle, u, b, len(uppers)))
+
     def step(self, pass_=None):
         check(lib().clay_batch_step(self.handle, stream_handle(pass_)))
 

@@ -1173,6 +1173,22 @@ struct clay_batch {
   std::vector<DevBuf> bufs;
   bool built = false;
   cudaGraphExec_t graph = nullptr;
+  // Per scene-size bucket thread-block size of the particle passes: a scene whose capacity is
+  // below bucket_upper[i] uses bucket_block[i]; others use tune.sph_block. One launch per
+  // distinct block size per pass.
+  std::vector<int64_t> bucket_upper;
+  std::vector<int> bucket_block;
+  struct PartGroup {
+    Work* w;
+    int n;
+    int T;
+  };
+  std::vector<PartGroup> groups;
+  int block_of(int64_t capacity) const {
+    for (size_t i = 0; i < bucket_upper.size(); i++)
+      if (capacity < bucket_upper[i]) return bucket_block[i];
+    return tune.sph_block;
+  }
   int64_t launches_per_step = 0;
   // The scenes' FluidParams, contiguous, written from pinned memory in one copy per frame
   // (double-buffered so the host never overwrites a copy still in flight).
@@ -1249,13 +1265,24 @@ int batch_build(clay_batch* b) {
   std::vector<SceneDev> scenes;
   std::vector<Work> wp, we, wsc;
   b->max_substeps = 0;
+  std::vector<int> blocks;
+  std::vector<std::vector<Work>> by_block;
   for (size_t i = 0; i < b->sims.size(); i++) {
     clay_fluid* f = b->sims[i];
     scenes.push_back(f->hs);
     b->max_substeps = std::max(b->max_substeps, f->substeps);
     uint32_t obj = static_cast<uint32_t>(i);
-    for (int64_t x = 0; x < f->capacity; x += T)
-      wp.push_back({obj, 0u, static_cast<uint32_t>(x), static_cast<uint32_t>(std::min<int64_t>(T, f->capacity - x))});
+    const int Ts = b->block_of(f->capacity);
+    size_t gi = std::find(blocks.begin(), blocks.end(), Ts) - blocks.begin();
+    if (gi == blocks.size()) {
+      blocks.push_back(Ts);
+      by_block.emplace_back();
+    }
+    for (int64_t x = 0; x < f->capacity; x += Ts) {
+      Work wk{obj, 0u, static_cast<uint32_t>(x), static_cast<uint32_t>(std::min<int64_t>(Ts, f->capacity - x))};
+      wp.push_back(wk);
+      by_block[gi].push_back(wk);
+    }
     int eb = static_cast<int>(std::min<int64_t>(8, (f->capacity + T - 1) / T));
     for (int e = 0; e < eb; e++) we.push_back({obj, 0u, static_cast<uint32_t>(e * T), static_cast<uint32_t>(eb * T)});
     for (uint32_t p = 0; p < f->parts_scan; p++) wsc.push_back({obj, p, 0u, 0u});
@@ -1297,6 +1324,12 @@ int batch_build(clay_batch* b) {
       (rc = b->upload_table(&b->w_ssplat, wss)) || (rc = b->upload_table(&b->w_sres, wsr)))
     return rc;
   b->n_part = static_cast<int>(wp.size());
+  b->groups.clear();
+  for (size_t g = 0; g < blocks.size(); g++) {
+    Work* w = nullptr;
+    if ((rc = b->upload_table(&w, by_block[g]))) return rc;
+    b->groups.push_back({w, static_cast<int>(by_block[g].size()), blocks[g]});
+  }
   b->n_emit = static_cast<int>(we.size());
   b->n_scan = static_cast<int>(wsc.size());
   b->n_xsplat = static_cast<int>(wxs.size());
@@ -1317,18 +1350,19 @@ int batch_enqueue(clay_batch* b, cudaStream_t s) {
   if (b->n_part) {
     CK(L_emit(d, b->w_emit, b->n_emit, T, s));
     for (int sub = 0; sub < b->max_substeps; sub++) {
-      CK(L_cell_key(d, b->w_part, b->n_part, T, sub, s));
-      CK(L_cell_count(d, b->w_part, b->n_part, T, sub, s));
+      for (auto& g : b->groups) CK(L_cell_key(d, g.w, g.n, g.T, sub, s));
+      for (auto& g : b->groups) CK(L_cell_count(d, g.w, g.n, g.T, sub, s));
       CK(L_scan_partial(d, b->w_scan, b->n_scan, sub, s));
       CK(L_scan_final(d, b->w_scan, b->n_scan, sub, s));
-      CK(L_cell_scatter(d, b->w_part, b->n_part, T, sub, s));
-      CK(L_cell_order(d, b->w_part, b->n_part, T, sub, s));
-      if (b->mode == CLAY_MODE_REFERENCE) {
-        CK(L_density_ref(d, b->w_part, b->n_part, T, sub, s));
-        CK(L_forces_ref(d, b->w_part, b->n_part, T, sub, s));
-      } else {
-        CK(L_density_fast(d, b->w_part, b->n_part, T, sub, s));
-        CK(L_forces_fast(d, b->w_part, b->n_part, T, sub, s));
+      for (auto& g : b->groups) CK(L_cell_scatter(d, g.w, g.n, g.T, sub, s));
+      for (auto& g : b->groups) CK(L_cell_order(d, g.w, g.n, g.T, sub, s));
+      for (auto& g : b->groups) {
+        if (b->mode == CLAY_MODE_REFERENCE) CK(L_density_ref(d, g.w, g.n, g.T, sub, s));
+        else CK(L_density_fast(d, g.w, g.n, g.T, sub, s));
+      }
+      for (auto& g : b->groups) {
+        if (b->mode == CLAY_MODE_REFERENCE) CK(L_forces_ref(d, g.w, g.n, g.T, sub, s));
+        else CK(L_forces_fast(d, g.w, g.n, g.T, sub, s));
       }
     }
   }
@@ -1379,6 +1413,19 @@ int clay_batch_set_tuning(clay_batch* b, const clay_batch_tuning* t) {
     return fail(CLAY_EINVAL, "sph_block %d must be a multiple of 32 in 64..256", t->sph_block);
   b->tune = *t;
   b->tune.splat_block = kSplatThreads;
+  b->release();
+  return CLAY_OK;
+}
+
+int clay_batch_set_bucket_blocks(clay_batch* b, const int64_t* upper, const int32_t* blocks, int n) {
+  if (!b || n < 0 || (n > 0 && (!upper || !blocks))) return fail(CLAY_EINVAL, "clay_batch_set_bucket_blocks: bad argument");
+  for (int i = 0; i < n; i++) {
+    if (blocks[i] < 64 || blocks[i] > 256 || (blocks[i] & 31))
+      return fail(CLAY_EINVAL, "bucket block %d must be a multiple of 32 in 64..256", blocks[i]);
+    if (i > 0 && upper[i] <= upper[i - 1]) return fail(CLAY_EINVAL, "bucket bounds must increase");
+  }
+  b->bucket_upper.assign(upper, upper + n);
+  b->bucket_block.assign(blocks, blocks + n);
   b->release();
   return CLAY_OK;
 }
@@ -1493,20 +1540,26 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
   if (b->n_part) {
     if ((rc = timed("emit", [&] { return L_emit(d, b->w_emit, b->n_emit, T, s); }))) return rc;
     for (int sub = 0; sub < b->max_substeps; sub++) {
-      if ((rc = timed("cell_key", [&] { return L_cell_key(d, b->w_part, b->n_part, T, sub, s); }))) return rc;
-      if ((rc = timed("cell_count", [&] { return L_cell_count(d, b->w_part, b->n_part, T, sub, s); }))) return rc;
+      for (auto& g : b->groups)
+        if ((rc = timed("cell_key", [&] { return L_cell_key(d, g.w, g.n, g.T, sub, s); }))) return rc;
+      for (auto& g : b->groups)
+        if ((rc = timed("cell_count", [&] { return L_cell_count(d, g.w, g.n, g.T, sub, s); }))) return rc;
       if ((rc = timed("scan_partial", [&] { return L_scan_partial(d, b->w_scan, b->n_scan, sub, s); }))) return rc;
       if ((rc = timed("scan_final", [&] { return L_scan_final(d, b->w_scan, b->n_scan, sub, s); }))) return rc;
-      if ((rc = timed("cell_scatter", [&] { return L_cell_scatter(d, b->w_part, b->n_part, T, sub, s); }))) return rc;
-      if ((rc = timed("cell_order", [&] { return L_cell_order(d, b->w_part, b->n_part, T, sub, s); }))) return rc;
-      if ((rc = timed("density", [&] {
-             return ref ? L_density_ref(d, b->w_part, b->n_part, T, sub, s) : L_density_fast(d, b->w_part, b->n_part, T, sub, s);
-           })))
-        return rc;
-      if ((rc = timed("forces_integrate", [&] {
-             return ref ? L_forces_ref(d, b->w_part, b->n_part, T, sub, s) : L_forces_fast(d, b->w_part, b->n_part, T, sub, s);
-           })))
-        return rc;
+      for (auto& g : b->groups)
+        if ((rc = timed("cell_scatter", [&] { return L_cell_scatter(d, g.w, g.n, g.T, sub, s); }))) return rc;
+      for (auto& g : b->groups)
+        if ((rc = timed("cell_order", [&] { return L_cell_order(d, g.w, g.n, g.T, sub, s); }))) return rc;
+      for (auto& g : b->groups)
+        if ((rc = timed("density", [&] {
+               return ref ? L_density_ref(d, g.w, g.n, g.T, sub, s) : L_density_fast(d, g.w, g.n, g.T, sub, s);
+             })))
+          return rc;
+      for (auto& g : b->groups)
+        if ((rc = timed("forces_integrate", [&] {
+               return ref ? L_forces_ref(d, g.w, g.n, g.T, sub, s) : L_forces_fast(d, g.w, g.n, g.T, sub, s);
+             })))
+          return rc;
     }
   }
   if (b->n_ssplat && (rc = timed("splat", [&] { return L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, kSplatAccVoxels, s); }))) return rc;

@@ -413,6 +413,10 @@ typedef struct clay_batch_tuning {
 } clay_batch_tuning;
 int clay_batch_set_tuning(clay_batch* b, const clay_batch_tuning* t);
 int clay_batch_get_tuning(const clay_batch* b, clay_batch_tuning* t);
+/* Per scene-size bucket block sizes of the particle passes (the autotuner's output): a scene
+ * whose capacity is below upper[i] uses blocks[i] threads per block; larger scenes use the
+ * batch's sph_block. upper[] increasing; blocks[] multiples of 32 in 64..256. */
+int clay_batch_set_bucket_blocks(clay_batch* b, const int64_t* upper, const int32_t* blocks, int n);
 /* One frame for every scene: host bookkeeping of each sim (as clay_fluid_step), then the
  * batched passes (or the captured graph) on `stream`. */
 int clay_batch_step(clay_batch* b, void* stream);
