@@ -17,6 +17,7 @@ constexpr uint32_t kSentinel = 0xffffffffu;
 constexpr int kMaxLeaves = 8;
 constexpr int kMaxParts = 64;
 constexpr int kMaxMips = 8;
+constexpr uint32_t kMaxNbr = 64;  // neighbour-list slots per particle
 constexpr int kSplatWarps = 8;  // warps per block of the splat pass
 constexpr int kSplatAccVoxels = 4096;   // shared-memory minimum tile of the splat pass (spheres)
 constexpr int kSplatAccVoxelsDiscs = 4096;  // the same for oriented-disc clouds
@@ -105,7 +106,8 @@ struct __align__(16) SceneDev {
   uint32_t* sorted_id;
   float4* spos;
   float4* svel;
-  float4* sdp;  // density, pressure, 1/density (the reference's per-pair `1 / other.density`)
+  float4* sdp;  // density, pressure, 1/density (the reference's per-pair `1 / other.density`), neighbours
+  uint32_t* nbr;  // accepted neighbours of the density pass, slot-major: nbr[j * capacity + k]
   uint32_t* counts;
   uint32_t* cell_start;
   const FieldDev* world;
@@ -704,11 +706,18 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float h2 = S.h2, mp6 = S.mass_poly6;
   float rho = 0.0f, comp = 0.0f;
   const float4* __restrict__ spos = S.spos;
+  // the accepted neighbours, in visiting order, for the forces pass (slot-major: the forces
+  // pass reads a warp's lanes at one slot as one contiguous line)
+  uint32_t* __restrict__ nl = S.nbr + k;
+  const uint32_t stride = S.capacity;
+  uint32_t cnt = 0;
   for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
     float4 o = __ldg(spos + q);
     float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
     float r2 = (dx * dx + dy * dy) + dz * dz;
     if (r2 < h2) {
+      if (cnt < kMaxNbr) nl[cnt * stride] = q;
+      cnt++;
       float wv = h2 - r2;
       float term = mp6 * ((wv * wv) * wv);
       if (kFast) {
@@ -725,7 +734,7 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   if (kFast) rho = __fadd_rn(rho, comp);
   const float stiff = S.prm->stiffness;
   const float dens = fmaxf(rho, S.rest_floor);
-  S.sdp[k] = make_float4(dens, fmaxf(stiff * (rho - S.rest), 0.0f), __frcp_rn(dens), 0.0f);
+  S.sdp[k] = make_float4(dens, fmaxf(stiff * (rho - S.rest), 0.0f), __frcp_rn(dens), __uint_as_float(cnt));
 }
 
 // forces (fluid.ts:370-439) fused with integrate (fluid.ts:449-491). The neighbour pass
@@ -755,7 +764,7 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
   const float4* __restrict__ spos = S.spos;
   const float4* __restrict__ svel = S.svel;
   const float4* __restrict__ sdp = S.sdp;
-  for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
+  auto pair = [&](uint32_t q) {
     if (q == k) return;
     float4 o = __ldg(spos + q);
     float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
@@ -781,7 +790,18 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
       fy = fy - (dy * ir) * s;
       fz = fz - (dz * ir) * s;
     }
-  });
+  };
+  // The density pass of this substep stored the neighbours it accepted, in the same visiting
+  // order, with the same squared lengths: the list replaces the scan of the 27 cells. A
+  // particle with more than kMaxNbr neighbours scans the cells again.
+  const uint32_t cnt = __float_as_uint(mdp.w);
+  if (cnt <= kMaxNbr) {
+    const uint32_t* __restrict__ nl = S.nbr + k;
+    const uint32_t stride = S.capacity;
+    for (uint32_t j = 0; j < cnt; j++) pair(__ldg(nl + j * stride));
+  } else {
+    for_neighbours(S, b, overflow, cx, cy, cz, pair);
+  }
   float id = mdp.z;
   float ax = fx * id + P.gravity[0], ay = fy * id + P.gravity[1], az = fz * id + P.gravity[2];
   float t = clampf(P.viscosity, 0.0f, 1.0f);

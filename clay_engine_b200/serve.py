@@ -238,7 +238,7 @@ class Server:
 
 def scene_bytes_estimate(n_particles, bake_res, bake_mips, grid_res, collider_res=64, collider_mips=3):
     """Device bytes of one scene as the library allocates them (FluidSim + surface + collider)."""
-    per_particle = 48 + 4 * 4 + 16 + 16 + 16  # records, key/rank/tmp/id, spos, svel, sdp
+    per_particle = 48 + 4 * 4 + 16 + 16 + 16 + 4 * 64  # records, key/rank/tmp/id, spos, svel, sdp, neighbour list
     cells = grid_res ** 3
     bake = sum((bake_res >> m) ** 3 for m in range(bake_mips)) * (4 + 2 + 2)
     coll = sum((collider_res >> m) ** 3 for m in range(collider_mips)) * 4
