@@ -882,7 +882,7 @@ int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_o
   if ((rc = f->alloc(&f->parts, C)) || (rc = f->alloc(&f->prm, 1)) || (rc = f->alloc(&f->contacts, 1)) ||
       (rc = f->alloc(&f->gs, 1)) || (rc = f->alloc(&f->hs.key, C)) || (rc = f->alloc(&f->hs.rank, C)) ||
       (rc = f->alloc(&f->hs.tmp, C)) || (rc = f->alloc(&f->hs.sorted_id, C)) || (rc = f->alloc(&f->hs.spos, C)) ||
-      (rc = f->alloc(&f->hs.svel, C)) || (rc = f->alloc(&f->hs.sdp, C)) || (rc = f->alloc(&f->hs.nbr, C * kMaxNbr)) ||
+      (rc = f->alloc(&f->hs.svel, C)) || (rc = f->alloc(&f->hs.sdp, C)) || (rc = f->alloc(&f->hs.nbr, C * (kMaxNbr / 4))) ||
       (rc = f->alloc(&f->hs.counts, cells + 1)) || (rc = f->alloc(&f->hs.cell_start, cells + 2)) ||
       (rc = f->alloc(&f->d_scene, 1))) {
     clay_fluid_destroy(f);

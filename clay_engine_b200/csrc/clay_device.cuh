@@ -107,7 +107,7 @@ struct __align__(16) SceneDev {
   float4* spos;
   float4* svel;
   float4* sdp;  // density, pressure, 1/density (the reference's per-pair `1 / other.density`), neighbours
-  uint32_t* nbr;  // accepted neighbours of the density pass, slot-major: nbr[j * capacity + k]
+  uint4* nbr;  // accepted neighbours of the density pass, 4 per entry, slot-major: nbr[(j / 4) * capacity + k]
   uint32_t* counts;
   uint32_t* cell_start;
   const FieldDev* world;
@@ -706,17 +706,18 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float h2 = S.h2, mp6 = S.mass_poly6;
   float rho = 0.0f, comp = 0.0f;
   const float4* __restrict__ spos = S.spos;
-  // the accepted neighbours, in visiting order, for the forces pass (slot-major: the forces
-  // pass reads a warp's lanes at one slot as one contiguous line)
-  uint32_t* __restrict__ nl = S.nbr + k;
-  const uint32_t stride = S.capacity;
+  // The accepted neighbours, in visiting order, for the forces pass: entry j of particle k is
+  // word j % 4 of nbr[(j / 4) * capacity + k], so the forces pass reads 4 at a time and a
+  // warp's lanes at one slot as contiguous lines.
+  uint32_t* __restrict__ nl = reinterpret_cast<uint32_t*>(S.nbr + k);
+  const uint32_t stride = 4u * S.capacity;
   uint32_t cnt = 0;
   for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
     float4 o = __ldg(spos + q);
     float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
     float r2 = (dx * dx + dy * dy) + dz * dz;
     if (r2 < h2) {
-      if (cnt < kMaxNbr) nl[cnt * stride] = q;
+      if (cnt < kMaxNbr) nl[(cnt >> 2) * stride + (cnt & 3u)] = q;
       cnt++;
       float wv = h2 - r2;
       float term = mp6 * ((wv * wv) * wv);
@@ -796,9 +797,15 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
   // particle with more than kMaxNbr neighbours scans the cells again.
   const uint32_t cnt = __float_as_uint(mdp.w);
   if (cnt <= kMaxNbr) {
-    const uint32_t* __restrict__ nl = S.nbr + k;
+    const uint4* __restrict__ nl = S.nbr + k;
     const uint32_t stride = S.capacity;
-    for (uint32_t j = 0; j < cnt; j++) pair(__ldg(nl + j * stride));
+    for (uint32_t j = 0; j < cnt; j += 4) {
+      const uint4 e = __ldg(nl + (j / 4u) * stride);
+      pair(e.x);
+      if (j + 1 < cnt) pair(e.y);
+      if (j + 2 < cnt) pair(e.z);
+      if (j + 3 < cnt) pair(e.w);
+    }
   } else {
     for_neighbours(S, b, overflow, cx, cy, cz, pair);
   }
