@@ -1078,6 +1078,102 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     // their relative cost (the block walk's pair is ~3x cheaper for spheres, ~1.5x for discs)
     const uint64_t lhs = bnu * nlive * (has_n ? 2ull : 1ull);
     const uint64_t rhs = s_cost * 3ull;
+    // Spheres, union box within the shared tile: register-blocked block walk. A work item is
+    // a brick of 4 x 2 x 2 voxels against a slice of the block's particles; the squared
+    // lengths share dx*dx, dy*dy, dz*dz and dx*dx + dy*dy across the brick (the reference's
+    // rounding order is kept), minima go to the shared tile as float bits (non-negative
+    // floats order like their bit patterns), and the tile is turned into keys at the end.
+    if (!has_n && bnu <= acc_cap && bnu * nlive <= s_cost * 6ull) {
+      extern __shared__ uint32_t s_tile[];
+      const uint32_t nbu = static_cast<uint32_t>(bnu);
+      for (uint32_t v = threadIdx.x; v < nbu; v += blockDim.x) s_tile[v] = 0x7f800000u;
+      const uint32_t ux = static_cast<uint32_t>(bnx), uy = static_cast<uint32_t>(bny), uz = static_cast<uint32_t>(bnz);
+      const uint32_t ngx = (ux + 3u) >> 2, ngy = (uy + 1u) >> 1, ngz = (uz + 1u) >> 1;
+      const uint32_t ngroups = ngx * ngy * ngz;
+      // enough (brick, slice) items for two per thread, slices of at least 16 particles
+      const uint32_t nsl = max(1u, min((2u * blockDim.x + ngroups - 1u) / ngroups, (nlive + 15u) / 16u));
+      const uint32_t per = (nlive + nsl - 1u) / nsl;
+      auto ofloat = [](int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff); };
+      const int* pbk = reinterpret_cast<const int*>(s_pb);
+      const float pbx0 = ofloat(pbk[0]), pby0 = ofloat(pbk[1]), pbz0 = ofloat(pbk[2]);
+      const float pbx1 = ofloat(pbk[3]), pby1 = ofloat(pbk[4]), pbz1 = ofloat(pbk[5]);
+      const float cull = reach * 1.0001f + 1e-5f;
+      const float cull2 = cull * cull;
+      __syncthreads();
+      for (uint32_t it = threadIdx.x; it < ngroups * nsl; it += blockDim.x) {
+        const uint32_t sl = it / ngroups, g = it - sl * ngroups;
+        const uint32_t gx = g % ngx, rest = g / ngx;
+        const uint32_t lx0 = gx * 4u, ly0 = (rest % ngy) * 2u, lz0 = (rest / ngy) * 2u;  // brick corner in the union box
+        const int x0 = bx0 + static_cast<int>(lx0), y0 = by0 + static_cast<int>(ly0), z0 = bz0 + static_cast<int>(lz0);
+        float cx[4], cy[2], cz[2];
+#pragma unroll
+        for (int k = 0; k < 4; k++) cx[k] = (static_cast<float>(x0 + k) + 0.5f) * voxel;
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+          cy[k] = (static_cast<float>(y0 + k) + 0.5f) * voxel;
+          cz[k] = (static_cast<float>(z0 + k) + 0.5f) * voxel;
+        }
+        {
+          // a brick farther than the reach from the particles' bounding box: nothing to lower
+          const float ex = fmaxf(fmaxf(pbx0 - cx[3], cx[0] - pbx1), 0.0f);
+          const float ey = fmaxf(fmaxf(pby0 - cy[1], cy[0] - pby1), 0.0f);
+          const float ez = fmaxf(fmaxf(pbz0 - cz[1], cz[0] - pbz1), 0.0f);
+          if (ex * ex + ey * ey + ez * ez > cull2) continue;
+        }
+        float b[16];
+#pragma unroll
+        for (int k = 0; k < 16; k++) b[k] = __int_as_float(0x7f800000);
+        const uint32_t j1 = min(nlive, (sl + 1u) * per);
+#pragma unroll 2
+        for (uint32_t j = sl * per; j < j1; j++) {
+          const float4 q = s_cp[j];
+          float dx2[4], dy2[2], dz2[2];
+#pragma unroll
+          for (int k = 0; k < 4; k++) {
+            const float d = cx[k] - q.x;
+            dx2[k] = d * d;
+          }
+#pragma unroll
+          for (int k = 0; k < 2; k++) {
+            const float dy = cy[k] - q.y, dz = cz[k] - q.z;
+            dy2[k] = dy * dy;
+            dz2[k] = dz * dz;
+          }
+#pragma unroll
+          for (int yy = 0; yy < 2; yy++)
+#pragma unroll
+            for (int xx = 0; xx < 4; xx++) {
+              const float t = dx2[xx] + dy2[yy];
+#pragma unroll
+              for (int zz = 0; zz < 2; zz++) b[xx + 4 * yy + 8 * zz] = fminf(b[xx + 4 * yy + 8 * zz], t + dz2[zz]);
+            }
+        }
+#pragma unroll
+        for (int zz = 0; zz < 2; zz++)
+#pragma unroll
+          for (int yy = 0; yy < 2; yy++)
+#pragma unroll
+            for (int xx = 0; xx < 4; xx++) {
+              const uint32_t lx = lx0 + xx, ly = ly0 + yy, lz = lz0 + zz;
+              const float v = b[xx + 4 * yy + 8 * zz];
+              if (lx < ux && ly < uy && lz < uz && v < __int_as_float(0x7f800000))
+                atomicMin(&s_tile[lx + ux * (ly + uy * lz)], __float_as_uint(v));
+            }
+      }
+      __syncthreads();
+      for (uint32_t v = threadIdx.x; v < nbu; v += blockDim.x) {
+        const uint32_t bits = s_tile[v];
+        if (bits == 0x7f800000u) continue;
+        const float sd = __fsqrt_rn(__uint_as_float(bits)) - radius;
+        if (sd < bw) {
+          const int x = bx0 + static_cast<int>(v % ux), y = by0 + static_cast<int>((v / ux) % uy),
+                    z = bz0 + static_cast<int>(v / (ux * uy));
+          atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
+                    enc_key(sd, bw));
+        }
+      }
+      return;
+    }
     if (bnu < (1ull << 30) && lhs <= rhs) {
       const uint32_t ngx = static_cast<uint32_t>((bnx + 3) >> 2);
       const uint32_t ngroups = ngx * static_cast<uint32_t>(bny * bnz);
