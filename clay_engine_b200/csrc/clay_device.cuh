@@ -19,6 +19,7 @@ constexpr int kMaxParts = 64;
 constexpr int kMaxMips = 8;
 constexpr uint32_t kMaxNbr = 64;  // neighbour-list slots per particle
 constexpr int kSplatWarps = 8;  // warps per block of the splat pass
+constexpr int kSplatItems = 2048;  // compacted (brick, slice) items of the sphere block walk
 constexpr int kSplatAccVoxels = 4096;   // shared-memory minimum tile of the splat pass (spheres)
 constexpr int kSplatAccVoxelsDiscs = 4096;  // the same for oriented-disc clouds
 
@@ -1090,20 +1091,95 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       const uint32_t ux = static_cast<uint32_t>(bnx), uy = static_cast<uint32_t>(bny), uz = static_cast<uint32_t>(bnz);
       const uint32_t ngx = (ux + 3u) >> 2, ngy = (uy + 1u) >> 1, ngz = (uz + 1u) >> 1;
       const uint32_t ngroups = ngx * ngy * ngz;
-      // enough (brick, slice) items for two per thread, slices of at least 16 particles
-      const uint32_t nsl = max(1u, min((2u * blockDim.x + ngroups - 1u) / ngroups, (nlive + 15u) / 16u));
+      // slices of ~32 consecutive (cell-ordered, so spatially close) particles, each with its
+      // own bounding box: a brick out of reach of a slice's box skips that slice
+      const uint32_t nsl = max(1u, (nlive + 31u) >> 5);  // <= kSplatWarps
       const uint32_t per = (nlive + nsl - 1u) / nsl;
-      auto ofloat = [](int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff); };
-      const int* pbk = reinterpret_cast<const int*>(s_pb);
-      const float pbx0 = ofloat(pbk[0]), pby0 = ofloat(pbk[1]), pbz0 = ofloat(pbk[2]);
-      const float pbx1 = ofloat(pbk[3]), pby1 = ofloat(pbk[4]), pbz1 = ofloat(pbk[5]);
+      __shared__ float s_sb[kSplatWarps][6];
+      if (static_cast<uint32_t>(wid) < nsl) {
+        const uint32_t j0 = static_cast<uint32_t>(wid) * per, j1 = min(nlive, j0 + per);
+        float a0 = __int_as_float(0x7f800000), a1 = a0, a2 = a0, b0 = -a0, b1 = -a0, b2 = -a0;
+        for (uint32_t j = j0 + lane; j < j1; j += 32) {
+          const float4 q = s_cp[j];
+          a0 = fminf(a0, q.x);
+          a1 = fminf(a1, q.y);
+          a2 = fminf(a2, q.z);
+          b0 = fmaxf(b0, q.x);
+          b1 = fmaxf(b1, q.y);
+          b2 = fmaxf(b2, q.z);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          a0 = fminf(a0, __shfl_xor_sync(0xffffffffu, a0, o));
+          a1 = fminf(a1, __shfl_xor_sync(0xffffffffu, a1, o));
+          a2 = fminf(a2, __shfl_xor_sync(0xffffffffu, a2, o));
+          b0 = fmaxf(b0, __shfl_xor_sync(0xffffffffu, b0, o));
+          b1 = fmaxf(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+          b2 = fmaxf(b2, __shfl_xor_sync(0xffffffffu, b2, o));
+        }
+        if (lane == 0) {
+          s_sb[wid][0] = a0;
+          s_sb[wid][1] = a1;
+          s_sb[wid][2] = a2;
+          s_sb[wid][3] = b0;
+          s_sb[wid][4] = b1;
+          s_sb[wid][5] = b2;
+        }
+      }
       const float cull = reach * 1.0001f + 1e-5f;
       const float cull2 = cull * cull;
+      __shared__ uint16_t s_items[kSplatItems];
+      __shared__ uint32_t s_nitems;
+      if (threadIdx.x == 0) s_nitems = 0u;
       __syncthreads();
-      for (uint32_t it = threadIdx.x; it < ngroups * nsl; it += blockDim.x) {
-        const uint32_t sl = it / ngroups, g = it - sl * ngroups;
-        const uint32_t gx = g % ngx, rest = g / ngx;
-        const uint32_t lx0 = gx * 4u, ly0 = (rest % ngy) * 2u, lz0 = (rest / ngy) * 2u;  // brick corner in the union box
+      const uint32_t nall = ngroups * nsl;
+      auto brick_of = [&](uint32_t it, uint32_t& sl, uint32_t& lx0, uint32_t& ly0, uint32_t& lz0) {
+        sl = it / ngroups;
+        const uint32_t g = it - sl * ngroups;
+        const uint32_t rest = g / ngx;
+        lx0 = (g - rest * ngx) * 4u;  // brick corner in the union box
+        ly0 = (rest % ngy) * 2u;
+        lz0 = (rest / ngy) * 2u;
+      };
+      // a brick farther than the reach from a slice's bounding box: nothing to lower
+      auto culled = [&](uint32_t sl, uint32_t lx0, uint32_t ly0, uint32_t lz0) {
+        const float* sb = s_sb[sl];
+        const float x0f = (static_cast<float>(bx0 + static_cast<int>(lx0)) + 0.5f) * voxel;
+        const float y0f = (static_cast<float>(by0 + static_cast<int>(ly0)) + 0.5f) * voxel;
+        const float z0f = (static_cast<float>(bz0 + static_cast<int>(lz0)) + 0.5f) * voxel;
+        const float x1f = (static_cast<float>(bx0 + static_cast<int>(lx0) + 3) + 0.5f) * voxel;
+        const float y1f = (static_cast<float>(by0 + static_cast<int>(ly0) + 1) + 0.5f) * voxel;
+        const float z1f = (static_cast<float>(bz0 + static_cast<int>(lz0) + 1) + 0.5f) * voxel;
+        const float ex = fmaxf(fmaxf(sb[0] - x1f, x0f - sb[3]), 0.0f);
+        const float ey = fmaxf(fmaxf(sb[1] - y1f, y0f - sb[4]), 0.0f);
+        const float ez = fmaxf(fmaxf(sb[2] - z1f, z0f - sb[5]), 0.0f);
+        return ex * ex + ey * ey + ez * ez > cull2;
+      };
+      // the (brick, slice) items that survive the cull, compacted so that lanes stay busy
+      const bool compact = nall <= static_cast<uint32_t>(kSplatItems);
+      if (compact) {
+        for (uint32_t base = 0; base < nall; base += blockDim.x) {
+          const uint32_t it = base + threadIdx.x;
+          bool keep = false;
+          if (it < nall) {
+            uint32_t sl, lx0, ly0, lz0;
+            brick_of(it, sl, lx0, ly0, lz0);
+            keep = !culled(sl, lx0, ly0, lz0);
+          }
+          const uint32_t m = __ballot_sync(0xffffffffu, keep);
+          uint32_t o = 0;
+          if (lane == 0 && m) o = atomicAdd(&s_nitems, static_cast<uint32_t>(__popc(m)));
+          o = __shfl_sync(0xffffffffu, o, 0);
+          if (keep) s_items[o + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(it);
+        }
+        __syncthreads();
+      }
+      const uint32_t nwork = compact ? s_nitems : nall;
+      for (uint32_t i = threadIdx.x; i < nwork; i += blockDim.x) {
+        const uint32_t it = compact ? static_cast<uint32_t>(s_items[i]) : i;
+        uint32_t sl, lx0, ly0, lz0;
+        brick_of(it, sl, lx0, ly0, lz0);
+        if (!compact && culled(sl, lx0, ly0, lz0)) continue;
         const int x0 = bx0 + static_cast<int>(lx0), y0 = by0 + static_cast<int>(ly0), z0 = bz0 + static_cast<int>(lz0);
         float cx[4], cy[2], cz[2];
 #pragma unroll
@@ -1112,13 +1188,6 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
         for (int k = 0; k < 2; k++) {
           cy[k] = (static_cast<float>(y0 + k) + 0.5f) * voxel;
           cz[k] = (static_cast<float>(z0 + k) + 0.5f) * voxel;
-        }
-        {
-          // a brick farther than the reach from the particles' bounding box: nothing to lower
-          const float ex = fmaxf(fmaxf(pbx0 - cx[3], cx[0] - pbx1), 0.0f);
-          const float ey = fmaxf(fmaxf(pby0 - cy[1], cy[0] - pby1), 0.0f);
-          const float ez = fmaxf(fmaxf(pbz0 - cz[1], cz[0] - pbz1), 0.0f);
-          if (ex * ex + ey * ey + ez * ez > cull2) continue;
         }
         float b[16];
 #pragma unroll
