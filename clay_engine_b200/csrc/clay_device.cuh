@@ -766,17 +766,15 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
   const float4* __restrict__ spos = S.spos;
   const float4* __restrict__ svel = S.svel;
   const float4* __restrict__ sdp = S.sdp;
-  auto pair = [&](uint32_t q) {
+  // one neighbour q with its cell-ordered position, density record and velocity
+  auto accum = [&](uint32_t q, const float4 o, const float4 odp, const float4 ov) {
     if (q == k) return;
-    float4 o = __ldg(spos + q);
     float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
     float r2 = (dx * dx + dy * dy) + dz * dz;
     if (r2 >= h2) return;
-    const float4 odp = __ldg(sdp + q);
     const float inv = odp.z;
     float w0 = h2 - r2;
     float wv = (w0 * w0) * w0;
-    float4 ov = __ldg(svel + q);
     vsx = vsx + ov.x * wv;
     vsy = vsy + ov.y * wv;
     vsz = vsz + ov.z * wv;
@@ -793,19 +791,41 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
       fz = fz - (dz * ir) * s;
     }
   };
+  auto pair = [&](uint32_t q) {
+    if (q == k) return;
+    const float4 o = __ldg(spos + q);
+    float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+    if ((dx * dx + dy * dy) + dz * dz >= h2) return;
+    accum(q, o, __ldg(sdp + q), __ldg(svel + q));
+  };
   // The density pass of this substep stored the neighbours it accepted, in the same visiting
-  // order, with the same squared lengths: the list replaces the scan of the 27 cells. A
-  // particle with more than kMaxNbr neighbours scans the cells again.
+  // order, with the same squared lengths: the list replaces the scan of the 27 cells, and
+  // every load of a group of kForceLoads neighbours is issued before any of them is used (a
+  // list entry is a neighbour, so nothing waits on the distance test). A particle with more
+  // than kMaxNbr neighbours scans the cells again.
+  constexpr int kForceLoads = 2;
   const uint32_t cnt = __float_as_uint(mdp.w);
   if (cnt <= kMaxNbr) {
     const uint4* __restrict__ nl = S.nbr + k;
     const uint32_t stride = S.capacity;
     for (uint32_t j = 0; j < cnt; j += 4) {
       const uint4 e = __ldg(nl + (j / 4u) * stride);
-      pair(e.x);
-      if (j + 1 < cnt) pair(e.y);
-      if (j + 2 < cnt) pair(e.z);
-      if (j + 3 < cnt) pair(e.w);
+      const uint32_t qa[4] = {e.x, e.y, e.z, e.w};
+#pragma unroll
+      for (int g = 0; g < 4; g += kForceLoads) {
+        float4 o[kForceLoads], d[kForceLoads], v[kForceLoads];
+#pragma unroll
+        for (int u = 0; u < kForceLoads; u++) {
+          if (j + g + u < cnt) {  // entries past the count hold no index
+            o[u] = __ldg(spos + qa[g + u]);
+            d[u] = __ldg(sdp + qa[g + u]);
+            v[u] = __ldg(svel + qa[g + u]);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kForceLoads; u++)
+          if (j + g + u < cnt) accum(qa[g + u], o[u], d[u], v[u]);
+      }
     }
   } else {
     for_neighbours(S, b, overflow, cx, cy, cz, pair);
