@@ -167,66 +167,110 @@ def run_serving(root, args, seed, stream):
 # Clocks during the timed region
 
 class ClockSampler:
+    """SM clock and clock-event reasons of one GPU, sampled every few milliseconds by a thread
+    through NVML (read-only queries), each sample time-stamped so the summary covers exactly the
+    window between mark() and stop(). Falls back to `nvidia-smi -lms` where NVML is missing."""
+
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, device):
+    def __init__(self, device, period_s=0.005):
         self.device = device
+        self.period = period_s
+        self.samples = []  # (time, sm_mhz, reason bits)
+        self.max_mhz = None
+        self.stop_flag = threading.Event()
+        self.t = None
         self.proc = None
-        self.lines = []
+        self.start = self.end = None
+
+    def _handle(self, N):
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return N.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return N.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _nvml_loop(self, N, h):
+        while not self.stop_flag.is_set():
+            try:
+                mhz = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+                bits = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((time.perf_counter(), float(mhz), int(bits)))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def _smi_loop(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz, self.max_mhz = float(f[1]), float(f[2])
+            except ValueError:
+                continue
+            bits = 0
+            for (nm, b), v in zip(self.REASONS, f[5:9]):
+                if v.lower().startswith("active"):
+                    bits |= b
+            self.samples.append((time.perf_counter(), mhz, bits))
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
-            # nvidia-smi's start-up holds the driver for a moment: let it finish before timing
-            t0 = time.time()
-            while not self.lines and time.time() - t0 < 15:
-                time.sleep(0.05)
-        except OSError:
-            self.proc = None
+            import pynvml as N
+
+            N.nvmlInit()
+            h = self._handle(N)
+            self.max_mhz = float(N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM))
+            self.t = threading.Thread(target=self._nvml_loop, args=(N, h), daemon=True)
+        except Exception:
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                              "--format=csv,noheader,nounits", "-lms", "100"],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.t = threading.Thread(target=self._smi_loop, daemon=True)
+            except OSError:
+                return self
+        self.t.start()
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 15:  # the first sample is in
+            time.sleep(0.01)
         return self
 
     def mark(self):
         """Starts the sample window of the timed region."""
-        self.start = len(self.lines)
+        self.start = time.perf_counter()
 
     def stop(self):
-        self.end = len(self.lines)
-
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+        self.end = time.perf_counter()
 
     def __exit__(self, *a):
+        self.stop_flag.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.t:
+            self.t.join(timeout=5)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        lines = self.lines[getattr(self, "start", 0):getattr(self, "end", len(self.lines)) + 1]
-        for ln in lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+        t0 = self.start if self.start is not None else -float("inf")
+        t1 = self.end if self.end is not None else float("inf")
+        inside = [x for x in self.samples if t0 <= x[0] <= t1]
+        if not inside and self.samples:  # a window shorter than the period: the nearest sample
+            inside = [min(self.samples, key=lambda x: abs(x[0] - t0))]
+        reasons = sorted({nm for _, _, bits in inside for nm, b in self.REASONS if bits & b})
+        sm = [x[1] for x in inside]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
                 "samples": len(sm)}
 
 
@@ -351,16 +395,17 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-# Algorithmic bytes per unit of each kernel (the compulsory DRAM traffic if every input were
-# read once and every output written once; neighbour re-reads are cache reuse, not counted).
+# Algorithmic bytes per particle and substep of the neighbour passes (the compulsory DRAM
+# traffic if every input were read once and every output written once; neighbour re-reads
+# are cache reuse and the neighbour list is an intermediate, neither is counted).
 BYTES_PER_PARTICLE = {
-    "cell_key": 16 + 4,            # pos in, key out
-    "cell_count": 4 + 4 + 4,       # key in, local key + rank out
-    "cell_scatter": 4 + 4 + 4,     # key, rank in, id out
-    "cell_order": 4 + 4 + 32 + 4 + 32,  # id, key in, pos+vel in; id, pos+vel out
-    "density": 16 + 8,             # pos in, density+pressure out
-    "forces_integrate": 16 + 16 + 8 + 4 + 48,  # pos, vel, rho/p, id in; particle record out
+    "density": 16 + 16,                        # pos in; density, pressure, 1/density, count out
+    "forces_integrate": 16 + 16 + 16 + 4 + 48,  # pos, vel, density record, id in; particle record out
 }
+# DRAM bytes (read + written) per particle of one k_splat launch over the fluid surfaces (3
+# levels), from the ncu capture summarised in profiles/k_splat_batched_128_scenes.md:
+# 107,436,288 + 5,356,032 bytes for 1,940,550 particles.
+SPLAT_TRAFFIC_PER_PARTICLE = (107436288 + 5356032) / 1940550
 
 
 def main():
@@ -489,20 +534,28 @@ def main():
     mips = sims[0].surface.volume.mipLevels if sims else 0
     n_sims = len(sims)
     splat_bytes = 16 * particles * mips + 8 * touched
-    # ---- per-kernel times of one frame (events around each launch) for the roofline
-    top = max(prof.items(), key=lambda kv: kv[1][0])
+    # ---- roofline of the dominant kernel, k_splat (its fluid-surface launch "splat": the
+    # SplatField bake of every fluid), from the per-launch event times of one frame
     peak, peak_kind = load_peaks()
-    roof = None
-    if top[0] in BYTES_PER_PARTICLE or top[0] == "splat":
-        per_launch_bytes = BYTES_PER_PARTICLE[top[0]] * particles if top[0] != "splat" else splat_bytes
-        avg_ms = top[1][0] / top[1][1]
-        achieved = per_launch_bytes / (avg_ms / 1000) / 1e9
-        roof = {"bound": "hbm", "kernel": top[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": per_launch_bytes, "avg_launch_ms": avg_ms}
-    else:
-        roof = {"bound": "hbm", "kernel": top[0], "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
-                "traffic": None, "peak_source": peak_kind}
+    splat_ms, splat_launches = prof.get("splat", (None, 0))
+    roof = {"bound": "hbm", "kernel": "k_splat (fluid surfaces)", "achieved": None, "peak": peak, "unit": "GB/s",
+            "frac": None, "traffic": None, "peak_source": peak_kind}
+    if splat_ms:
+        avg_ms = splat_ms / splat_launches
+        achieved = splat_bytes / (avg_ms / 1000) / 1e9
+        roof.update({"achieved": achieved, "frac": achieved / peak,
+                     "traffic": SPLAT_TRAFFIC_PER_PARTICLE * particles,
+                     "algorithmic_bytes_per_launch": splat_bytes, "avg_launch_ms": avg_ms,
+                     "limiter": "instruction issue (ncu: ~82% issue active, DRAM ~1% of peak)"})
+    # the neighbour passes against the same peak (one launch per block-size group and substep)
+    others = {}
+    for name, per in BYTES_PER_PARTICLE.items():
+        if name in prof:
+            ms_k, n_k = prof[name]
+            byt = per * particles * 2 / max(n_k, 1)  # 2 substeps spread over the launches
+            others[name] = {"achieved_gbs": byt / (ms_k / n_k / 1000) / 1e9, "avg_launch_ms": ms_k / n_k,
+                            "algorithmic_bytes_per_launch": byt}
+    roof["neighbour_passes"] = others
 
     # ---- serving: free the batched scenes first, then a resident pool under Poisson arrivals
     batch.destroy()
