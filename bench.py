@@ -103,10 +103,11 @@ def build_scenes(root, n_scenes, seed, with_bodies=True):
     return sims, bodies, keep
 
 
-def serve_pool(root, n_scenes, seed):
-    """The serving configuration: `n_scenes` resident scenes, particle counts log-uniform over
-    2k-256k, bake volumes 32^3 / 64^3 / 128^3 (seeded choice), a 64^3 collider of 8 brushes each.
-    Returns (factory, estimate)."""
+def serve_pool(root, n_scenes, seed, stream, budget):
+    """The serving configuration: a native server holding `n_scenes` registered scenes, particle
+    counts log-uniform over 2k-256k, bake volumes 32^3 / 64^3 / 128^3 (seeded choice), a 64^3
+    collider of 8 brushes each (built up front: colliders stay resident, the budget covers the
+    scenes' FluidSims). Returns (server, particle counts)."""
     import clay_engine_b200 as ce
     from clay_engine_b200 import scenes, serve
 
@@ -114,52 +115,40 @@ def serve_pool(root, n_scenes, seed):
     counts = scenes.log_uniform_counts(n_scenes, cfg["n_lo"], cfg["n_hi"], seed)
     rng = np.random.default_rng(seed + 1)
     bakes = [int(cfg["bakes"][int(b)]) for b in rng.integers(0, len(cfg["bakes"]), n_scenes)]
-    G = serve.grid_res_for(24.0, 0.22)
-
-    def opts(i):
-        o = dict(scenes.CONFIG3["fluid"])
-        o.update(capacity=int(counts[i]), bakeResolution=bakes[i], bakeMipLevels=max(1, int(math.log2(bakes[i] / 8))))
-        return o
-
-    def factory(i):
+    srv = serve.Server(root, stream, budget_bytes=budget)
+    for i in range(n_scenes):
         vol = ce.SdfVolume(root, resolution=64, worldSize=24.0, origin=scenes.WORLD_ORIGIN)
         vol.build(scenes.random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10), hi=(10, 1.0, 10)))
         field = ce.volumeField(vol)
-        sim = ce.FluidSim(root, field, opts(i))
+        o = dict(scenes.CONFIG3["fluid"])
+        o.update(capacity=int(counts[i]), bakeResolution=bakes[i], bakeMipLevels=max(1, int(math.log2(bakes[i] / 8))))
         n = int(counts[i])
         side = math.ceil(n ** (1 / 3)) * 0.1
-        sim.upload(scenes.lattice_block(n, 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i))
-        return sim, [field, vol]
-
-    def estimate(i):
-        return serve.scene_bytes_estimate(int(counts[i]), bakes[i], max(1, int(math.log2(bakes[i] / 8))), G)
-
-    return factory, estimate, counts
+        srv.add_scene(field, o, scenes.lattice_block(n, 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i), keep=[vol])
+    return srv, counts
 
 
 def run_serving(root, args, seed, stream):
     from clay_engine_b200 import scenes, serve
 
     cfg = scenes.CONFIG5
-    factory, estimate, counts = serve_pool(root, args.serve_pool, seed)
-    srv = serve.Server(root, factory, estimate, args.serve_pool, cfg["budget_bytes"])
     t0 = time.perf_counter()
-    for i in range(args.serve_pool):
-        if not srv.admit(i):
-            break
+    srv, counts = serve_pool(root, args.serve_pool, seed, stream, cfg["budget_bytes"])
+    # every scene once (admits them and warms the kernels), then the measured arrivals
+    srv.serve([(0.0, i, 1) for i in range(args.serve_pool)], timeout_s=600)
     setup_s = time.perf_counter() - t0
-    # warm the kernels on a few scenes, then reset the statistics
-    srv.serve([(0.0, i, 1) for i in range(min(8, args.serve_pool))], stream)
-    srv.stats = serve.ServeStats()
     arrivals = serve.poisson_arrivals(args.serve_rate, args.serve_window, args.serve_pool, cfg["k_lo"], cfg["k_hi"],
                                       seed + 2)
-    srv.serve(arrivals, stream, timeout_s=600)
-    out = srv.stats.summary()
+    out = srv.serve(arrivals, timeout_s=600)
+    st = srv.stats()
     out.update(rate_req_s=args.serve_rate, window_s_arrivals=args.serve_window, requests=len(arrivals),
-               resident_scenes=len(srv.resident), resident_gb=srv.used_bytes() / 1e9, setup_s=setup_s,
-               budget_gb=cfg["budget_bytes"] / 1e9, demand_particle_steps_s=float(
-                   args.serve_rate * (cfg["k_lo"] + cfg["k_hi"]) / 2 * np.mean(counts)))
+               resident_scenes=st["resident_scenes"], resident_gb=st["resident_bytes"] / 1e9, setup_s=setup_s,
+               budget_gb=cfg["budget_bytes"] / 1e9, server="native (clay_server_*)",
+               demand_particle_steps_s=float(args.serve_rate * (cfg["k_lo"] + cfg["k_hi"]) / 2 * np.mean(counts)))
     srv.close()
+    for f in srv.keep:
+        if hasattr(f, "destroy"):
+            f.destroy()
     return out
 
 
@@ -312,7 +301,7 @@ def cpu_sample(n_scenes, seed, max_particles, threads, frames=1):
             ref.step()
     dt = time.perf_counter() - t0
     desc = (f"{len(chosen)} of the {n_scenes} batched scenes nearest the median size, {total} particles, "
-            f"{frames} frame(s) each, f32 oracle with OpenMP")
+            f"{frames} frame(s) each, f32 oracle, {threads} thread(s)")
     return total * frames / dt, total * frames, dt, desc
 
 
@@ -571,6 +560,9 @@ def main():
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, total, dt, desc = cpu_sample(n_scenes, seed, 1_500_000, os.cpu_count() or 1, frames=2)
         cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port", "sample": desc}
+        # the same oracle on one core, on a smaller sample (~10 s)
+        v1, _, _, desc1 = cpu_sample(n_scenes, seed, 120_000, 1, frames=1)
+        cpu["one_core"] = {"value": v1, "unit": UNIT, "cores": 1, "sample": desc1}
 
     if rank == 0:
         line = {

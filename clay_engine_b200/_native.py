@@ -109,6 +109,18 @@ class BatchTuning(C.Structure):
     _fields_ = [("sph_block", C.c_int32), ("splat_block", C.c_int32), ("use_graph", C.c_int32)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("budget_bytes", C.c_uint64), ("depth", C.c_int32), ("max_batch", C.c_int32),
+                ("mode", C.c_int32), ("sph_block", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("frames", C.c_int64),
+                ("scene_frames", C.c_int64), ("particle_steps", C.c_int64), ("admissions", C.c_int64),
+                ("evictions", C.c_int64), ("resident_bytes", C.c_uint64), ("resident_scenes", C.c_int32),
+                ("inflight", C.c_int32)]
+
+
 P = C.c_void_p
 I = C.c_int
 D = C.c_double
@@ -170,6 +182,18 @@ SIGNATURES = {
     "clay_batch_read_contacts_async": (I, [P, P, P]),
     "clay_batch_profile": (I, [P, P, C.POINTER(PhaseTime), I, C.POINTER(C.c_int)]),
     "clay_batch_launches_per_step": (I, [P, C.POINTER(C.c_int64)]),
+    "clay_server_create": (I, [P, C.POINTER(ServerOpts), P, C.POINTER(P)]),
+    "clay_server_destroy": (None, [P]),
+    "clay_server_add_scene": (I, [P, P, C.POINTER(FluidOpts), P, C.c_int64, C.POINTER(C.c_int32)]),
+    "clay_server_submit": (I, [P, C.c_int32, C.c_int32, C.POINTER(C.c_int64)]),
+    "clay_server_pump": (I, [P, C.POINTER(C.c_int32)]),
+    "clay_server_wait": (I, [P, D]),
+    "clay_server_drain": (I, [P]),
+    "clay_server_poll": (I, [P, C.c_int64, C.POINTER(C.c_int32), C.POINTER(D)]),
+    "clay_server_get_stats": (I, [P, C.POINTER(ServerStats)]),
+    "clay_server_scene_sim": (I, [P, C.c_int32, C.POINTER(P)]),
+    "clay_server_download": (I, [P, C.c_int32, P, C.c_int64, C.POINTER(C.c_int64)]),
+    "clay_fluid_estimate_bytes": (I, [C.POINTER(FluidOpts), C.POINTER(C.c_uint64)]),
     "clay_kernel_launch_count": (C.c_uint64, []),
 }
 

@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "--expt-relaxed-constexpr"]
 UNITS = [("kern_ref.cu", ["-fmad=false"]), ("kern_fast.cu", ["-fmad=true"]),
-         ("clay_api.cu", ["-fmad=false"]), ("splat_static.cu", ["-fmad=false"])]
+         ("clay_api.cu", ["-fmad=false"]), ("splat_static.cu", ["-fmad=false"]), ("clay_server.cu", [])]
 HEADERS = ["clay_device.cuh", "launch.h"]
 
 

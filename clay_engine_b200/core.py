@@ -345,28 +345,16 @@ _PARAM_FIELD = {"gravity": "gravity", "dt": "dt", "emitPos": "emit_pos", "emitRa
 class FluidSim:
     """`FluidSim` (fluid.ts:111-582)."""
 
-    def __init__(self, root: Root, world: TracedField | None, options: dict | None = None, **kw):
-        opts = dict(options or {})
-        opts.update(kw)
-        o = N.FluidOpts()
-        for key, val in opts.items():
-            if key == "label":
-                continue
-            if key not in _FLUID_OPT_KEYS:
-                raise ClayError(N.CLAY_EINVAL, f"FluidSim: unknown option '{key}'")
-            if val is None:
-                continue
-            o.set |= N.FLUID[key]
-            name = _FLUID_FIELD.get(key, key)
-            if key in ("origin", "gravity"):
-                getattr(o, name)[:] = [float(x) for x in val]
-            elif key in ("capacity", "bucket", "bakeResolution", "bakeMipLevels", "substeps"):
-                setattr(o, name, int(val))
-            else:
-                setattr(o, name, float(val))
-        h = C.c_void_p()
-        check(lib().clay_fluid_create(root.handle, None if world is None else world.handle, C.byref(o), C.byref(h)))
-        self.handle = h.value
+    def __init__(self, root: Root, world: TracedField | None, options: dict | None = None, _handle=None, **kw):
+        self.owned = _handle is None
+        if _handle is None:
+            o = fluid_options(options, **kw)
+            h = C.c_void_p()
+            check(lib().clay_fluid_create(root.handle, None if world is None else world.handle, C.byref(o),
+                                          C.byref(h)))
+            self.handle = h.value
+        else:
+            self.handle = _handle
         self.root = root
         self.world = world
         info = N.FluidInfo()
@@ -455,9 +443,40 @@ class FluidSim:
         return out[: self.particleCount]
 
     def destroy(self):
-        if self.handle:
+        if self.handle and self.owned:
             lib().clay_fluid_destroy(self.handle)
         self.handle = None
+
+
+def fluid_options(options: dict | None = None, **kw) -> N.FluidOpts:
+    """`FluidSimOptions` (fluid.ts:60-108) as the C ABI takes them: a field per option and a
+    bit per option that is set, so unset ones resolve to the reference's defaults."""
+    opts = dict(options or {})
+    opts.update(kw)
+    o = N.FluidOpts()
+    for key, val in opts.items():
+        if key == "label":
+            continue
+        if key not in _FLUID_OPT_KEYS:
+            raise ClayError(N.CLAY_EINVAL, f"FluidSim: unknown option '{key}'")
+        if val is None:
+            continue
+        o.set |= N.FLUID[key]
+        name = _FLUID_FIELD.get(key, key)
+        if key in ("origin", "gravity"):
+            getattr(o, name)[:] = [float(x) for x in val]
+        elif key in ("capacity", "bucket", "bakeResolution", "bakeMipLevels", "substeps"):
+            setattr(o, name, int(val))
+        else:
+            setattr(o, name, float(val))
+    return o
+
+
+def fluid_estimate_bytes(options: dict | None = None, **kw) -> int:
+    """Device bytes a FluidSim with these options allocates (its surface included)."""
+    out = C.c_uint64()
+    check(lib().clay_fluid_estimate_bytes(C.byref(fluid_options(options, **kw)), C.byref(out)))
+    return int(out.value)
 
 
 class Batch:

@@ -39,6 +39,23 @@ int fail(int code, const char* fmt, ...) {
   return code;
 }
 
+}  // namespace
+
+namespace clay {
+// The same error slot for the other host translation units (the server).
+int set_error(int code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+}  // namespace clay
+
+namespace {
+
 #define CK(x)                                                                                 \
   do {                                                                                        \
     cudaError_t e_ = (x);                                                                     \
@@ -816,14 +833,11 @@ static void fill_scene(clay_fluid* f) {
   s.world = f->world ? f->world->d : nullptr;
 }
 
-int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_opts* opts, clay_fluid** out) {
-  if (!ctx || !out) return fail(CLAY_EINVAL, "clay_fluid_create: NULL argument");
-  clay_fluid_opts o{};
-  if (opts) o = *opts;
-  clay_fluid* f = new clay_fluid();
-  f->ctx = ctx;
-  f->world = world;
-  // fluid.ts:141-160
+}  // extern "C"
+
+namespace {
+// FluidSim options with the reference's defaults (fluid.ts:141-160), validated.
+int fluid_options(const clay_fluid_opts& o, clay_fluid* f) {
   f->capacity = (o.set & CLAY_FLUID_CAPACITY) ? o.capacity : 8192;
   f->spacing = (o.set & CLAY_FLUID_SPACING) ? o.spacing : 0.45;
   f->h = (o.set & CLAY_FLUID_SMOOTHING) ? o.smoothing : f->spacing * 2.2;
@@ -842,14 +856,54 @@ int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_o
     for (int k = 0; k < 3; k++) org[k] = o.origin[k];
   for (int k = 0; k < 3; k++) f->origin[k] = org[k];
   f->substeps = (o.set & CLAY_FLUID_SUBSTEPS) ? o.substeps : 3;
-  if (f->capacity <= 0 || f->capacity > (1ll << 30)) {
-    long long cap = static_cast<long long>(f->capacity);
-    delete f;
-    return fail(CLAY_EINVAL, "FluidSim: capacity %lld must be in 1..2^30", cap);
-  }
-  if (!(f->spacing > 0) || !(f->h > 0) || f->bucket <= 0 || f->substeps < 0) {
-    delete f;
+  if (f->capacity <= 0 || f->capacity > (1ll << 30))
+    return fail(CLAY_EINVAL, "FluidSim: capacity %lld must be in 1..2^30", static_cast<long long>(f->capacity));
+  if (!(f->spacing > 0) || !(f->h > 0) || f->bucket <= 0 || f->substeps < 0)
     return fail(CLAY_EINVAL, "FluidSim: spacing, smoothing and bucket must be positive and substeps non-negative");
+  return CLAY_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int clay_fluid_estimate_bytes(const clay_fluid_opts* opts, uint64_t* out) {
+  if (!out) return fail(CLAY_EINVAL, "clay_fluid_estimate_bytes: out is NULL");
+  clay_fluid_opts o{};
+  if (opts) o = *opts;
+  clay_fluid f;
+  int rc = fluid_options(o, &f);
+  if (!rc) rc = fluid_derive(&f);
+  if (rc) return rc;
+  // the allocations of clay_fluid_create: per particle, per grid cell, fixed, then the surface
+  const uint64_t C = static_cast<uint64_t>(f.capacity);
+  const uint64_t cells = static_cast<uint64_t>(f.G) * f.G * f.G;
+  uint64_t b = C * (sizeof(ParticleDev) + 4 * sizeof(uint32_t) + 3 * sizeof(float4) + (kMaxNbr / 4) * sizeof(uint4)) +
+               (cells + 1) * sizeof(uint32_t) + (cells + 2) * sizeof(uint32_t) + sizeof(ParamsDev) + sizeof(ContactsDev) +
+               sizeof(GridState) + sizeof(SceneDev);
+  uint64_t t = 0;
+  for (int m = 0; m < f.bake_mips; m++) {
+    const uint64_t r = static_cast<uint64_t>(f.bake_res >> m);
+    t += r * r * r;
+  }
+  // volume planes (f16 distance, f16 material) and uniform, its field, the key grid, descriptors
+  b += t * (2 * sizeof(__half) + sizeof(uint32_t)) + sizeof(VolParamsDev) + sizeof(FieldDev) + 2 * sizeof(SplatDev);
+  *out = b;
+  return CLAY_OK;
+}
+
+int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_opts* opts, clay_fluid** out) {
+  if (!ctx || !out) return fail(CLAY_EINVAL, "clay_fluid_create: NULL argument");
+  clay_fluid_opts o{};
+  if (opts) o = *opts;
+  clay_fluid* f = new clay_fluid();
+  f->ctx = ctx;
+  f->world = world;
+  {
+    int rc0 = fluid_options(o, f);
+    if (rc0) {
+      delete f;
+      return rc0;
+    }
   }
   if (world && world->ctx != ctx) {
     delete f;

@@ -1,64 +1,29 @@
 """Continuous-batching server for step-and-bake requests over device-resident scenes.
 
-A request asks one scene to advance `k` frames (each frame: FluidSim.step, i.e. the substeps
-and the SplatField bake) and is done when its last frame has completed on the device. The
-server keeps every admitted scene's particles, grids and volumes resident in HBM and, every
-frame, launches one batched step (`Batch.step_subset`) over the scenes that have a request in
-progress. Requests that arrive while frames are on the GPU join at the next frame boundary,
-so their work overlaps with requests already in flight; frames are enqueued up to `depth`
-ahead of the device.
+The scheduling loop is native (`clay_server_*` in include/clay_fluid.h): a request asks one
+scene to advance `k` frames (each frame: FluidSim.step, i.e. the substeps and the SplatField
+bake) and is done when its last frame has completed on the device. Every frame the server
+launches one batched step over the scenes that have a request in progress; requests arriving
+while frames run join at the next frame boundary, and up to `depth` frames are in flight.
+Scenes become resident when a request needs them, within a device-byte budget: idle scenes are
+evicted least-recently-used first (their particle state is kept on the host and restored when
+they return). Latency of a request = device completion of its last frame - its submission,
+on one clock (a CUDA event tied to the host's steady clock).
 
-Admission is by an HBM budget: a scene is made resident only when its estimated bytes fit
-beside the scenes already resident; otherwise idle scenes are evicted least-recently-used
-first (their particle state is kept on the host and restored when they return), and a
-request whose scene cannot be admitted waits until memory frees up.
-
-Latency of a request = device completion time of its last frame - its arrival time, both on
-one clock: the host clock at the start is tied to a CUDA event recorded on the idle stream.
+This module is the Python face of that server: scene registration from FluidSim options,
+the replay of an arrival schedule (`serve`), and the latency statistics.
 """
 from __future__ import annotations
 
-import collections
+import ctypes as C
 import math
 import time
-from dataclasses import dataclass, field
 
 import numpy as np
 
-from .core import Batch
-
-
-@dataclass
-class Request:
-    rid: int
-    scene: int
-    k: int
-    t_arrival: float
-    remaining: int = 0
-    t_done: float | None = None
-    particles: int = 0
-
-
-@dataclass
-class ServeStats:
-    completed: int = 0
-    particle_steps: float = 0.0
-    frames: int = 0
-    scene_frames: int = 0
-    latencies: list = field(default_factory=list)
-    t_first: float = 0.0
-    t_last: float = 0.0
-    evictions: int = 0
-    admissions: int = 0
-
-    def summary(self) -> dict:
-        lat = np.asarray(self.latencies) if self.latencies else np.zeros(1)
-        span = max(self.t_last - self.t_first, 1e-9)
-        return {"completed": self.completed, "throughput": self.particle_steps / span,
-                "p50_ms": float(np.percentile(lat, 50) * 1000), "p99_ms": float(np.percentile(lat, 99) * 1000),
-                "mean_ms": float(lat.mean() * 1000), "frames": self.frames,
-                "mean_batch": self.scene_frames / max(self.frames, 1), "window_s": span,
-                "evictions": self.evictions, "admissions": self.admissions}
+from . import _native as N
+from ._native import ClayError, check, lib, stream_handle
+from .core import PARTICLE_DTYPE, FluidSim, fluid_estimate_bytes, fluid_options
 
 
 def poisson_arrivals(rate, duration, n_scenes, k_lo, k_hi, seed):
@@ -73,177 +38,133 @@ def poisson_arrivals(rate, duration, n_scenes, k_lo, k_hi, seed):
     return out
 
 
+def _check(rc):
+    if rc == N.CLAY_ENOMEM:
+        raise MemoryError(lib().clay_last_error().decode(errors="replace"))
+    check(rc)
+
+
 class Server:
-    """`factory(i)` creates scene i on the device and returns (FluidSim, keepalive list);
-    `estimate(i)` is its device bytes (used for admission before creating it)."""
+    """A `clay_server`: scenes registered with `add_scene`, requests with `submit`."""
 
-    def __init__(self, root, factory, estimate, n_scenes, budget_bytes, depth=2, max_batch=1 << 30,
-                 sph_block=256):
+    def __init__(self, root, stream=None, budget_bytes=0, depth=2, max_batch=0, mode="fast", sph_block=0):
+        o = N.ServerOpts(budget_bytes=int(budget_bytes), depth=int(depth), max_batch=int(max_batch),
+                         mode=N.MODE_REFERENCE if mode == "reference" else N.MODE_FAST, sph_block=int(sph_block))
+        h = C.c_void_p()
+        self.stream = stream
+        _check(lib().clay_server_create(root.handle, C.byref(o), stream_handle(stream), C.byref(h)))
+        self.handle = h.value
         self.root = root
-        self.factory = factory
-        self.estimate = estimate
-        self.n_scenes = n_scenes
-        self.budget = budget_bytes
-        self.depth = depth
-        self.max_batch = max_batch
-        self.sph_block = sph_block
-        self.resident = collections.OrderedDict()  # scene -> (sim, keep, bytes); LRU order
-        self.snapshots = {}
-        self.batch = None
-        self.index = {}
-        self.dirty = True
-        self.stats = ServeStats()
-        self.busy = set()
+        self.budget = int(budget_bytes)
+        self.tickets = []
+        self.keep = []  # colliders of the registered scenes: they must outlive the server
 
-    # -- residency ---------------------------------------------------------------------------
-    def used_bytes(self) -> int:
-        return sum(v[2] for v in self.resident.values())
+    # -- scenes and requests ----------------------------------------------------------------
+    def add_scene(self, world, options: dict, particles: np.ndarray | None = None, keep=()) -> int:
+        o = fluid_options(options)
+        a = np.ascontiguousarray(particles if particles is not None else np.zeros(0, PARTICLE_DTYPE), PARTICLE_DTYPE)
+        sid = C.c_int32()
+        _check(lib().clay_server_add_scene(self.handle, None if world is None else world.handle, C.byref(o),
+                                           a.ctypes.data if len(a) else None, len(a), C.byref(sid)))
+        self.keep += [world, *keep]
+        return int(sid.value)
 
-    def admit(self, scene) -> bool:
-        if scene in self.resident:
-            self.resident.move_to_end(scene)
-            return True
-        need = self.estimate(scene)
-        if need > self.budget:
-            raise MemoryError(f"scene {scene} needs {need} bytes, over the {self.budget}-byte budget")
-        while self.used_bytes() + need > self.budget:
-            victim = next((s for s in self.resident if s not in self.busy), None)
-            if victim is None:
-                return False
-            self.evict(victim)
-        before = self.root.bytes_in_use()
-        sim, keep = self.factory(scene)
-        if scene in self.snapshots:
-            sim.upload(self.snapshots.pop(scene))
-        self.resident[scene] = (sim, keep, self.root.bytes_in_use() - before)
-        self.stats.admissions += 1
-        self.dirty = True
-        return True
+    def submit(self, scene: int, frames: int) -> int:
+        t = C.c_int64()
+        _check(lib().clay_server_submit(self.handle, int(scene), int(frames), C.byref(t)))
+        self.tickets.append(int(t.value))
+        return int(t.value)
 
-    def evict(self, scene):
-        import torch
+    def pump(self) -> bool:
+        launched = C.c_int32()
+        _check(lib().clay_server_pump(self.handle, C.byref(launched)))
+        return bool(launched.value)
 
-        sim, keep, _ = self.resident.pop(scene)
-        torch.cuda.synchronize()  # its last frame may still be running on the serving stream
-        self.snapshots[scene] = sim.download()
-        sim.destroy()
-        for x in keep:
-            if hasattr(x, "destroy"):
-                x.destroy()
-        self.stats.evictions += 1
-        self.dirty = True
+    def wait(self, timeout_ms: float = -1.0):
+        _check(lib().clay_server_wait(self.handle, float(timeout_ms)))
 
-    def _rebuild(self):
-        if self.batch is not None:
-            self.batch.destroy()
-        order = list(self.resident)
-        self.index = {s: i for i, s in enumerate(order)}
-        self.batch = Batch(self.root, [self.resident[s][0] for s in order], sph_block=self.sph_block, use_graph=False)
-        self.dirty = False
+    def drain(self):
+        _check(lib().clay_server_drain(self.handle))
 
-    def sim(self, scene):
-        return self.resident[scene][0]
+    def poll(self, ticket: int):
+        done, lat = C.c_int32(), C.c_double()
+        _check(lib().clay_server_poll(self.handle, int(ticket), C.byref(done), C.byref(lat)))
+        return bool(done.value), float(lat.value)
 
-    # -- the request loop --------------------------------------------------------------------
-    def serve(self, arrivals, stream, timeout_s=600.0):
-        """Runs until every arrival (t, scene, k) has completed. Returns the requests."""
-        import torch
+    def stats(self) -> dict:
+        s = N.ServerStats()
+        _check(lib().clay_server_get_stats(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in N.ServerStats._fields_}
 
-        reqs = [Request(i, s, k, t) for i, (t, s, k) in enumerate(arrivals)]
-        for r in reqs:
-            r.remaining = r.k
-        waiting = collections.defaultdict(collections.deque)
-        active = {}
-        inflight = collections.deque()
-        nxt = 0
-        done = 0
-        stream.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        ev0.synchronize()
+    def sim(self, scene: int) -> FluidSim | None:
+        """The scene's FluidSim while resident (a view: the server owns it), else None."""
+        h = C.c_void_p()
+        _check(lib().clay_server_scene_sim(self.handle, int(scene), C.byref(h)))
+        return None if not h.value else FluidSim(self.root, None, _handle=h.value)
+
+    def download(self, scene: int) -> np.ndarray:
+        """The scene's particles after all its submitted frames (resident or evicted)."""
+        n = C.c_int64()
+        _check(lib().clay_server_download(self.handle, int(scene), None, 0, C.byref(n)))
+        out = np.zeros(int(n.value), PARTICLE_DTYPE)
+        _check(lib().clay_server_download(self.handle, int(scene), out.ctypes.data if len(out) else None, len(out),
+                                          C.byref(n)))
+        return out
+
+    # -- an arrival schedule ------------------------------------------------------------------
+    def serve(self, arrivals, timeout_s=600.0) -> dict:
+        """Replays `arrivals` [(t, scene, k)] (t in seconds from now, sorted): each request is
+        submitted once its time has come, the server is pumped in between. Returns the
+        statistics of these requests."""
+        first = len(self.tickets)
+        s0 = self.stats()
         t0 = time.perf_counter()
-        self.stats.t_first = reqs[0].t_arrival if reqs else 0.0
-        while done < len(reqs):
+        nxt = 0
+        while True:
             now = time.perf_counter() - t0
             if now > timeout_s:
-                raise TimeoutError(f"serving did not finish within {timeout_s} s ({done}/{len(reqs)} done)")
-            while nxt < len(reqs) and reqs[nxt].t_arrival <= now:
-                waiting[reqs[nxt].scene].append(reqs[nxt])
+                raise TimeoutError(f"serving did not finish within {timeout_s} s")
+            while nxt < len(arrivals) and arrivals[nxt][0] <= now:
+                self.submit(arrivals[nxt][1], arrivals[nxt][2])
                 nxt += 1
-            # activate the head request of every waiting scene whose scene can be resident
-            for scene in list(waiting):
-                if scene in active or not waiting[scene]:
-                    continue
-                if self.admit(scene):
-                    r = waiting[scene].popleft()
-                    r.particles = self.sim(scene).particleCount
-                    active[scene] = r
-                    self.busy.add(scene)
-                if not waiting[scene]:
-                    del waiting[scene]
-            launched = False
-            if active and len(inflight) < self.depth:
-                if self.dirty:
-                    stream.synchronize()
-                    self._rebuild()
-                scenes = list(active)[: self.max_batch]
-                self.batch.step_subset([self.index[s] for s in scenes], stream)
-                ev = torch.cuda.Event(enable_timing=True)
-                ev.record(stream)
-                finished = []
-                for s in scenes:
-                    r = active[s]
-                    r.remaining -= 1
-                    self.stats.particle_steps += r.particles
-                    if r.remaining == 0:
-                        finished.append(r)
-                        del active[s]
-                        self.busy.discard(s)
-                inflight.append((ev, finished))
-                self.stats.frames += 1
-                self.stats.scene_frames += len(scenes)
-                launched = True
-            # retire completed frames
-            while inflight and inflight[0][0].query():
-                ev, finished = inflight.popleft()
-                t = ev0.elapsed_time(ev) / 1000.0
-                for r in finished:
-                    r.t_done = t
-                    self.stats.latencies.append(t - r.t_arrival)
-                    self.stats.completed += 1
-                    self.stats.t_last = max(self.stats.t_last, t)
-                    done += 1
-            if not launched:
-                if inflight and len(inflight) >= self.depth:
-                    inflight[0][0].synchronize()
-                elif not active and nxt < len(reqs):
-                    wait = reqs[nxt].t_arrival - (time.perf_counter() - t0)
-                    if wait > 0:
-                        time.sleep(min(wait, 0.002))
-                elif inflight:
-                    inflight[0][0].synchronize()
-        return reqs
+            launched = self.pump()
+            st = self.stats()
+            if nxt == len(arrivals) and st["completed"] == st["submitted"]:
+                break
+            if launched:
+                continue
+            gap = (arrivals[nxt][0] - (time.perf_counter() - t0)) if nxt < len(arrivals) else None
+            if st["inflight"] > 0:
+                # wait on the device, but not past the next arrival
+                self.wait(-1.0 if gap is None else max(0.0, min(gap, 0.005)) * 1000.0)
+            elif gap is not None:
+                time.sleep(max(0.0, min(gap, 0.002)))
+            else:
+                self.drain()  # raises when waiting scenes can never be admitted
+        span = time.perf_counter() - t0
+        lat = np.array([self.poll(t)[1] for t in self.tickets[first:]]) if len(self.tickets) > first else np.zeros(1)
+        st = self.stats()
+        return {"completed": st["completed"] - s0["completed"],
+                "throughput": (st["particle_steps"] - s0["particle_steps"]) / max(span, 1e-9),
+                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "mean_ms": float(lat.mean()), "frames": st["frames"] - s0["frames"],
+                "mean_batch": (st["scene_frames"] - s0["scene_frames"]) / max(st["frames"] - s0["frames"], 1),
+                "window_s": span, "evictions": st["evictions"] - s0["evictions"],
+                "admissions": st["admissions"] - s0["admissions"]}
 
     def close(self):
-        if self.batch is not None:
-            self.batch.destroy()
-            self.batch = None
-        for s in list(self.resident):
-            sim, keep, _ = self.resident.pop(s)
-            sim.destroy()
-            for x in keep:
-                if hasattr(x, "destroy"):
-                    x.destroy()
+        if self.handle:
+            lib().clay_server_destroy(self.handle)
+        self.handle = None
 
 
-def scene_bytes_estimate(n_particles, bake_res, bake_mips, grid_res, collider_res=64, collider_mips=3):
-    """Device bytes of one scene as the library allocates them (FluidSim + surface + collider)."""
-    per_particle = 48 + 4 * 4 + 16 + 16 + 16 + 4 * 64  # records, key/rank/tmp/id, spos, svel, sdp, neighbour list
-    cells = grid_res ** 3
-    bake = sum((bake_res >> m) ** 3 for m in range(bake_mips)) * (4 + 2 + 2)
-    coll = sum((collider_res >> m) ** 3 for m in range(collider_mips)) * 4
-    return int(n_particles * per_particle + (2 * cells + 3) * 4 + bake + coll + 4096)
+def scene_bytes_estimate(options: dict) -> int:
+    """Device bytes of one scene's FluidSim (particles, grids, neighbour list, surface)."""
+    return fluid_estimate_bytes(options)
 
 
 def grid_res_for(world_size, h):
     return int(math.ceil(world_size / h)) + 2
+
+
+__all__ = ["Server", "ClayError", "poisson_arrivals", "scene_bytes_estimate", "grid_res_for"]

@@ -440,6 +440,69 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
 int clay_batch_launches_per_step(const clay_batch* b, int64_t* out);
 
 /* ------------------------------------------------------------------------------------
+ * Continuous-batching server (no reference counterpart: the reference steps the scenes of
+ * one game). Serves requests "advance scene i by k frames" (each frame: FluidSim.step with
+ * its bake) over many registered scenes. Each frame it launches one clay_batch_step_subset
+ * over the scenes with a request in progress; requests arriving while frames run join at the
+ * next frame boundary; up to `depth` frames are in flight. Scenes become resident (their
+ * FluidSim created) when a request needs them, within a device-byte budget: idle scenes are
+ * evicted least-recently-used first, keeping their particle state on the host, and get it
+ * back on return. Colliders stay owned by the caller and must outlive the server.
+ * One host thread per server; all device work goes to the server's stream.
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_server clay_server;
+typedef struct clay_server_opts {
+  uint64_t budget_bytes; /* device bytes the resident scenes may hold; 0: no limit */
+  int32_t depth;         /* frames in flight, 1..8; 0: 2 */
+  int32_t max_batch;     /* scenes stepped per frame; 0: every scene with a request */
+  int32_t mode;          /* CLAY_MODE_FAST or CLAY_MODE_REFERENCE */
+  int32_t sph_block;     /* threads per block of the particle passes; 0: the batch default */
+} clay_server_opts;
+int clay_server_create(clay_ctx* ctx, const clay_server_opts* opts, void* stream, clay_server** out);
+/* Waits for the frames in flight, then frees every resident scene. */
+void clay_server_destroy(clay_server* s);
+/* Registers a scene (not resident until a request needs it): its FluidSim options, the
+ * collider it collides with (may be NULL) and its initial particles (copied; count <= the
+ * capacity). Its id is returned in `scene_out` (0, 1, 2, ... in registration order). */
+int clay_server_add_scene(clay_server* s, const clay_field* world, const clay_fluid_opts* opts,
+                          const clay_fluid_particle* particles, int64_t count, int32_t* scene_out);
+/* Queues `frames` (>= 1) frames of `scene`, arriving now (the host's steady clock). A scene's
+ * requests run one after another in submission order. */
+int clay_server_submit(clay_server* s, int32_t scene, int32_t frames, int64_t* ticket_out);
+/* One scheduling step, without waiting on the device: retire completed frames, admit scenes
+ * that have requests, launch at most one frame. `launched` (may be NULL): 1 if it did. */
+int clay_server_pump(clay_server* s, int32_t* launched);
+/* Waits until the oldest frame in flight completes (and retires it), or `timeout_ms` passes
+ * (< 0: no limit). Returns at once when nothing is in flight. */
+int clay_server_wait(clay_server* s, double timeout_ms);
+/* Pumps, waiting on the oldest frame when nothing can launch, until every submitted request
+ * is done. CLAY_ENOMEM when a waiting scene can never fit the budget. */
+int clay_server_drain(clay_server* s);
+/* done = 1 once the ticket's last frame has completed on the device; latency_ms = that
+ * completion minus the submission, on one clock (a CUDA event tied to the host clock). */
+int clay_server_poll(const clay_server* s, int64_t ticket, int32_t* done, double* latency_ms);
+typedef struct clay_server_stats {
+  int64_t submitted;
+  int64_t completed;
+  int64_t frames;        /* batched launches */
+  int64_t scene_frames;  /* scenes stepped, summed over frames */
+  int64_t particle_steps;
+  int64_t admissions;
+  int64_t evictions;
+  uint64_t resident_bytes;
+  int32_t resident_scenes;
+  int32_t inflight;
+} clay_server_stats;
+int clay_server_get_stats(const clay_server* s, clay_server_stats* out);
+/* The scene's FluidSim while it is resident, else NULL (valid until the next pump). */
+int clay_server_scene_sim(clay_server* s, int32_t scene, clay_fluid** sim_out);
+/* The scene's particle state after all its submitted frames: waits for them, then copies
+ * from the device (resident) or the host snapshot (evicted). `n_out`: live particles. */
+int clay_server_download(clay_server* s, int32_t scene, clay_fluid_particle* host, int64_t cap, int64_t* n_out);
+/* Device bytes a FluidSim with these options allocates (what the server budgets with). */
+int clay_fluid_estimate_bytes(const clay_fluid_opts* opts, uint64_t* out);
+
+/* ------------------------------------------------------------------------------------
  * Number of library kernel launches enqueued by this process so far (all objects).
  * ---------------------------------------------------------------------------------- */
 uint64_t clay_kernel_launch_count(void);

@@ -1,6 +1,7 @@
-"""Continuous-batching server: every request's result is the same alone and in the mix (bit for
-bit: scenes in one batched launch never interact), admission respects the HBM budget, an
-evicted scene comes back with its state, and a scene over the budget is refused."""
+"""Continuous-batching server (clay_server_*): every request's result is the same alone and in
+the mix (bit for bit: scenes in one batched launch never interact), admission respects the
+device-byte budget, an evicted scene comes back with its state, a scene over the budget is
+refused, and the byte estimate is what a FluidSim allocates."""
 import numpy as np
 import pytest
 
@@ -10,110 +11,125 @@ ORIGIN = (-12.0, -4.0, -12.0)
 COUNTS = [1500, 3000, 800, 2200, 1200]
 
 
-def factory_for(root):
+def options(i):
+    return dict(capacity=COUNTS[i], spacing=0.1, radius=0.05, substeps=2, bakeResolution=32, bakeBand=4.0,
+                worldSize=24.0, origin=ORIGIN)
+
+
+def particles(i):
+    from clay_engine_b200 import scenes
+
+    p = scenes.lattice_block(COUNTS[i], 0.1, (0.2 * i, 0.5, -0.3 * i), 7 + i)
+    p["vel"] = (0.1 * i, -1.0, 0.0)
+    return p
+
+
+@pytest.fixture(scope="module")
+def colliders(root):
     import clay_engine_b200 as ce
     from clay_engine_b200 import scenes
 
-    def make(i):
+    out = []
+    for i in range(len(COUNTS)):
         vol = ce.SdfVolume(root, resolution=64, worldSize=24.0, origin=ORIGIN)
         vol.build(scenes.random_brushes(6, seed=100 + i))
-        field = ce.volumeField(vol)
-        sim = ce.FluidSim(root, field, dict(capacity=COUNTS[i], spacing=0.1, radius=0.05, substeps=2,
-                                            bakeResolution=32, bakeBand=4.0, worldSize=24.0, origin=ORIGIN))
-        p = scenes.lattice_block(COUNTS[i], 0.1, (0.2 * i, 0.5, -0.3 * i), 7 + i)
-        p["vel"] = (0.1 * i, -1.0, 0.0)
-        sim.upload(p)
-        return sim, [field, vol]
-
-    return make
+        out.append((ce.volumeField(vol), vol))
+    yield out
+    for f, v in out:
+        f.destroy()
+        v.destroy()
 
 
-def estimate(i):
-    from clay_engine_b200 import serve
-
-    return serve.scene_bytes_estimate(COUNTS[i], 32, 2, serve.grid_res_for(24.0, 0.22))
-
-
-def state(sim):
-    g = sim.download()
-    d, _ = sim.surface.volume.download()
-    return g, d
-
-
-def same(a, b):
-    ga, da = a
-    gb, db = b
-    for name in ("pos", "vel", "density", "pressure", "nvel"):
-        if not np.array_equal(np.ascontiguousarray(ga[name]).view(np.uint32),
-                              np.ascontiguousarray(gb[name]).view(np.uint32)):
-            return False
-    return np.array_equal(da, db)
-
-
-def test_same_alone_and_in_the_mix(root):
-    import torch
-
+def server(root, colliders, budget, stream):
     from clay_engine_b200.serve import Server
 
-    stream = torch.cuda.Stream()
-    make = factory_for(root)
-    alone = Server(root, make, estimate, 5, 1 << 40)
-    mix = Server(root, make, estimate, 5, 1 << 40)
-    alone.serve([(0.0, 0, 3)], stream)
-    # scene 0 gets the same request (k=3) while other scenes' requests overlap with it
-    mix.serve([(0.0, 1, 2), (0.0, 0, 3), (0.001, 2, 5), (0.002, 1, 1), (0.003, 3, 4), (0.004, 4, 2)], stream)
-    torch.cuda.synchronize()
-    assert same(state(alone.sim(0)), state(mix.sim(0)))
-    # and both equal the plain path: the scene stepped on its own three times
-    sim, keep = make(0)
-    for _ in range(3):
+    srv = Server(root, stream, budget_bytes=budget)
+    for i in range(len(COUNTS)):
+        assert srv.add_scene(colliders[i][0], options(i), particles(i)) == i
+    return srv
+
+
+def plain(root, colliders, i, frames, stream):
+    import torch
+
+    import clay_engine_b200 as ce
+
+    sim = ce.FluidSim(root, colliders[i][0], options(i))
+    sim.upload(particles(i))
+    for _ in range(frames):
         sim.step(stream)
     torch.cuda.synchronize()
-    assert same(state(sim), state(mix.sim(0)))
-    assert mix.stats.completed == 6 and mix.stats.frames >= 5
-    s = mix.stats.summary()
+    return sim
+
+
+def same_particles(ga, gb):
+    return all(np.array_equal(np.ascontiguousarray(ga[n]).view(np.uint32), np.ascontiguousarray(gb[n]).view(np.uint32))
+               for n in ("pos", "vel", "density", "pressure", "nvel"))
+
+
+def test_same_alone_and_in_the_mix(root, colliders):
+    import torch
+
+    stream = torch.cuda.Stream()
+    alone = server(root, colliders, 0, stream)
+    mix = server(root, colliders, 0, stream)
+    alone.serve([(0.0, 0, 3)])
+    # scene 0 gets the same request (k=3) while other scenes' requests overlap with it
+    s = mix.serve([(0.0, 1, 2), (0.0, 0, 3), (0.001, 2, 5), (0.002, 1, 1), (0.003, 3, 4), (0.004, 4, 2)])
+    torch.cuda.synchronize()
+    a, m = alone.sim(0), mix.sim(0)
+    assert same_particles(a.download(), m.download())
+    assert np.array_equal(a.surface.volume.download()[0], m.surface.volume.download()[0])
+    # and both equal the plain path: the scene stepped on its own three times
+    ref = plain(root, colliders, 0, 3, stream)
+    assert same_particles(ref.download(), m.download())
+    assert np.array_equal(ref.surface.volume.download()[0], m.surface.volume.download()[0])
+    assert s["completed"] == 6 and s["frames"] >= 5
     assert s["p99_ms"] >= s["p50_ms"] > 0
-    sim.destroy()
+    assert mix.stats()["resident_scenes"] == 5
+    ref.destroy()
     alone.close()
     mix.close()
 
 
-def test_budget_admission_and_eviction_keep_state(root):
+def test_budget_admission_and_eviction_keep_state(root, colliders):
     import torch
 
-    from clay_engine_b200.serve import Server
+    from clay_engine_b200 import serve
 
     stream = torch.cuda.Stream()
-    make = factory_for(root)
-    budget = estimate(1) + estimate(3) + 1024  # two of the larger scenes at a time
-    srv = Server(root, make, estimate, 5, budget)
-    srv.serve([(0.0, 0, 2), (0.0, 1, 2), (0.0, 2, 1), (0.0, 3, 2), (0.001, 4, 1), (0.002, 0, 2)], stream)
-    assert srv.stats.completed == 6
-    assert srv.stats.evictions > 0
-    assert srv.used_bytes() <= budget
+    est = [serve.scene_bytes_estimate(options(i)) for i in range(len(COUNTS))]
+    budget = est[1] + est[3] + 1024  # two of the larger scenes at a time
+    srv = server(root, colliders, budget, stream)
+    s = srv.serve([(0.0, 0, 2), (0.0, 1, 2), (0.0, 2, 1), (0.0, 3, 2), (0.001, 4, 1), (0.002, 0, 2)])
+    st = srv.stats()
+    assert s["completed"] == 6 and st["completed"] == 6
+    assert st["evictions"] > 0
+    assert st["resident_bytes"] <= budget
     # scene 0 made 4 frames in two requests, possibly evicted and restored in between
-    # (a scene restored after its last frame has not re-baked yet, so the particle state is
-    # what is compared)
-    srv.admit(0)
-    got = state(srv.sim(0))[0]
-    ref, keep = make(0)
-    for _ in range(4):
-        ref.step(stream)
-    torch.cuda.synchronize()
-    want = state(ref)[0]
-    for name in ("pos", "vel", "density", "pressure", "nvel"):
-        assert np.array_equal(np.ascontiguousarray(got[name]).view(np.uint32),
-                              np.ascontiguousarray(want[name]).view(np.uint32)), name
-    ref.destroy()
+    for i, frames in ((0, 4), (1, 2), (2, 1)):
+        ref = plain(root, colliders, i, frames, stream)
+        assert same_particles(srv.download(i), ref.download()), i
+        ref.destroy()
     srv.close()
 
 
-def test_scene_over_budget_is_refused(root):
+def test_scene_over_budget_is_refused(root, colliders):
     import torch
 
-    from clay_engine_b200.serve import Server
-
-    srv = Server(root, factory_for(root), estimate, 5, 1000)
+    srv = server(root, colliders, 1000, torch.cuda.Stream())
     with pytest.raises(MemoryError):
-        srv.serve([(0.0, 1, 1)], torch.cuda.Stream(), timeout_s=30)
+        srv.serve([(0.0, 1, 1)], timeout_s=30)
     srv.close()
+
+
+def test_estimate_is_what_a_sim_allocates(root, colliders):
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import serve
+
+    for i in (0, 3):
+        before = root.bytes_in_use()
+        sim = ce.FluidSim(root, colliders[i][0], options(i))
+        used = root.bytes_in_use() - before
+        assert used == serve.scene_bytes_estimate(options(i))
+        sim.destroy()
