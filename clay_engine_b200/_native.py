@@ -109,6 +109,14 @@ class BatchTuning(C.Structure):
     _fields_ = [("sph_block", C.c_int32), ("splat_block", C.c_int32), ("use_graph", C.c_int32)]
 
 
+class ExtractorOpts(C.Structure):
+    _fields_ = [("set", C.c_uint32), ("resolution", C.c_int32), ("body", C.c_int32), ("base", C.c_int32),
+                ("capacity", C.c_int32), ("pad", C.c_int32), ("motion", C.c_void_p)]
+
+
+CLAY_EXTRACT_RESOLUTION = 1
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("budget_bytes", C.c_uint64), ("depth", C.c_int32), ("max_batch", C.c_int32),
                 ("mode", C.c_int32), ("sph_block", C.c_int32)]
@@ -194,6 +202,14 @@ SIGNATURES = {
     "clay_server_scene_sim": (I, [P, C.c_int32, C.POINTER(P)]),
     "clay_server_download": (I, [P, C.c_int32, P, C.c_int64, C.POINTER(C.c_int64)]),
     "clay_fluid_estimate_bytes": (I, [C.POINTER(FluidOpts), C.POINTER(C.c_uint64)]),
+    "clay_extractor_create": (I, [P, P, P, C.c_int64, P, C.c_int32, C.POINTER(ExtractorOpts), C.POINTER(P)]),
+    "clay_extractor_destroy": (None, [P]),
+    "clay_extractor_set_region": (I, [P, C.POINTER(D), D, C.POINTER(D), I]),
+    "clay_extractor_extract": (I, [P, P]),
+    "clay_extractor_views": (I, [P, C.POINTER(P), C.POINTER(P), C.POINTER(C.c_int64)]),
+    "clay_extractor_read_counts_async": (I, [P, P, P]),
+    "clay_extractor_read_indices_async": (I, [P, P, P, P]),
+    "clay_field_offset_device": (I, [P, P, C.POINTER(P)]),
     "clay_kernel_launch_count": (C.c_uint64, []),
 }
 

@@ -202,6 +202,83 @@ def offsetField(f: TracedField, offset) -> TracedField:
     return TracedField(h.value, True, (f,))
 
 
+def motion_buffer(center=(0.0, 0.0, 0.0), velocity=(0.0, 0.0, 0.0)):
+    """An ExtractMotion (extract.ts:30-45) as an 8-float CUDA tensor: centre, pad, velocity, pad."""
+    import torch
+
+    return torch.tensor([*center, 0.0, *velocity, 0.0], dtype=torch.float32, device="cuda")
+
+
+def offsetFieldDevice(f: TracedField, device_offset) -> TracedField:
+    """offsetField(f, () => offset) with the offset read on the device at every sample (3 floats
+    at `device_offset`, a CUDA tensor or pointer that must outlive the field), e.g. the centre
+    of an ExtractMotion."""
+    h = C.c_void_p()
+    check(lib().clay_field_offset_device(f.handle, _dev_ptr(device_offset), C.byref(h)))
+    return TracedField(h.value, True, (f, device_offset))
+
+
+def _dev_ptr(x) -> int:
+    """A device pointer from a CUDA tensor or an int."""
+    return int(x) if isinstance(x, int) else int(x.data_ptr())
+
+
+class SurfaceExtractor:
+    """`SurfaceExtractor` (sim/extract.ts:84-484): naive surface nets of `field`'s zero level
+    set into a ParticleSet held by the caller as device memory: `particles` (96-byte Particle
+    records, `set_capacity` of them) and `bodies` (64-byte Body records, `max_bodies`).
+    `motion`: an optional caller-owned ExtractMotion (8 device floats: centre, pad, velocity,
+    pad, e.g. a CUDA tensor made by `motion_buffer`)."""
+
+    def __init__(self, root: Root, particles, set_capacity: int, bodies, max_bodies: int, field: TracedField,
+                 body: int, base: int, capacity: int, resolution: int | None = None, motion=None):
+        o = N.ExtractorOpts(body=int(body), base=int(base), capacity=int(capacity),
+                            motion=None if motion is None else _dev_ptr(motion))
+        if resolution is not None:
+            o.set |= N.CLAY_EXTRACT_RESOLUTION
+            o.resolution = int(resolution)
+        h = C.c_void_p()
+        check(lib().clay_extractor_create(root.handle, field.handle, _dev_ptr(particles), int(set_capacity),
+                                          _dev_ptr(bodies), int(max_bodies), C.byref(o), C.byref(h)))
+        self.handle = h.value
+        self.root = root
+        self.field = field
+        self.resolution = 32 if resolution is None else int(resolution)
+        self._keep = (particles, bodies, motion)
+        idx, draw, qc = C.c_void_p(), C.c_void_p(), C.c_int64()
+        check(lib().clay_extractor_views(self.handle, C.byref(idx), C.byref(draw), C.byref(qc)))
+        self.indices_ptr, self.draw_args_ptr, self.quadCapacity = idx.value, draw.value, int(qc.value)
+
+    def setRegion(self, origin, size: float, vel=(0.0, 0.0, 0.0), preserveMotion: bool = False):
+        o = (C.c_double * 3)(*[float(x) for x in origin])
+        v = (C.c_double * 3)(*[float(x) for x in vel])
+        check(lib().clay_extractor_set_region(self.handle, o, float(size), v, 1 if preserveMotion else 0))
+
+    def extract(self, pass_=None):
+        check(lib().clay_extractor_extract(self.handle, stream_handle(pass_)))
+
+    def counts(self, stream=None):
+        """(dual vertices, quads) of the last extraction, before the capacity clamps."""
+        out = np.zeros(2, np.uint32)
+        check(lib().clay_extractor_read_counts_async(self.handle, out.ctypes.data, stream_handle(stream)))
+        _sync(stream)
+        return int(out[0]), int(out[1])
+
+    def indices(self, stream=None):
+        """(triangles as an (n, 3) uint32 array, draw arguments) of the last extraction."""
+        idx = np.zeros(self.quadCapacity * 6, np.uint32)
+        draw = np.zeros(4, np.uint32)
+        check(lib().clay_extractor_read_indices_async(self.handle, idx.ctypes.data, draw.ctypes.data,
+                                                      stream_handle(stream)))
+        _sync(stream)
+        return idx[: int(draw[0])].reshape(-1, 3), draw
+
+    def destroy(self):
+        if self.handle:
+            lib().clay_extractor_destroy(self.handle)
+        self.handle = None
+
+
 @dataclass
 class ParticleCloud:
     """`ParticleCloud` (splat.ts:15-38) as device arrays.

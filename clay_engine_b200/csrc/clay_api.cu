@@ -169,6 +169,7 @@ struct clay_field {
   struct Leaf {
     clay_volume* vol;
     double off[3];
+    const float* dyn = nullptr;  // device offset applied outermost (an extractor's motion centre)
   };
   std::vector<Leaf> leaves;
   FieldDev h{};
@@ -186,6 +187,7 @@ struct clay_field {
         any = any || leaves[i].off[k] != 0.0;
       }
       h.leaf[i].has_offset = any ? 1 : 0;
+      h.leaf[i].dyn_offset = leaves[i].dyn;
     }
     dirty = true;
   }
@@ -1782,6 +1784,167 @@ int clay_batch_step_subset(clay_batch* b, const int32_t* scenes, int n, void* st
   if (n_splat) CK(L_splat(b->d_surf, W + o_splat, n_splat, 1, kSplatAccVoxels, s));
   if (n_res) CK(L_resolve(b->d_surf, W + o_res, n_res, s));
   return CLAY_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// SurfaceExtractor (extract.ts:84-484).
+struct clay_extractor {
+  clay_ctx* ctx = nullptr;
+  const clay_field* field = nullptr;
+  ExtractDev h{};
+  ExtractDev* d = nullptr;
+  std::vector<DevBuf> bufs;
+  bool dirty = true;
+  int blocks = 0;
+
+  template <class T>
+  int alloc(T** p, size_t count) {
+    void* q = nullptr;
+    int rc = ctx->dev_alloc(&q, sizeof(T) * std::max<size_t>(count, 1));
+    if (rc) return rc;
+    bufs.push_back({q, sizeof(T) * std::max<size_t>(count, 1)});
+    *p = static_cast<T*>(q);
+    return CLAY_OK;
+  }
+  int flush(cudaStream_t s) {
+    if (field) {
+      int rc = const_cast<clay_field*>(field)->flush(s);
+      if (rc) return rc;
+      h.field = field->d;
+    }
+    if (!dirty) return CLAY_OK;
+    int rc = ctx->upload(d, &h, sizeof(h), s);
+    if (rc) return rc;
+    dirty = false;
+    return CLAY_OK;
+  }
+};
+
+extern "C" {
+
+int clay_extractor_create(clay_ctx* ctx, const clay_field* field, void* particles, int64_t set_capacity, void* bodies,
+                          int32_t max_bodies, const clay_extractor_opts* opts, clay_extractor** out) {
+  if (!ctx || !field || !particles || !bodies || !opts || !out)
+    return fail(CLAY_EINVAL, "clay_extractor_create: NULL argument");
+  if (field->ctx != ctx) return fail(CLAY_EINVAL, "SurfaceExtractor: the field belongs to another context");
+  const int res = (opts->set & CLAY_EXTRACT_RESOLUTION) ? opts->resolution : 32;  // extract.ts:99
+  if (res < 2 || res > 512) return fail(CLAY_EINVAL, "SurfaceExtractor: resolution %d outside 2..512", res);
+  if (opts->capacity < 0 || opts->base < 0)
+    return fail(CLAY_EINVAL, "SurfaceExtractor: base and capacity must be non-negative");
+  if (static_cast<int64_t>(opts->base) + opts->capacity > set_capacity)  // extract.ts:101-103
+    return fail(CLAY_EINVAL, "SurfaceExtractor: slice [%d, %lld) exceeds set capacity", opts->base,
+                static_cast<long long>(opts->base) + opts->capacity);
+  if (opts->body < 0 || opts->body >= max_bodies)
+    return fail(CLAY_EINVAL, "SurfaceExtractor: body %d outside the set's %d bodies", opts->body, max_bodies);
+  if ((reinterpret_cast<uintptr_t>(particles) & 15) || (reinterpret_cast<uintptr_t>(bodies) & 15))
+    return fail(CLAY_EINVAL, "SurfaceExtractor: particle and body buffers must be 16-byte aligned");
+  clay_extractor* x = new clay_extractor();
+  x->ctx = ctx;
+  x->field = field;
+  ExtractDev& h = x->h;
+  const int64_t cells = static_cast<int64_t>(res) * res * res;
+  x->blocks = static_cast<int>((cells + kExtractThreads - 1) / kExtractThreads);
+  h.particles = static_cast<unsigned char*>(particles);
+  h.bodies = static_cast<unsigned char*>(bodies);
+  h.res = res;
+  h.body = opts->body;
+  h.base = opts->base;
+  h.capacity = opts->capacity;
+  // a closed surface-nets mesh has about as many quads as vertices (extract.ts:105-107)
+  h.quad_cap = static_cast<int32_t>(std::ceil(opts->capacity * 1.5));
+  h.has_motion = opts->motion ? 1 : 0;
+  h.motion = opts->motion;
+  if (reinterpret_cast<uintptr_t>(opts->motion) & 15) {
+    delete x;
+    return fail(CLAY_EINVAL, "SurfaceExtractor: the motion buffer must be 16-byte aligned");
+  }
+  h.nblocks = x->blocks;
+  h.cell = 0.1f;  // the reference's initial region (extract.ts:124-129)
+  int rc;
+  float4* rec = nullptr;
+  if ((rc = x->alloc(&x->d, 1)) || (rc = x->alloc(&h.id_grid, cells)) || (rc = x->alloc(&rec, cells * 2)) ||
+      (rc = x->alloc(&h.blk, x->blocks)) || (rc = x->alloc(&h.qblk, x->blocks)) || (rc = x->alloc(&h.qmask, cells)) ||
+      (rc = x->alloc(&h.indices, static_cast<size_t>(h.quad_cap) * 6)) || (rc = x->alloc(&h.draw_args, 4)) ||
+      (rc = x->alloc(&h.counters, 2))) {
+    clay_extractor_destroy(x);
+    return rc;
+  }
+  h.rec = rec;
+  CK(cudaMemset(h.counters, 0, 2 * sizeof(uint32_t)));
+  CK(cudaMemset(h.draw_args, 0, 4 * sizeof(uint32_t)));
+  *out = x;
+  return CLAY_OK;
+}
+
+void clay_extractor_destroy(clay_extractor* x) {
+  if (!x) return;
+  for (auto& b : x->bufs) x->ctx->dev_free(b.p, b.n);
+  delete x;
+}
+
+int clay_extractor_set_region(clay_extractor* x, const double origin[3], double size, const double vel[3],
+                              int preserve_motion) {
+  if (!x || !origin) return fail(CLAY_EINVAL, "clay_extractor_set_region: NULL argument");
+  for (int k = 0; k < 3; k++) {
+    x->h.origin[k] = static_cast<float>(origin[k]);
+    x->h.vel[k] = vel ? static_cast<float>(vel[k]) : 0.0f;
+  }
+  x->h.cell = static_cast<float>(size / x->h.res);  // extract.ts:451-463: cell = size / resolution
+  x->h.preserve = preserve_motion ? 1u : 0u;
+  x->dirty = true;
+  return CLAY_OK;
+}
+
+int clay_extractor_extract(clay_extractor* x, void* stream) {
+  if (!x) return fail(CLAY_EINVAL, "clay_extractor_extract: NULL extractor");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = x->flush(s);
+  if (rc) return rc;
+  CK(L_ext_reset(x->d, s));
+  CK(L_ext_cells(x->d, x->blocks, s));
+  CK(L_ext_scan(x->d, 0, s));
+  CK(L_ext_emit(x->d, x->blocks, s));
+  CK(L_ext_qcount(x->d, x->blocks, s));
+  CK(L_ext_scan(x->d, 1, s));
+  CK(L_ext_qemit(x->d, x->blocks, s));
+  CK(L_ext_finish(x->d, s));
+  return CLAY_OK;
+}
+
+int clay_extractor_views(clay_extractor* x, uint32_t** indices, uint32_t** draw_args, int64_t* quad_capacity) {
+  if (!x) return fail(CLAY_EINVAL, "clay_extractor_views: NULL extractor");
+  if (indices) *indices = x->h.indices;
+  if (draw_args) *draw_args = x->h.draw_args;
+  if (quad_capacity) *quad_capacity = x->h.quad_cap;
+  return CLAY_OK;
+}
+
+int clay_extractor_read_counts_async(clay_extractor* x, uint32_t* host_counts, void* stream) {
+  if (!x || !host_counts) return fail(CLAY_EINVAL, "clay_extractor_read_counts_async: NULL argument");
+  CK(cudaMemcpyAsync(host_counts, x->h.counters, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                     static_cast<cudaStream_t>(stream)));
+  return CLAY_OK;
+}
+
+int clay_extractor_read_indices_async(clay_extractor* x, uint32_t* host_indices, uint32_t* host_draw_args, void* stream) {
+  if (!x || !host_indices || !host_draw_args) return fail(CLAY_EINVAL, "clay_extractor_read_indices_async: NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  CK(cudaMemcpyAsync(host_indices, x->h.indices, sizeof(uint32_t) * 6 * static_cast<size_t>(x->h.quad_cap),
+                     cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(host_draw_args, x->h.draw_args, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  return CLAY_OK;
+}
+
+int clay_field_offset_device(const clay_field* f, const float* device_offset, clay_field** out) {
+  if (!f || !device_offset || !out) return fail(CLAY_EINVAL, "clay_field_offset_device: NULL argument");
+  std::vector<clay_field::Leaf> l = f->leaves;
+  for (auto& leaf : l) {
+    if (leaf.dyn) return fail(CLAY_EINVAL, "clay_field_offset_device: the field already follows a device offset");
+    leaf.dyn = device_offset;
+  }
+  return make_field(f->ctx, std::move(l), out);
 }
 
 }  // extern "C"

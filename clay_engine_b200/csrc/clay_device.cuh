@@ -69,12 +69,32 @@ struct __align__(16) VolParamsDev {
   const __half* mat;
 };
 
-// One leaf of a collider: volumeField(volume), optionally offsetField-moved.
+// One leaf of a collider: volumeField(volume), optionally offsetField-moved by a constant
+// and, outermost, by an offset read on the device (an extractor's GPU-side motion centre).
 struct LeafDev {
   const VolParamsDev* vp;
   float offset[3];
   int32_t has_offset;
+  const float* dyn_offset;
 };
+
+// The point in a leaf's own frame: offsetField subtracts its offset (trace/field.ts:396-429),
+// the outermost one first.
+__device__ __forceinline__ void leaf_point(const LeafDev& lf, float px, float py, float pz, float& qx, float& qy, float& qz) {
+  qx = px;
+  qy = py;
+  qz = pz;
+  if (lf.dyn_offset) {
+    qx = qx - lf.dyn_offset[0];
+    qy = qy - lf.dyn_offset[1];
+    qz = qz - lf.dyn_offset[2];
+  }
+  if (lf.has_offset) {
+    qx = qx - lf.offset[0];
+    qy = qy - lf.offset[1];
+    qz = qz - lf.offset[2];
+  }
+}
 struct __align__(16) FieldDev {
   int32_t n;
   int32_t pad[3];
@@ -147,6 +167,30 @@ struct __align__(16) SplatDev {
 struct Work {
   uint32_t obj, sub, first, n;
 };
+
+// A SurfaceExtractor (extract.ts:84-484) as the kernels see it: the field, the caller's
+// ParticleSet (96-byte Particle and 64-byte Body records), the scratch of one extraction,
+// the region uniform and the optional GPU-side motion (centre xyz, pad, velocity xyz, pad).
+struct __align__(16) ExtractDev {
+  const FieldDev* field;
+  unsigned char* particles;
+  unsigned char* bodies;
+  float* motion;
+  uint32_t* id_grid;   // res^3, +1 biased particle index, 0: no dual vertex
+  float4* rec;         // res^3 x 2: (vertex, material), (normal, has-vertex)
+  uint32_t* blk;       // per block of 256 cells: vertex count, then its exclusive offset
+  uint32_t* qblk;      // per block of 256 lattice points: quad count, then offset
+  unsigned char* qmask;  // res^3: the edges (x, y, z bits) whose quad is emitted
+  uint32_t* indices;   // quad_cap x 6
+  uint32_t* draw_args; // vertexCount, instanceCount, firstVertex, firstInstance
+  uint32_t* counters;  // vertex cells, quads (before the capacity clamps)
+  float origin[3];
+  float cell;
+  float vel[3];
+  uint32_t preserve;
+  int32_t res, body, base, capacity, quad_cap, has_motion, nblocks, pad_;
+};
+constexpr int kExtractThreads = 256;  // cells (lattice points) per block of the grid passes
 
 // The brush record (brush.ts:52-78), 80 bytes.
 struct BrushDev {
@@ -312,12 +356,8 @@ __device__ __forceinline__ int field_pick(const FieldDev* f, float px, float py,
   for (int i = 0; i < n; i++) {
     const LeafDev& lf = f->leaf[i];
     Vol v = load_vol(lf.vp);
-    float qx = px, qy = py, qz = pz;
-    if (lf.has_offset) {
-      qx = px - lf.offset[0];
-      qy = py - lf.offset[1];
-      qz = pz - lf.offset[2];
-    }
+    float qx, qy, qz;
+    leaf_point(lf, px, py, pz, qx, qy, qz);
     float s0, s1;
     vol_sample(v, qx, qy, qz, s0, s1);
     if (best < 0 || !(bx < s0)) {
@@ -335,13 +375,22 @@ __device__ __forceinline__ void field_normal(const FieldDev* f, int child, float
                                              float& nz) {
   const LeafDev& lf = f->leaf[child];
   Vol v = load_vol(lf.vp);
-  float qx = px, qy = py, qz = pz;
-  if (lf.has_offset) {
-    qx = px - lf.offset[0];
-    qy = py - lf.offset[1];
-    qz = pz - lf.offset[2];
-  }
+  float qx, qy, qz;
+  leaf_point(lf, px, py, pz, qx, qy, qz);
   vol_normal(v, qx, qy, qz, nx, ny, nz);
+}
+
+// field(p, 0).y of the child `field_pick` chose at p (trace/field.ts:147-150,288-293,
+// volume.ts:288-296): the material channel, trilinear like the distance, 0 outside the box.
+__device__ __forceinline__ float field_material(const FieldDev* f, int child, float px, float py, float pz) {
+  if (child < 0) return 0.0f;
+  const LeafDev& lf = f->leaf[child];
+  Vol v = load_vol(lf.vp);
+  float qx, qy, qz;
+  leaf_point(lf, px, py, pz, qx, qy, qz);
+  if (sd_box(qx - v.cx, qy - v.cy, qz - v.cz, v.half) > 0.0f) return 0.0f;
+  v.dist = lf.vp->mat;
+  return trilinear(v, qx, qy, qz);
 }
 
 // ---------------------------------------------------------------------------------------
@@ -1693,6 +1742,399 @@ __global__ void k_cell_index(const SceneDev* __restrict__ scenes, uint32_t* __re
   bool in = cx >= 0 && cy >= 0 && cz >= 0 && cx < S.G && cy < S.G && cz < S.G;
   uint32_t g = static_cast<uint32_t>(S.G);
   out[i] = in ? static_cast<uint32_t>(cx) + g * (static_cast<uint32_t>(cy) + g * static_cast<uint32_t>(cz)) : kSentinel;
+}
+
+// ---------------------------------------------------------------------------------------
+// SurfaceExtractor.extract (extract.ts:469-475): naive surface nets of the field's zero set
+// on a res^3 lattice. The reference hands out particle and quad slots with atomics, so their
+// order is unspecified; here a block scan gives them in lattice order (cells, then lattice
+// points with their +x, +y, +z edges), which makes the output, the centre of mass included,
+// deterministic and reproducible by the CPU restatement.
+
+// Block-wide exclusive scan of one value per thread (256 threads); returns the block total.
+__device__ __forceinline__ uint32_t ext_block_scan(uint32_t v, uint32_t& excl) {
+  __shared__ uint32_t s_w[kExtractThreads / 32];
+  const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  uint32_t x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= static_cast<uint32_t>(o)) x += y;
+  }
+  if (lane == 31) s_w[wid] = x;
+  __syncthreads();
+  uint32_t before = 0, total = 0;
+  for (uint32_t k = 0; k < kExtractThreads / 32; k++) {
+    const uint32_t t = s_w[k];
+    if (k < wid) before += t;
+    total += t;
+  }
+  excl = before + x - v;
+  __syncthreads();
+  return total;
+}
+
+// The scan origin (extract.ts:169-178) and the emitted velocity (:179-188).
+__device__ __forceinline__ void ext_origin(const ExtractDev& E, float& ox, float& oy, float& oz) {
+  ox = E.origin[0];
+  oy = E.origin[1];
+  oz = E.origin[2];
+  if (E.has_motion) {
+    ox = ox + E.motion[0];
+    oy = oy + E.motion[1];
+    oz = oz + E.motion[2];
+  }
+}
+
+__device__ __forceinline__ float ext_dist(const ExtractDev& E, float px, float py, float pz) {
+  float sx = 0.0f, sy = 0.0f;
+  if (E.field->n > 0) field_pick(E.field, px, py, pz, sx, sy);
+  return sx;
+}
+
+// reset (extract.ts:194-246): with motion and preserveMotion, the centre and mean velocity of
+// the body's current particles (per-thread strided sums, then a tree) become the motion.
+__global__ void __launch_bounds__(kExtractThreads) k_ext_reset(const ExtractDev* __restrict__ e) {
+  const ExtractDev& E = *e;
+  const uint32_t li = threadIdx.x;
+  if (li == 0) {
+    E.counters[0] = 0u;
+    E.counters[1] = 0u;
+  }
+  if (!E.has_motion) return;
+  __shared__ float s_sum[kExtractThreads][6];
+  const unsigned char* bd = E.bodies + static_cast<size_t>(E.body) * 64;
+  const uint32_t first = *reinterpret_cast<const uint32_t*>(bd + 12);
+  const uint32_t count = *reinterpret_cast<const uint32_t*>(bd + 44);
+  const bool keep = E.preserve != 0u;
+  float s[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  if (keep) {
+    for (uint32_t t = li; t < count; t += kExtractThreads) {
+      const float* p = reinterpret_cast<const float*>(E.particles + static_cast<size_t>(first + t) * 96);
+      s[0] = s[0] + p[0];
+      s[1] = s[1] + p[1];
+      s[2] = s[2] + p[2];
+      s[3] = s[3] + p[8];
+      s[4] = s[4] + p[9];
+      s[5] = s[5] + p[10];
+    }
+  }
+  for (int k = 0; k < 6; k++) s_sum[li][k] = s[k];
+  __syncthreads();
+  for (uint32_t h = kExtractThreads / 2; h > 0; h >>= 1) {
+    if (li < h)
+      for (int k = 0; k < 6; k++) s_sum[li][k] = s_sum[li][k] + s_sum[li + h][k];
+    __syncthreads();
+  }
+  if (li == 0 && keep && count > 0) {
+    const float inv = __fdiv_rn(1.0f, static_cast<float>(count));
+    for (int k = 0; k < 3; k++) {
+      E.motion[k] = s_sum[0][k] * inv;
+      E.motion[4 + k] = s_sum[0][3 + k] * inv;
+    }
+  }
+}
+
+// (crossing point * weight, weight) of one lattice edge (extract.ts:155-163); mix(a, b, t) is
+// a * (1 - t) + b * t.
+__device__ __forceinline__ void ext_cross(float ax, float ay, float az, float da, float bx, float by, float bz, float db,
+                                          float& sx, float& sy, float& sz, float& sw) {
+  float cx = 0.0f, cy = 0.0f, cz = 0.0f, cw = 0.0f;
+  if (!(da * db >= 0.0f)) {
+    const float t = clampf(__fdiv_rn(da, da - db), 0.0f, 1.0f);
+    const float u = 1.0f - t;
+    cx = ax * u + bx * t;
+    cy = ay * u + by * t;
+    cz = az * u + bz * t;
+    cw = 1.0f;
+  }
+  sx = sx + cx;
+  sy = sy + cy;
+  sz = sz + cz;
+  sw = sw + cw;
+}
+
+// cells (extract.ts:249-327): the dual vertex of every cell whose corners straddle the
+// surface, snapped onto it by one Lipschitz step; the block's count of vertices.
+__global__ void __launch_bounds__(kExtractThreads) k_ext_cells(const ExtractDev* __restrict__ e) {
+  const ExtractDev& E = *e;
+  const uint32_t R = static_cast<uint32_t>(E.res);
+  const uint32_t idx = blockIdx.x * kExtractThreads + threadIdx.x;
+  uint32_t has = 0;
+  if (idx < R * R * R) {
+    const uint32_t gx = idx % R, gy = (idx / R) % R, gz = idx / (R * R);
+    float ox, oy, oz;
+    ext_origin(E, ox, oy, oz);
+    const float c = E.cell;
+    const float x0 = ox + static_cast<float>(gx) * c, y0 = oy + static_cast<float>(gy) * c, z0 = oz + static_cast<float>(gz) * c;
+    const float x1 = x0 + c, y1 = y0 + c, z1 = z0 + c;
+    const float d0 = ext_dist(E, x0, y0, z0), dx = ext_dist(E, x1, y0, z0), dy = ext_dist(E, x0, y1, z0),
+                dz = ext_dist(E, x0, y0, z1), dxy = ext_dist(E, x1, y1, z0), dxz = ext_dist(E, x1, y0, z1),
+                dyz = ext_dist(E, x0, y1, z1), dxyz = ext_dist(E, x1, y1, z1);
+    float ax = 0.0f, ay = 0.0f, az = 0.0f, aw = 0.0f;
+    // the twelve edges in the reference's order
+    ext_cross(x0, y0, z0, d0, x1, y0, z0, dx, ax, ay, az, aw);
+    ext_cross(x0, y1, z0, dy, x1, y1, z0, dxy, ax, ay, az, aw);
+    ext_cross(x0, y0, z1, dz, x1, y0, z1, dxz, ax, ay, az, aw);
+    ext_cross(x0, y1, z1, dyz, x1, y1, z1, dxyz, ax, ay, az, aw);
+    ext_cross(x0, y0, z0, d0, x0, y1, z0, dy, ax, ay, az, aw);
+    ext_cross(x1, y0, z0, dx, x1, y1, z0, dxy, ax, ay, az, aw);
+    ext_cross(x0, y0, z1, dz, x0, y1, z1, dyz, ax, ay, az, aw);
+    ext_cross(x1, y0, z1, dxz, x1, y1, z1, dxyz, ax, ay, az, aw);
+    ext_cross(x0, y0, z0, d0, x0, y0, z1, dz, ax, ay, az, aw);
+    ext_cross(x1, y0, z0, dx, x1, y0, z1, dxz, ax, ay, az, aw);
+    ext_cross(x0, y1, z0, dy, x0, y1, z1, dyz, ax, ay, az, aw);
+    ext_cross(x1, y1, z0, dxy, x1, y1, z1, dxyz, ax, ay, az, aw);
+    float4 r0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), r1 = r0;
+    if (!(aw < 0.5f)) {
+      const float inv = __fdiv_rn(1.0f, aw);
+      const float vx = ax * inv, vy = ay * inv, vz = az * inv;
+      float nx = 0.0f, ny = 1.0f, nz = 0.0f, sv = 0.0f, sm = 0.0f;
+      int child = -1;
+      if (E.field->n > 0) {
+        child = field_pick(E.field, vx, vy, vz, sv, sm);
+        field_normal(E.field, child, vx, vy, vz, nx, ny, nz);
+      }
+      const float px = vx - nx * sv, py = vy - ny * sv, pz = vz - nz * sv;
+      float mat = 0.0f;
+      if (E.field->n > 0) {
+        float s0, s1;
+        const int ch = field_pick(E.field, px, py, pz, s0, s1);
+        mat = field_material(E.field, ch, px, py, pz);
+      }
+      r0 = make_float4(px, py, pz, mat);
+      r1 = make_float4(nx, ny, nz, 1.0f);
+      has = 1;
+    }
+    E.rec[2 * static_cast<size_t>(idx)] = r0;
+    E.rec[2 * static_cast<size_t>(idx) + 1] = r1;
+  }
+  uint32_t excl;
+  const uint32_t total = ext_block_scan(has, excl);
+  if (threadIdx.x == 0) E.blk[blockIdx.x] = total;
+}
+
+// Exclusive scan of the per-block counts of `which` (0: vertices, 1: quads) in one block,
+// and the grand total into the counter.
+__global__ void __launch_bounds__(1024) k_ext_scan(const ExtractDev* __restrict__ e, int which) {
+  const ExtractDev& E = *e;
+  uint32_t* a = which == 0 ? E.blk : E.qblk;
+  const uint32_t n = static_cast<uint32_t>(E.nblocks);
+  __shared__ uint32_t s_w[32];
+  __shared__ uint32_t s_carry;
+  if (threadIdx.x == 0) s_carry = 0u;
+  __syncthreads();
+  const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  for (uint32_t base = 0; base < n; base += 1024) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = i < n ? a[i] : 0u;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= static_cast<uint32_t>(o)) x += y;
+    }
+    if (lane == 31) s_w[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t t = s_w[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, t, o);
+        if (lane >= static_cast<uint32_t>(o)) t += y;
+      }
+      s_w[lane] = t;
+    }
+    __syncthreads();
+    const uint32_t carry = s_carry;
+    if (i < n) a[i] = carry + (wid > 0 ? s_w[wid - 1] : 0u) + x - v;
+    __syncthreads();
+    if (threadIdx.x == 0) s_carry = carry + s_w[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) E.counters[which] = s_carry;
+}
+
+// emit (extract.ts:306-326): the Particle records of the vertices in lattice order, the
+// biased ids of the cells; vertices past the slice's capacity are dropped (id 0).
+__global__ void __launch_bounds__(kExtractThreads) k_ext_emit(const ExtractDev* __restrict__ e) {
+  const ExtractDev& E = *e;
+  const uint32_t R = static_cast<uint32_t>(E.res);
+  const uint32_t idx = blockIdx.x * kExtractThreads + threadIdx.x;
+  const bool in = idx < R * R * R;
+  float4 r0 = make_float4(0.0f, 0.0f, 0.0f, 0.0f), r1 = r0;
+  if (in) {
+    r0 = E.rec[2 * static_cast<size_t>(idx)];
+    r1 = E.rec[2 * static_cast<size_t>(idx) + 1];
+  }
+  const uint32_t has = (in && r1.w > 0.5f) ? 1u : 0u;
+  uint32_t excl;
+  ext_block_scan(has, excl);
+  if (!in) return;
+  const uint32_t slot = E.blk[blockIdx.x] + excl;
+  if (!has || slot >= static_cast<uint32_t>(E.capacity)) {
+    E.id_grid[idx] = 0u;
+    return;
+  }
+  const uint32_t id = static_cast<uint32_t>(E.base) + slot;
+  float vx = E.vel[0], vy = E.vel[1], vz = E.vel[2];
+  if (E.has_motion) {
+    vx = E.motion[4];
+    vy = E.motion[5];
+    vz = E.motion[6];
+  }
+  float4* out = reinterpret_cast<float4*>(E.particles + static_cast<size_t>(id) * 96);
+  out[0] = make_float4(r0.x, r0.y, r0.z, __uint_as_float(static_cast<uint32_t>(E.body)));  // pos, body
+  out[1] = make_float4(r0.x, r0.y, r0.z, r0.w);                                            // prev, material
+  out[2] = make_float4(vx, vy, vz, 0.0f);                                                  // vel
+  out[3] = make_float4(vx, vy, vz, 0.0f);                                                  // velPrev
+  out[4] = make_float4(r0.x, r0.y, r0.z, 0.0f);                                            // rest
+  out[5] = make_float4(r1.x, r1.y, r1.z, 0.0f);                                            // restNormal
+  E.id_grid[idx] = id + 1u;
+}
+
+__device__ __forceinline__ uint32_t ext_id(const ExtractDev& E, uint32_t x, uint32_t y, uint32_t z) {
+  const uint32_t R = static_cast<uint32_t>(E.res);
+  return E.id_grid[x + R * (y + R * z)];
+}
+
+// The three quads a lattice point may own (extract.ts:352-392): for edge a (0: +x, 1: +y,
+// 2: +z) whose ends straddle the surface, the ids of the four cells around it in the
+// reference's order; all four must hold a vertex.
+__device__ __forceinline__ bool ext_quad(const ExtractDev& E, uint32_t i, uint32_t j, uint32_t k, int a, float dL, float lx,
+                                         float ly, float lz, uint32_t q[4]) {
+  const uint32_t hi = static_cast<uint32_t>(E.res) - 1u;
+  const float c = E.cell;
+  if (a == 0) {
+    if (!(j >= 1 && k >= 1 && j <= hi && k <= hi)) return false;
+    if (!(ext_dist(E, lx + c, ly + 0.0f, lz + 0.0f) * dL < 0.0f)) return false;
+    q[0] = ext_id(E, i, j - 1, k - 1);
+    q[1] = ext_id(E, i, j, k - 1);
+    q[2] = ext_id(E, i, j, k);
+    q[3] = ext_id(E, i, j - 1, k);
+  } else if (a == 1) {
+    if (!(i >= 1 && k >= 1 && i <= hi && k <= hi)) return false;
+    if (!(ext_dist(E, lx + 0.0f, ly + c, lz + 0.0f) * dL < 0.0f)) return false;
+    q[0] = ext_id(E, i - 1, j, k - 1);
+    q[1] = ext_id(E, i - 1, j, k);
+    q[2] = ext_id(E, i, j, k);
+    q[3] = ext_id(E, i, j, k - 1);
+  } else {
+    if (!(i >= 1 && j >= 1 && i <= hi && j <= hi)) return false;
+    if (!(ext_dist(E, lx + 0.0f, ly + 0.0f, lz + c) * dL < 0.0f)) return false;
+    q[0] = ext_id(E, i - 1, j - 1, k);
+    q[1] = ext_id(E, i, j - 1, k);
+    q[2] = ext_id(E, i, j, k);
+    q[3] = ext_id(E, i - 1, j, k);
+  }
+  return q[0] != 0u && q[1] != 0u && q[2] != 0u && q[3] != 0u;
+}
+
+// quads, pass 1: which of a lattice point's edges emit, and the block's count.
+__global__ void __launch_bounds__(kExtractThreads) k_ext_qcount(const ExtractDev* __restrict__ e) {
+  const ExtractDev& E = *e;
+  const uint32_t R = static_cast<uint32_t>(E.res);
+  const uint32_t idx = blockIdx.x * kExtractThreads + threadIdx.x;
+  uint32_t m = 0;
+  if (idx < R * R * R) {
+    const uint32_t i = idx % R, j = (idx / R) % R, k = idx / (R * R);
+    float ox, oy, oz;
+    ext_origin(E, ox, oy, oz);
+    const float c = E.cell;
+    const float lx = ox + static_cast<float>(i) * c, ly = oy + static_cast<float>(j) * c, lz = oz + static_cast<float>(k) * c;
+    const float dL = ext_dist(E, lx, ly, lz);
+    uint32_t q[4];
+    for (int a = 0; a < 3; a++)
+      if (ext_quad(E, i, j, k, a, dL, lx, ly, lz, q)) m |= 1u << a;
+    E.qmask[idx] = static_cast<unsigned char>(m);
+  }
+  uint32_t excl;
+  const uint32_t total = ext_block_scan(static_cast<uint32_t>(__popc(m)), excl);
+  if (threadIdx.x == 0) E.qblk[blockIdx.x] = total;
+}
+
+// quads, pass 2: six indices per quad (extract.ts:330-350), wound by the sign at the low end.
+__global__ void __launch_bounds__(kExtractThreads) k_ext_qemit(const ExtractDev* __restrict__ e) {
+  const ExtractDev& E = *e;
+  const uint32_t R = static_cast<uint32_t>(E.res);
+  const uint32_t idx = blockIdx.x * kExtractThreads + threadIdx.x;
+  const bool in = idx < R * R * R;
+  const uint32_t m = in ? static_cast<uint32_t>(E.qmask[idx]) : 0u;
+  uint32_t excl;
+  ext_block_scan(static_cast<uint32_t>(__popc(m)), excl);
+  if (!m) return;
+  const uint32_t i = idx % R, j = (idx / R) % R, k = idx / (R * R);
+  float ox, oy, oz;
+  ext_origin(E, ox, oy, oz);
+  const float c = E.cell;
+  const float lx = ox + static_cast<float>(i) * c, ly = oy + static_cast<float>(j) * c, lz = oz + static_cast<float>(k) * c;
+  const float dL = ext_dist(E, lx, ly, lz);
+  const bool flip = !(dL < 0.0f);
+  uint32_t slot = E.qblk[blockIdx.x] + excl;
+  for (int a = 0; a < 3; a++) {
+    if (!(m & (1u << a))) continue;
+    uint32_t q[4];
+    ext_quad(E, i, j, k, a, dL, lx, ly, lz, q);
+    if (slot < static_cast<uint32_t>(E.quad_cap)) {
+      uint32_t* o = E.indices + static_cast<size_t>(slot) * 6;
+      const uint32_t i0 = q[0] - 1u, i1 = (flip ? q[3] : q[1]) - 1u, i2 = q[2] - 1u, i3 = (flip ? q[1] : q[3]) - 1u;
+      o[0] = i0;
+      o[1] = i1;
+      o[2] = i2;
+      o[3] = i0;
+      o[4] = i2;
+      o[5] = i3;
+    }
+    slot++;
+  }
+}
+
+// finish (extract.ts:395-436): the body record (first, count, rest centre of mass, rotation
+// reset) and the draw arguments.
+__global__ void __launch_bounds__(kExtractThreads) k_ext_finish(const ExtractDev* __restrict__ e) {
+  const ExtractDev& E = *e;
+  const uint32_t li = threadIdx.x;
+  const uint32_t n = min(E.counters[0], static_cast<uint32_t>(E.capacity));
+  __shared__ float s_g[kExtractThreads][3];
+  float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+  for (uint32_t t = li; t < n; t += kExtractThreads) {
+    const float* p = reinterpret_cast<const float*>(E.particles + static_cast<size_t>(E.base + t) * 96 + 64);  // rest
+    sx = sx + p[0];
+    sy = sy + p[1];
+    sz = sz + p[2];
+  }
+  s_g[li][0] = sx;
+  s_g[li][1] = sy;
+  s_g[li][2] = sz;
+  __syncthreads();
+  for (uint32_t h = kExtractThreads / 2; h > 0; h >>= 1) {
+    if (li < h)
+      for (int k = 0; k < 3; k++) s_g[li][k] = s_g[li][k] + s_g[li + h][k];
+    __syncthreads();
+  }
+  if (li != 0) return;
+  const float inv = __fdiv_rn(1.0f, fmaxf(static_cast<float>(n), 1.0f));
+  const float cx = s_g[0][0] * inv, cy = s_g[0][1] * inv, cz = s_g[0][2] * inv;
+  unsigned char* bd = E.bodies + static_cast<size_t>(E.body) * 64;
+  float* f = reinterpret_cast<float*>(bd);
+  uint32_t* u = reinterpret_cast<uint32_t*>(bd);
+  u[3] = static_cast<uint32_t>(E.base);  // first
+  u[11] = n;                             // count
+  f[8] = cx;                             // restCom
+  f[9] = cy;
+  f[10] = cz;
+  f[0] = cx;                             // com
+  f[1] = cy;
+  f[2] = cz;
+  f[4] = 0.0f;                           // rot
+  f[5] = 0.0f;
+  f[6] = 0.0f;
+  f[7] = 1.0f;
+  const uint32_t q = min(E.counters[1], static_cast<uint32_t>(E.quad_cap));
+  E.draw_args[0] = q * 6u;
+  E.draw_args[1] = 1u;
+  E.draw_args[2] = 0u;
+  E.draw_args[3] = 0u;
 }
 
 // Gathers the ContactList of every scene of a batch into one array (one readback).

@@ -66,6 +66,21 @@ cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, 
 cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t st) {
   CLAY_LAUNCH(k_resolve, blocks, kResolveThreads, st, d, w);
 }
+cudaError_t L_ext_reset(const ExtractDev* e, cudaStream_t st) { CLAY_LAUNCH(k_ext_reset, 1, kExtractThreads, st, e); }
+cudaError_t L_ext_cells(const ExtractDev* e, int blocks, cudaStream_t st) {
+  CLAY_LAUNCH(k_ext_cells, blocks, kExtractThreads, st, e);
+}
+cudaError_t L_ext_scan(const ExtractDev* e, int which, cudaStream_t st) { CLAY_LAUNCH(k_ext_scan, 1, 1024, st, e, which); }
+cudaError_t L_ext_emit(const ExtractDev* e, int blocks, cudaStream_t st) {
+  CLAY_LAUNCH(k_ext_emit, blocks, kExtractThreads, st, e);
+}
+cudaError_t L_ext_qcount(const ExtractDev* e, int blocks, cudaStream_t st) {
+  CLAY_LAUNCH(k_ext_qcount, blocks, kExtractThreads, st, e);
+}
+cudaError_t L_ext_qemit(const ExtractDev* e, int blocks, cudaStream_t st) {
+  CLAY_LAUNCH(k_ext_qemit, blocks, kExtractThreads, st, e);
+}
+cudaError_t L_ext_finish(const ExtractDev* e, cudaStream_t st) { CLAY_LAUNCH(k_ext_finish, 1, kExtractThreads, st, e); }
 cudaError_t L_build(const BuildLevelDev& lv, const BrushDev* brushes, int n, cudaStream_t st) {
   dim3 g(lv.tiles, lv.tiles, lv.tiles);
   CLAY_LAUNCH(k_build, g, 256, st, lv, brushes, n);

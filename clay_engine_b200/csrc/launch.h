@@ -37,6 +37,14 @@ cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int thre
 // acc_voxels: size of the shared-memory minimum tile (dynamic shared memory, 4 B per voxel).
 cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, uint32_t acc_voxels, cudaStream_t st);
 cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t st);
+// SurfaceExtractor passes (grid passes: `blocks` blocks of kExtractThreads lattice cells).
+cudaError_t L_ext_reset(const ExtractDev* e, cudaStream_t st);
+cudaError_t L_ext_cells(const ExtractDev* e, int blocks, cudaStream_t st);
+cudaError_t L_ext_scan(const ExtractDev* e, int which, cudaStream_t st);
+cudaError_t L_ext_emit(const ExtractDev* e, int blocks, cudaStream_t st);
+cudaError_t L_ext_qcount(const ExtractDev* e, int blocks, cudaStream_t st);
+cudaError_t L_ext_qemit(const ExtractDev* e, int blocks, cudaStream_t st);
+cudaError_t L_ext_finish(const ExtractDev* e, cudaStream_t st);
 cudaError_t L_build(const BuildLevelDev& lv, const BrushDev* brushes, int n, cudaStream_t st);
 cudaError_t L_cell_index(const SceneDev* s, uint32_t* out, int n, cudaStream_t st);
 cudaError_t L_gather_contacts(const SceneDev* s, int n, ContactsDev* out, cudaStream_t st);

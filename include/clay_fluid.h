@@ -440,6 +440,54 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
 int clay_batch_launches_per_step(const clay_batch* b, int64_t* out);
 
 /* ------------------------------------------------------------------------------------
+ * SurfaceExtractor (lib/src/sim/extract.ts:84-484): naive surface nets of a field's zero
+ * level set on a res^3 lattice, written into a caller-owned ParticleSet: one 96-byte
+ * Particle record (particles.ts:18-34) per dual vertex in the slice [base, base+capacity),
+ * a quad index list (6 indices per quad, extract.ts:330-350), and the body record's first,
+ * count, rest centre of mass, centre of mass and rotation (64-byte Body, particles.ts:52-68)
+ * plus indirect draw arguments (extract.ts:395-436). Particle and quad slots come in lattice
+ * order (the reference's atomics leave the order unspecified).
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_extractor clay_extractor;
+#define CLAY_EXTRACT_RESOLUTION (1u << 0)
+typedef struct clay_extractor_opts {
+  uint32_t set;        /* CLAY_EXTRACT_RESOLUTION: `resolution` given, else 32 (extract.ts:99) */
+  int32_t resolution;  /* lattice cells per axis */
+  int32_t body;        /* body index in the set */
+  int32_t base;        /* first particle of this body's slice */
+  int32_t capacity;    /* particles the extractor may emit */
+  int32_t pad;
+  /* optional ExtractMotion (extract.ts:30-45): 8 device floats (centre xyz, pad, velocity
+   * xyz, pad), owned by the caller; the region is then relative to its centre, emitted
+   * particles take its velocity, and preserveMotion refreshes it from the live body */
+  float* motion;
+} clay_extractor_opts;
+/* `particles` (set_capacity records) and `bodies` (max_bodies records): device memory,
+ * 16-byte aligned, owned by the caller. The field must outlive the extractor. Refuses a
+ * slice past the set's capacity with the reference's message (extract.ts:101-103). */
+int clay_extractor_create(clay_ctx* ctx, const clay_field* field, void* particles, int64_t set_capacity, void* bodies,
+                          int32_t max_bodies, const clay_extractor_opts* opts, clay_extractor** out);
+void clay_extractor_destroy(clay_extractor* x);
+/* setRegion (extract.ts:451-463): cell = size / resolution; with motion, origin is relative
+ * to the motion's centre and preserve_motion snapshots the body's current centre and mean
+ * velocity into it at the next extraction. */
+int clay_extractor_set_region(clay_extractor* x, const double origin[3], double size, const double vel[3],
+                              int preserve_motion);
+/* extract (extract.ts:469-475): reset, cells, quads, finish, on `stream`. */
+int clay_extractor_extract(clay_extractor* x, void* stream);
+/* Device views: the quad index list (quad_capacity * 6 u32) and the 4 draw arguments. */
+int clay_extractor_views(clay_extractor* x, uint32_t** indices, uint32_t** draw_args, int64_t* quad_capacity);
+/* The extraction's dual-vertex and quad counts before the capacity clamps (SimCounters). */
+int clay_extractor_read_counts_async(clay_extractor* x, uint32_t* host_counts, void* stream);
+/* The quad index list (quad_capacity * 6 u32) and the 4 draw arguments, into host memory. */
+int clay_extractor_read_indices_async(clay_extractor* x, uint32_t* host_indices, uint32_t* host_draw_args, void* stream);
+/* offsetField(field, () => offset) with the offset read from device memory at every sample
+ * (trace/field.ts:396-429), e.g. an ExtractMotion's centre, so a body-local field follows
+ * the centre an extraction computes on the GPU. `device_offset`: 3 floats that must outlive
+ * the field. */
+int clay_field_offset_device(const clay_field* f, const float* device_offset, clay_field** out);
+
+/* ------------------------------------------------------------------------------------
  * Continuous-batching server (no reference counterpart: the reference steps the scenes of
  * one game). Serves requests "advance scene i by k frames" (each frame: FluidSim.step with
  * its bake) over many registered scenes. Each frame it launches one clay_batch_step_subset

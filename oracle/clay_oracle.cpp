@@ -137,9 +137,21 @@ struct VolU {
   T origin[3], voxel, extent, band, center[3], half;
   T grad_h;
   const uint16_t* dist;
+  const uint16_t* mat;
   T offset[3];
   bool has_offset;
+  T dyn[3];  // offset applied outermost, set by the extractor from its motion centre
+  bool has_dyn;
 };
+
+// offsetField (trace/field.ts:396-429): the outermost offset is subtracted first.
+template <class T>
+V3<T> leaf_point(const VolU<T>& u, V3<T> p) {
+  V3<T> q = p;
+  if (u.has_dyn) q = q - v3(u.dyn[0], u.dyn[1], u.dyn[2]);
+  if (u.has_offset) q = q - v3(u.offset[0], u.offset[1], u.offset[2]);
+  return q;
+}
 
 template <class T>
 VolU<T> make_volu(const orc_volume& v, const double* off) {
@@ -158,8 +170,11 @@ VolU<T> make_volu(const orc_volume& v, const double* off) {
   // gradient: h = voxelSize * gradScale, both f32 (volume.ts:299-302).
   u.grad_h = u.voxel * K<T>(v.gradient_voxels);
   u.dist = v.dist;
+  u.mat = v.mat;
   u.has_offset = false;
+  u.has_dyn = false;
   for (int k = 0; k < 3; k++) {
+    u.dyn[k] = T(0);
     u.offset[k] = off ? K<T>(off[k]) : T(0);
     if (off && off[k] != 0.0) u.has_offset = true;
   }
@@ -275,7 +290,7 @@ int field_pick(const FieldU<T>& f, V3<T> p, T out[2]) {
   T bs[2] = {T(0), T(0)};
   for (int i = 0; i < f.n; i++) {
     const VolU<T>& u = f.v[i];
-    V3<T> q = u.has_offset ? p - v3(u.offset[0], u.offset[1], u.offset[2]) : p;
+    V3<T> q = leaf_point(u, p);
     T s[2];
     vol_sample(u, q, s);
     if (best < 0 || !(bs[0] < s[0])) {
@@ -292,8 +307,20 @@ int field_pick(const FieldU<T>& f, V3<T> p, T out[2]) {
 template <class T>
 V3<T> field_normal(const FieldU<T>& f, V3<T> p, int child) {
   const VolU<T>& u = f.v[child];
-  V3<T> q = u.has_offset ? p - v3(u.offset[0], u.offset[1], u.offset[2]) : p;
-  return vol_normal(u, q);
+  return vol_normal(u, leaf_point(u, p));
+}
+
+// field(p, 0).y of the child field_pick chose (trace/field.ts:147-150,288-293,412-415,
+// volume.ts:288-296): the material plane, trilinear like the distance, 0 outside the box.
+template <class T>
+T field_material(const FieldU<T>& f, V3<T> p, int child) {
+  if (child < 0) return T(0);
+  VolU<T> u = f.v[child];
+  V3<T> q = leaf_point(u, p);
+  V3<T> c = v3(u.center[0], u.center[1], u.center[2]);
+  if (sd_box(q - c, v3(u.half, u.half, u.half)) > T(0)) return T(0);
+  u.dist = u.mat;
+  return trilinear(u, q);
 }
 
 // ----------------------------------------------------------------------------------------
@@ -1152,3 +1179,208 @@ void orc_build_brushes(const orc_volume* vol, const orc_brush* brushes, int32_t 
 }
 
 }  // extern "C"
+
+
+// ----------------------------------------------------------------------------------------
+// SurfaceExtractor.extract (sim/extract.ts:194-436) in f32, with the slot order of the CUDA
+// path: dual vertices in lattice order, quads by lattice point then +x, +y, +z edge (the
+// reference's atomics leave the order unspecified). Reductions follow the 256-thread
+// strided sums and tree of the reference's single-workgroup passes.
+namespace {
+constexpr int kThreads = 256;
+
+float ext_dist(const FieldU<float>& f, float x, float y, float z) {
+  float s[2] = {0.0f, 0.0f};
+  if (f.n > 0) field_pick(f, v3(x, y, z), s);
+  return s[0];
+}
+
+void ext_cross(float ax, float ay, float az, float da, float bx, float by, float bz, float db, float acc[4]) {
+  float cx = 0.0f, cy = 0.0f, cz = 0.0f, cw = 0.0f;
+  if (!(da * db >= 0.0f)) {
+    float t = da / (da - db);
+    t = std::min(std::max(t, 0.0f), 1.0f);
+    const float u = 1.0f - t;
+    cx = ax * u + bx * t;
+    cy = ay * u + by * t;
+    cz = az * u + bz * t;
+    cw = 1.0f;
+  }
+  acc[0] = acc[0] + cx;
+  acc[1] = acc[1] + cy;
+  acc[2] = acc[2] + cz;
+  acc[3] = acc[3] + cw;
+}
+}  // namespace
+
+void orc_extract(const orc_extract_cfg* cfg, const orc_field* field, float* motion, unsigned char* particles,
+                 unsigned char* bodies, uint32_t* indices, uint32_t* draw_args, uint32_t* counters, uint32_t* id_grid) {
+  FieldU<float> f = make_field<float>(field);
+  const int R = cfg->res;
+  const int64_t cells = static_cast<int64_t>(R) * R * R;
+  counters[0] = counters[1] = 0;
+  // reset
+  if (cfg->has_motion && motion) {
+    const unsigned char* bd = bodies + static_cast<size_t>(cfg->body) * 64;
+    uint32_t first, count;
+    std::memcpy(&first, bd + 12, 4);
+    std::memcpy(&count, bd + 44, 4);
+    const bool keep = cfg->preserve != 0;
+    std::vector<float> sum(static_cast<size_t>(kThreads) * 6, 0.0f);
+    if (keep)
+      for (int li = 0; li < kThreads; li++)
+        for (uint32_t t = li; t < count; t += kThreads) {
+          const float* p = reinterpret_cast<const float*>(particles + static_cast<size_t>(first + t) * 96);
+          for (int k = 0; k < 3; k++) {
+            sum[li * 6 + k] = sum[li * 6 + k] + p[k];
+            sum[li * 6 + 3 + k] = sum[li * 6 + 3 + k] + p[8 + k];
+          }
+        }
+    for (int h = kThreads / 2; h > 0; h >>= 1)
+      for (int li = 0; li < h; li++)
+        for (int k = 0; k < 6; k++) sum[li * 6 + k] = sum[li * 6 + k] + sum[(li + h) * 6 + k];
+    if (keep && count > 0) {
+      const float inv = 1.0f / static_cast<float>(count);
+      for (int k = 0; k < 3; k++) {
+        motion[k] = sum[k] * inv;
+        motion[4 + k] = sum[3 + k] * inv;
+      }
+    }
+  }
+  if (cfg->has_motion && motion && cfg->offset_by_motion)
+    for (int i = 0; i < f.n; i++) {
+      f.v[i].has_dyn = true;
+      for (int k = 0; k < 3; k++) f.v[i].dyn[k] = motion[k];
+    }
+  float ox = cfg->origin[0], oy = cfg->origin[1], oz = cfg->origin[2];
+  if (cfg->has_motion && motion) {
+    ox = ox + motion[0];
+    oy = oy + motion[1];
+    oz = oz + motion[2];
+  }
+  float vx = cfg->vel[0], vy = cfg->vel[1], vz = cfg->vel[2];
+  if (cfg->has_motion && motion) {
+    vx = motion[4];
+    vy = motion[5];
+    vz = motion[6];
+  }
+  const float c = cfg->cell;
+  // cells
+  uint32_t slot = 0;
+  for (int64_t idx = 0; idx < cells; idx++) {
+    const int gx = static_cast<int>(idx % R), gy = static_cast<int>((idx / R) % R), gz = static_cast<int>(idx / (static_cast<int64_t>(R) * R));
+    const float x0 = ox + static_cast<float>(gx) * c, y0 = oy + static_cast<float>(gy) * c, z0 = oz + static_cast<float>(gz) * c;
+    const float x1 = x0 + c, y1 = y0 + c, z1 = z0 + c;
+    const float d0 = ext_dist(f, x0, y0, z0), dx = ext_dist(f, x1, y0, z0), dy = ext_dist(f, x0, y1, z0),
+                dz = ext_dist(f, x0, y0, z1), dxy = ext_dist(f, x1, y1, z0), dxz = ext_dist(f, x1, y0, z1),
+                dyz = ext_dist(f, x0, y1, z1), dxyz = ext_dist(f, x1, y1, z1);
+    float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    ext_cross(x0, y0, z0, d0, x1, y0, z0, dx, acc);
+    ext_cross(x0, y1, z0, dy, x1, y1, z0, dxy, acc);
+    ext_cross(x0, y0, z1, dz, x1, y0, z1, dxz, acc);
+    ext_cross(x0, y1, z1, dyz, x1, y1, z1, dxyz, acc);
+    ext_cross(x0, y0, z0, d0, x0, y1, z0, dy, acc);
+    ext_cross(x1, y0, z0, dx, x1, y1, z0, dxy, acc);
+    ext_cross(x0, y0, z1, dz, x0, y1, z1, dyz, acc);
+    ext_cross(x1, y0, z1, dxz, x1, y1, z1, dxyz, acc);
+    ext_cross(x0, y0, z0, d0, x0, y0, z1, dz, acc);
+    ext_cross(x1, y0, z0, dx, x1, y0, z1, dxz, acc);
+    ext_cross(x0, y1, z0, dy, x0, y1, z1, dyz, acc);
+    ext_cross(x1, y1, z0, dxy, x1, y1, z1, dxyz, acc);
+    if (acc[3] < 0.5f) {
+      id_grid[idx] = 0;
+      continue;
+    }
+    counters[0]++;
+    const float inv = 1.0f / acc[3];
+    const V3<float> v = v3(acc[0] * inv, acc[1] * inv, acc[2] * inv);
+    float s[2] = {0.0f, 0.0f};
+    V3<float> n = v3(0.0f, 1.0f, 0.0f);
+    if (f.n > 0) {
+      const int child = field_pick(f, v, s);
+      n = field_normal(f, v, child);
+    }
+    const V3<float> p = v3(v.x - n.x * s[0], v.y - n.y * s[0], v.z - n.z * s[0]);
+    float mat = 0.0f;
+    if (f.n > 0) {
+      float s2[2];
+      const int ch = field_pick(f, p, s2);
+      mat = field_material(f, p, ch);
+    }
+    const uint32_t sl = slot++;
+    if (sl >= static_cast<uint32_t>(cfg->capacity)) {
+      id_grid[idx] = 0;
+      continue;
+    }
+    const uint32_t id = static_cast<uint32_t>(cfg->base) + sl;
+    float* out = reinterpret_cast<float*>(particles + static_cast<size_t>(id) * 96);
+    const uint32_t body = static_cast<uint32_t>(cfg->body);
+    float rec[24] = {p.x, p.y, p.z, 0.0f, p.x, p.y, p.z, mat, vx, vy, vz, 0.0f, vx, vy, vz, 0.0f,
+                     p.x, p.y, p.z, 0.0f, n.x, n.y, n.z, 0.0f};
+    std::memcpy(&rec[3], &body, 4);
+    std::memcpy(out, rec, sizeof(rec));
+    id_grid[idx] = id + 1;
+  }
+  // quads
+  const uint32_t hi = static_cast<uint32_t>(R) - 1u;
+  auto cid = [&](uint32_t x, uint32_t y, uint32_t z) {
+    return id_grid[x + static_cast<uint32_t>(R) * (y + static_cast<uint32_t>(R) * z)];
+  };
+  uint32_t qslot = 0;
+  for (int64_t idx = 0; idx < cells; idx++) {
+    const uint32_t i = static_cast<uint32_t>(idx % R), j = static_cast<uint32_t>((idx / R) % R),
+                   k = static_cast<uint32_t>(idx / (static_cast<int64_t>(R) * R));
+    const float lx = ox + static_cast<float>(i) * c, ly = oy + static_cast<float>(j) * c, lz = oz + static_cast<float>(k) * c;
+    const float dL = ext_dist(f, lx, ly, lz);
+    const bool flip = !(dL < 0.0f);
+    for (int a = 0; a < 3; a++) {
+      uint32_t q[4];
+      if (a == 0) {
+        if (!(j >= 1 && k >= 1 && j <= hi && k <= hi)) continue;
+        if (!(ext_dist(f, lx + c, ly + 0.0f, lz + 0.0f) * dL < 0.0f)) continue;
+        q[0] = cid(i, j - 1, k - 1), q[1] = cid(i, j, k - 1), q[2] = cid(i, j, k), q[3] = cid(i, j - 1, k);
+      } else if (a == 1) {
+        if (!(i >= 1 && k >= 1 && i <= hi && k <= hi)) continue;
+        if (!(ext_dist(f, lx + 0.0f, ly + c, lz + 0.0f) * dL < 0.0f)) continue;
+        q[0] = cid(i - 1, j, k - 1), q[1] = cid(i - 1, j, k), q[2] = cid(i, j, k), q[3] = cid(i, j, k - 1);
+      } else {
+        if (!(i >= 1 && j >= 1 && i <= hi && j <= hi)) continue;
+        if (!(ext_dist(f, lx + 0.0f, ly + 0.0f, lz + c) * dL < 0.0f)) continue;
+        q[0] = cid(i - 1, j - 1, k), q[1] = cid(i, j - 1, k), q[2] = cid(i, j, k), q[3] = cid(i - 1, j, k);
+      }
+      if (q[0] == 0 || q[1] == 0 || q[2] == 0 || q[3] == 0) continue;
+      counters[1]++;
+      const uint32_t qs = qslot++;
+      if (qs >= static_cast<uint32_t>(cfg->quad_cap)) continue;
+      uint32_t* o = indices + static_cast<size_t>(qs) * 6;
+      const uint32_t i0 = q[0] - 1, i1 = (flip ? q[3] : q[1]) - 1, i2 = q[2] - 1, i3 = (flip ? q[1] : q[3]) - 1;
+      o[0] = i0, o[1] = i1, o[2] = i2, o[3] = i0, o[4] = i2, o[5] = i3;
+    }
+  }
+  // finish
+  const uint32_t n = std::min(counters[0], static_cast<uint32_t>(cfg->capacity));
+  std::vector<float> g(static_cast<size_t>(kThreads) * 3, 0.0f);
+  for (int li = 0; li < kThreads; li++)
+    for (uint32_t t = li; t < n; t += kThreads) {
+      const float* p = reinterpret_cast<const float*>(particles + static_cast<size_t>(cfg->base + t) * 96 + 64);
+      for (int k = 0; k < 3; k++) g[li * 3 + k] = g[li * 3 + k] + p[k];
+    }
+  for (int h = kThreads / 2; h > 0; h >>= 1)
+    for (int li = 0; li < h; li++)
+      for (int k = 0; k < 3; k++) g[li * 3 + k] = g[li * 3 + k] + g[(li + h) * 3 + k];
+  const float inv = 1.0f / std::max(static_cast<float>(n), 1.0f);
+  const float com[3] = {g[0] * inv, g[1] * inv, g[2] * inv};
+  unsigned char* bd = bodies + static_cast<size_t>(cfg->body) * 64;
+  const uint32_t first = static_cast<uint32_t>(cfg->base);
+  const float rot[4] = {0.0f, 0.0f, 0.0f, 1.0f};
+  std::memcpy(bd + 0, com, 12);
+  std::memcpy(bd + 12, &first, 4);
+  std::memcpy(bd + 16, rot, 16);
+  std::memcpy(bd + 32, com, 12);
+  std::memcpy(bd + 44, &n, 4);
+  const uint32_t q = std::min(counters[1], static_cast<uint32_t>(cfg->quad_cap));
+  draw_args[0] = q * 6;
+  draw_args[1] = 1;
+  draw_args[2] = 0;
+  draw_args[3] = 0;
+}

@@ -183,6 +183,22 @@ void orc_eval_brush(const orc_brush* b, const float* pts, int32_t n, float* out)
 uint16_t orc_f32_to_f16(float f);
 float orc_f16_to_f32(uint16_t h);
 
+/* ---- sim/extract.ts: SurfaceExtractor.extract (f32) ---- */
+typedef struct orc_extract_cfg {
+  int32_t res, body, base, capacity, quad_cap, has_motion;
+  float origin[3];
+  float cell;
+  float vel[3];
+  uint32_t preserve;
+  int32_t offset_by_motion; /* the field's leaves follow the motion centre (offsetField) */
+  int32_t pad;
+} orc_extract_cfg;
+/* motion: 8 floats (centre, pad, velocity, pad), in/out, NULL without motion; particles and
+ * bodies: 96- and 64-byte records; indices: quad_cap * 6; draw_args[4]; counters[2];
+ * id_grid: res^3 (scratch, left holding the biased ids). */
+void orc_extract(const orc_extract_cfg* cfg, const orc_field* f, float* motion, unsigned char* particles,
+                 unsigned char* bodies, uint32_t* indices, uint32_t* draw_args, uint32_t* counters, uint32_t* id_grid);
+
 #ifdef __cplusplus
 }
 #endif

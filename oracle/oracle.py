@@ -8,6 +8,7 @@ forwards to the C++ restatement of the reference WGSL (see the header of
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 import subprocess
 
@@ -99,6 +100,14 @@ class SplatCfg(C.Structure):
     ]
 
 
+class ExtractCfg(C.Structure):
+    _fields_ = [
+        ("res", C.c_int32), ("body", C.c_int32), ("base", C.c_int32), ("capacity", C.c_int32),
+        ("quad_cap", C.c_int32), ("has_motion", C.c_int32), ("origin", C.c_float * 3), ("cell", C.c_float),
+        ("vel", C.c_float * 3), ("preserve", C.c_uint32), ("offset_by_motion", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
 BRUSH_DTYPE = np.dtype([
     ("pos", np.float32, 3), ("scale", np.float32), ("rot", np.float32, 4),
     ("size", np.float32, 3), ("radius", np.float32), ("material", np.float32),
@@ -153,6 +162,8 @@ def _declare(L):
     L.orc_splat_values_f64.argtypes = [C.POINTER(SplatCfg), C.POINTER(Cloud), f64p, C.c_int32]
     L.orc_build_brushes.argtypes = [C.POINTER(Volume), C.c_void_p, C.c_int32, u16p, u16p, C.c_int32]
     L.orc_eval_brush.argtypes = [C.c_void_p, f32p, C.c_int32, f32p]
+    L.orc_extract.argtypes = [C.POINTER(ExtractCfg), C.POINTER(Field), C.c_void_p, C.c_void_p, C.c_void_p, u32p,
+                              u32p, u32p, u32p]
 
 
 # ---------------------------------------------------------------------------------------
@@ -377,3 +388,24 @@ def eval_brush(brush: np.ndarray, pts) -> np.ndarray:
     out = np.zeros(len(pts), np.float32)
     lib().orc_eval_brush(b.ctypes.data, pts.ravel(), len(pts), out)
     return out
+
+
+def extract(field: Field, particles: np.ndarray, bodies: np.ndarray, res: int, body: int, base: int, capacity: int,
+            origin, size: float, vel=(0.0, 0.0, 0.0), motion: np.ndarray | None = None, preserve: bool = False,
+            offset_by_motion: bool = False):
+    """SurfaceExtractor.extract (sim/extract.ts:194-436) on the host, in place on the
+    ParticleSet records `particles` (96-byte) and `bodies` (64-byte); `motion` (8 float32,
+    in/out) with a motion-relative region. Returns (indices, draw_args, counters)."""
+    cfg = ExtractCfg(res=res, body=body, base=base, capacity=capacity, quad_cap=int(math.ceil(capacity * 1.5)),
+                     has_motion=1 if motion is not None else 0, cell=float(np.float32(size / res)),
+                     preserve=1 if preserve else 0, offset_by_motion=1 if offset_by_motion else 0)
+    cfg.origin[:] = [float(np.float32(x)) for x in origin]
+    cfg.vel[:] = [float(np.float32(x)) for x in vel]
+    assert particles.flags["C_CONTIGUOUS"] and bodies.flags["C_CONTIGUOUS"]
+    idx = np.zeros(cfg.quad_cap * 6, np.uint32)
+    draw = np.zeros(4, np.uint32)
+    cnt = np.zeros(2, np.uint32)
+    grid = np.zeros(res ** 3, np.uint32)
+    lib().orc_extract(C.byref(cfg), C.byref(field), None if motion is None else motion.ctypes.data,
+                      particles.ctypes.data, bodies.ctypes.data, idx, draw, cnt, grid)
+    return idx, draw, cnt
