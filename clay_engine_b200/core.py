@@ -175,6 +175,26 @@ class TracedField:
         check(lib().clay_field_query(self.handle, pts.ctypes.data, len(pts), s.ctypes.data, n.ctypes.data, None))
         return s, n
 
+    def query_mip(self, points: np.ndarray, mip: int):
+        """(sample(p, mip), field(p, mip)) as (x, y) pairs at host points, on the device."""
+        pts = np.ascontiguousarray(points, np.float32).reshape(-1, 3)
+        s = np.zeros((len(pts), 2), np.float32)
+        f = np.zeros((len(pts), 2), np.float32)
+        check(lib().clay_field_query_mip(self.handle, pts.ctypes.data, len(pts), int(mip), s.ctypes.data,
+                                         f.ctypes.data, None))
+        return s, f
+
+    def bandWorld(self, mip: int) -> float:
+        return self._band_voxel(mip)[0]
+
+    def voxelWorld(self, mip: int) -> float:
+        return self._band_voxel(mip)[1]
+
+    def _band_voxel(self, mip):
+        b, v = C.c_float(), C.c_float()
+        check(lib().clay_field_band_voxel(self.handle, int(mip), C.byref(b), C.byref(v)))
+        return float(b.value), float(v.value)
+
     def setOffset(self, offset):
         check(lib().clay_field_set_offset(self.handle, *[float(x) for x in offset]))
 

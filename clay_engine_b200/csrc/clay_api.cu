@@ -146,6 +146,7 @@ struct clay_volume {
       h.center[k] = static_cast<float>(origin[k] + half);
     }
     h.voxel = static_cast<float>(world / res);
+    h.mips = mips;
     h.extent = static_cast<float>(world);
     h.half = static_cast<float>(half);
     h.band = static_cast<float>(band);
@@ -733,6 +734,49 @@ int clay_field_set_offset(clay_field* f, double dx, double dy, double dz) {
 }
 
 void clay_field_destroy(clay_field* f) { free_field(f); }
+
+int clay_field_query_mip(const clay_field* f, const float* pts, int n, int mip, float* sample_xy, float* field_xy,
+                         void* stream) {
+  if (!f || n < 0 || (n > 0 && (!pts || !sample_xy || !field_xy)))
+    return fail(CLAY_EINVAL, "clay_field_query_mip: bad argument");
+  if (mip < 0) return fail(CLAY_EINVAL, "clay_field_query_mip: mip %d < 0", mip);
+  if (n == 0) return CLAY_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = const_cast<clay_field*>(f)->flush(s);
+  if (rc) return rc;
+  float *dp = nullptr, *ds = nullptr, *df = nullptr;
+  CK(cudaMalloc(&dp, sizeof(float) * 3 * n));
+  CK(cudaMalloc(&ds, sizeof(float) * 2 * n));
+  CK(cudaMalloc(&df, sizeof(float) * 2 * n));
+  CK(cudaMemcpyAsync(dp, pts, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
+  CK(L_field_query_mip(f->d, dp, n, mip, ds, df, s));
+  CK(cudaMemcpyAsync(sample_xy, ds, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(field_xy, df, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  cudaFree(dp);
+  cudaFree(ds);
+  cudaFree(df);
+  return CLAY_OK;
+}
+
+int clay_field_band_voxel(const clay_field* f, int mip, float* band_world, float* voxel_world) {
+  if (!f || !band_world || !voxel_world || mip < 0) return fail(CLAY_EINVAL, "clay_field_band_voxel: bad argument");
+  if (f->leaves.empty()) return fail(CLAY_ESTATE, "clay_field_band_voxel: empty field");
+  float bw = 0.0f, vw = 0.0f;
+  for (size_t i = 0; i < f->leaves.size(); i++) {
+    const VolParamsDev& h = f->leaves[i].vol->h;
+    const float m = std::min(static_cast<float>(mip), static_cast<float>(h.mips - 1));  // capped
+    const float p2 = std::ldexp(1.0f, static_cast<int>(m));  // exp2 of an integer level
+    const float b = (h.band * h.voxel) * p2;
+    const float v = h.voxel * p2;
+    // unionField: min of the bands, max of the voxels (trace/field.ts:294-305)
+    bw = i == 0 ? b : std::min(bw, b);
+    vw = i == 0 ? v : std::max(vw, v);
+  }
+  *band_world = bw;
+  *voxel_world = vw;
+  return CLAY_OK;
+}
 
 int clay_field_query(const clay_field* f, const float* pts, int n, float* sxy, float* nrm, void* stream) {
   if (!f || n < 0 || (n > 0 && (!pts || !sxy || !nrm))) return fail(CLAY_EINVAL, "clay_field_query: bad argument");

@@ -65,7 +65,9 @@ struct __align__(16) VolParamsDev {
   float band;
   float grad_h;
   int32_t res;
-  const __half* dist;  // mip 0 plane
+  int32_t mips;
+  int32_t pad_;
+  const __half* dist;  // level 0 plane; level m follows at the sum of the finer levels' sizes
   const __half* mat;
 };
 
@@ -391,6 +393,70 @@ __device__ __forceinline__ float field_material(const FieldDev* f, int child, fl
   if (sd_box(qx - v.cx, qy - v.cy, qz - v.cz, v.half) > 0.0f) return 0.0f;
   v.dist = lf.vp->mat;
   return trilinear(v, qx, qy, qz);
+}
+
+// Level m of a volume, capped at its top level (trace/field.ts:117-124): the plane offset,
+// the side, and bandWorld(m) = band * voxelSize * exp2(m) (volume.ts:269-272).
+__device__ __forceinline__ int vol_level(const VolParamsDev* vp, int mip, size_t& off, int& R, float& bw) {
+  const int m = min(max(mip, 0), vp->mips - 1);
+  off = 0;
+  for (int l = 0; l < m; l++) {
+    const size_t r = static_cast<size_t>(vp->res >> l);
+    off += r * r * r;
+  }
+  R = vp->res >> m;
+  bw = (vp->band * vp->voxel) * ldexpf(1.0f, m);  // exp2 of an integer level: exactly 2^m
+  return m;
+}
+
+// volumeField.sample(p, mip) (trace/field.ts:135-146) and field(p, mip) (:147-150,
+// volume.ts:288-296) of one leaf: (dBox, 1) / (dBox, 0) outside the box, else
+// (raw * bandWorld, raw) / (raw * bandWorld, material) from level m's texels.
+__device__ __forceinline__ void leaf_sample_mip(const LeafDev& lf, float px, float py, float pz, int mip, float& sx,
+                                                float& sy, float& fy) {
+  Vol v = load_vol(lf.vp);
+  float qx, qy, qz;
+  leaf_point(lf, px, py, pz, qx, qy, qz);
+  const float dbox = sd_box(qx - v.cx, qy - v.cy, qz - v.cz, v.half);
+  if (dbox > 0.0f) {
+    sx = dbox;
+    sy = 1.0f;
+    fy = 0.0f;
+    return;
+  }
+  size_t off;
+  int R;
+  float bw;
+  vol_level(lf.vp, mip, off, R, bw);
+  v.res = R;
+  v.dist = lf.vp->dist + off;
+  const float raw = trilinear(v, qx, qy, qz);
+  v.dist = lf.vp->mat + off;
+  fy = trilinear(v, qx, qy, qz);
+  sx = raw * bw;
+  sy = raw;
+}
+
+// unionField.sample / field (trace/field.ts:264-293): the pair of the nearer child (the
+// later one on ties); both pick the same child, their x being the same distance.
+__device__ __forceinline__ void field_sample_mip(const FieldDev* f, float px, float py, float pz, int mip, float& sx,
+                                                 float& sy, float& fx, float& fy) {
+  int best = -1;
+  float bx = 0.0f, by = 0.0f, bf = 0.0f;
+  for (int i = 0; i < f->n; i++) {
+    float a, b, c;
+    leaf_sample_mip(f->leaf[i], px, py, pz, mip, a, b, c);
+    if (best < 0 || !(bx < a)) {
+      best = i;
+      bx = a;
+      by = b;
+      bf = c;
+    }
+  }
+  sx = bx;
+  sy = by;
+  fx = bx;
+  fy = bf;
 }
 
 // ---------------------------------------------------------------------------------------
@@ -2162,6 +2228,19 @@ __global__ void k_field_query(const FieldDev* __restrict__ f, const float* __res
   nrm[3 * i] = nx;
   nrm[3 * i + 1] = ny;
   nrm[3 * i + 2] = nz;
+}
+
+// Collider query at a level: sample(p, mip) and field(p, mip) at n points.
+__global__ void k_field_query_mip(const FieldDev* __restrict__ f, const float* __restrict__ pts, int n, int mip,
+                                  float* __restrict__ sxy, float* __restrict__ fxy) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float sx = 0.0f, sy = 0.0f, fx = 0.0f, fy = 0.0f;
+  if (f->n > 0) field_sample_mip(f, pts[3 * i], pts[3 * i + 1], pts[3 * i + 2], mip, sx, sy, fx, fy);
+  sxy[2 * i] = sx;
+  sxy[2 * i + 1] = sy;
+  fxy[2 * i] = fx;
+  fxy[2 * i + 1] = fy;
 }
 
 #endif  // CLAY_ONLY_NEIGHBOUR_PASSES

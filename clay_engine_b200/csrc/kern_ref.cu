@@ -66,6 +66,9 @@ cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, 
 cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t st) {
   CLAY_LAUNCH(k_resolve, blocks, kResolveThreads, st, d, w);
 }
+cudaError_t L_field_query_mip(const FieldDev* f, const float* pts, int n, int mip, float* sxy, float* fxy, cudaStream_t st) {
+  CLAY_LAUNCH(k_field_query_mip, (n + 255) / 256, 256, st, f, pts, n, mip, sxy, fxy);
+}
 cudaError_t L_ext_reset(const ExtractDev* e, cudaStream_t st) { CLAY_LAUNCH(k_ext_reset, 1, kExtractThreads, st, e); }
 cudaError_t L_ext_cells(const ExtractDev* e, int blocks, cudaStream_t st) {
   CLAY_LAUNCH(k_ext_cells, blocks, kExtractThreads, st, e);

@@ -161,6 +161,14 @@ void clay_field_destroy(clay_field* f);
  * All pointers are host memory; the call synchronises `stream`. */
 int clay_field_query(const clay_field* f, const float* points_xyz, int n, float* sample_xy,
                      float* nrm, void* stream);
+/* TracedField.sample(p, mip) and field(p, mip) (trace/field.ts:135-150, 264-293, 396-415)
+ * at n host points, the level capped at each volume's top level (:117-124): per point the
+ * (distance, raw) and (distance, material) pairs. Test and tool hook (allocates). */
+int clay_field_query_mip(const clay_field* f, const float* pts, int n, int mip, float* sample_xy, float* field_xy,
+                         void* stream);
+/* bandWorld(mip) and voxelWorld(mip) of the field (trace/field.ts:151-155, 294-305): the
+ * smallest band and the largest voxel over the union's volumes, each at its capped level. */
+int clay_field_band_voxel(const clay_field* f, int mip, float* band_world, float* voxel_world);
 
 /* ------------------------------------------------------------------------------------
  * ParticleCloud (lib/src/sim/splat.ts:15-38) and bodyCloud (splat.ts:47-72).

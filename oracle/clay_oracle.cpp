@@ -1182,6 +1182,62 @@ void orc_build_brushes(const orc_volume* vol, const orc_brush* brushes, int32_t 
 
 
 // ----------------------------------------------------------------------------------------
+// volumeField.sample(p, mip) / field(p, mip) (trace/field.ts:117-150, volume.ts:262-296) with
+// the level capped at the volume's top level, and their union / offset composition
+// (:264-293, :396-415). Level m: side res >> m, planes after the finer levels, bandWorld(m) =
+// band * voxelSize * 2^m.
+namespace {
+template <class T>
+void leaf_sample_mip(const VolU<T>& u0, V3<T> p, int mip, T out[3]) {
+  VolU<T> u = u0;
+  V3<T> q = leaf_point(u, p);
+  V3<T> c = v3(u.center[0], u.center[1], u.center[2]);
+  T dbox = sd_box(q - c, v3(u.half, u.half, u.half));
+  if (dbox > T(0)) {
+    out[0] = dbox;
+    out[1] = T(1);
+    out[2] = T(0);
+    return;
+  }
+  const int m = std::min(std::max(mip, 0), u.mips - 1);
+  size_t off = 0;
+  for (int l = 0; l < m; l++) {
+    const size_t r = static_cast<size_t>(u.res >> l);
+    off += r * r * r;
+  }
+  const uint16_t* dist = u.dist;
+  const uint16_t* mat = u.mat;
+  u.res = u0.res >> m;
+  u.dist = dist + off;
+  const T raw = trilinear(u, q);
+  u.dist = mat + off;
+  const T material = trilinear(u, q);
+  const T bw = (u.band * u.voxel) * std::ldexp(T(1), m);
+  out[0] = raw * bw;
+  out[1] = raw;
+  out[2] = material;
+}
+}  // namespace
+
+void orc_field_query_mip_f32(const orc_field* f, const float p[3], int mip, float sample_xy[2], float field_xy[2]) {
+  FieldU<float> fu = make_field<float>(f);
+  float best[3] = {0.0f, 0.0f, 0.0f};
+  for (int i = 0; i < fu.n; i++) {
+    float o[3];
+    leaf_sample_mip(fu.v[i], v3(p[0], p[1], p[2]), mip, o);
+    if (i == 0 || !(best[0] < o[0])) {
+      best[0] = o[0];
+      best[1] = o[1];
+      best[2] = o[2];
+    }
+  }
+  sample_xy[0] = best[0];
+  sample_xy[1] = best[1];
+  field_xy[0] = best[0];
+  field_xy[1] = best[2];
+}
+
+// ----------------------------------------------------------------------------------------
 // SurfaceExtractor.extract (sim/extract.ts:194-436) in f32, with the slot order of the CUDA
 // path: dual vertices in lattice order, quads by lattice point then +x, +y, +z edge (the
 // reference's atomics leave the order unspecified). Reductions follow the 256-thread

@@ -183,6 +183,9 @@ void orc_eval_brush(const orc_brush* b, const float* pts, int32_t n, float* out)
 uint16_t orc_f32_to_f16(float f);
 float orc_f16_to_f32(uint16_t h);
 
+/* ---- trace/field.ts: sample(p, mip) and field(p, mip), level capped (f32) ---- */
+void orc_field_query_mip_f32(const orc_field* f, const float p[3], int mip, float sample_xy[2], float field_xy[2]);
+
 /* ---- sim/extract.ts: SurfaceExtractor.extract (f32) ---- */
 typedef struct orc_extract_cfg {
   int32_t res, body, base, capacity, quad_cap, has_motion;

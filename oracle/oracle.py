@@ -162,6 +162,7 @@ def _declare(L):
     L.orc_splat_values_f64.argtypes = [C.POINTER(SplatCfg), C.POINTER(Cloud), f64p, C.c_int32]
     L.orc_build_brushes.argtypes = [C.POINTER(Volume), C.c_void_p, C.c_int32, u16p, u16p, C.c_int32]
     L.orc_eval_brush.argtypes = [C.c_void_p, f32p, C.c_int32, f32p]
+    L.orc_field_query_mip_f32.argtypes = [C.POINTER(Field), f32p, C.c_int32, f32p, f32p]
     L.orc_extract.argtypes = [C.POINTER(ExtractCfg), C.POINTER(Field), C.c_void_p, C.c_void_p, C.c_void_p, u32p,
                               u32p, u32p, u32p]
 
@@ -238,6 +239,18 @@ def field_query_f32(field: Field, pts: np.ndarray):
         lib().orc_field_query_f32(C.byref(field), np.ascontiguousarray(p), o2, o3)
         s[i], n[i] = o2, o3
     return s, n
+
+
+def field_query_mip_f32(field: Field, pts: np.ndarray, mip: int):
+    """sample(p, mip) and field(p, mip) at each point: two (n, 2) float32 arrays."""
+    pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+    s = np.zeros((len(pts), 2), np.float32)
+    f = np.zeros((len(pts), 2), np.float32)
+    o2, o2b = np.zeros(2, np.float32), np.zeros(2, np.float32)
+    for i, p in enumerate(pts):
+        lib().orc_field_query_mip_f32(C.byref(field), np.ascontiguousarray(p), int(mip), o2, o2b)
+        s[i], f[i] = o2, o2b
+    return s, f
 
 
 def fluid_cfg(**kw) -> FluidCfg:
