@@ -6,11 +6,11 @@ The compute runs in ``_build/libclayfluid.so`` (C ABI: ``include/clay_fluid.h``)
 package is the host-side mirror of the reference's classes. There is no CPU fallback.
 """
 from ._native import ClayError
-from .core import (PARTICLE_DTYPE, Batch, FluidSim, ParticleCloud, Root, SdfVolume, SplatField, SurfaceExtractor,
+from .core import (PARTICLE_DTYPE, Batch, ClaySolver, FluidSim, ParticleCloud, Root, SdfVolume, SplatField, SurfaceExtractor,
                    TracedField,
                    bodyCloud, init, kernel_launch_count, motion_buffer, offsetField, offsetFieldDevice, unionField,
                    volumeField)
 
-__all__ = ["ClayError", "PARTICLE_DTYPE", "Batch", "FluidSim", "ParticleCloud", "Root", "SdfVolume",
+__all__ = ["ClayError", "PARTICLE_DTYPE", "Batch", "ClaySolver", "FluidSim", "ParticleCloud", "Root", "SdfVolume",
            "SplatField", "SurfaceExtractor", "TracedField", "bodyCloud", "init", "kernel_launch_count", "motion_buffer", "offsetField", "offsetFieldDevice",
            "unionField", "volumeField"]

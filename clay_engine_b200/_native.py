@@ -117,6 +117,16 @@ class ExtractorOpts(C.Structure):
 CLAY_EXTRACT_RESOLUTION = 1
 
 
+class SolverOpts(C.Structure):
+    _fields_ = [("set", C.c_uint32), ("substeps", C.c_int32), ("gravity", C.c_double * 3), ("dt", C.c_double),
+                ("radius", C.c_double), ("friction", C.c_double), ("damping", C.c_double), ("max_speed", C.c_double),
+                ("rotation_iterations", C.c_int32), ("pad", C.c_int32)]
+
+
+SOLVER = {"gravity": 1, "dt": 2, "substeps": 4, "radius": 8, "friction": 16, "damping": 32, "maxSpeed": 64,
+          "rotationIterations": 128}
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("budget_bytes", C.c_uint64), ("depth", C.c_int32), ("max_batch", C.c_int32),
                 ("mode", C.c_int32), ("sph_block", C.c_int32)]
@@ -212,6 +222,10 @@ SIGNATURES = {
     "clay_extractor_read_counts_async": (I, [P, P, P]),
     "clay_extractor_read_indices_async": (I, [P, P, P, P]),
     "clay_field_offset_device": (I, [P, P, C.POINTER(P)]),
+    "clay_solver_create": (I, [P, P, P, C.c_int64, P, C.c_int32, C.POINTER(SolverOpts), C.POINTER(P)]),
+    "clay_solver_destroy": (None, [P]),
+    "clay_solver_set_force": (I, [P, C.c_uint32, C.POINTER(D), C.POINTER(D)]),
+    "clay_solver_step": (I, [P, C.c_int32, P]),
     "clay_kernel_launch_count": (C.c_uint64, []),
 }
 

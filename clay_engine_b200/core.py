@@ -299,6 +299,46 @@ class SurfaceExtractor:
         self.handle = None
 
 
+class ClaySolver:
+    """`ClaySolver` (sim/pbd.ts:78-424) over a ParticleSet held by the caller as device memory
+    (96-byte Particle records and 64-byte Body records), colliding against `world`. Options by
+    the reference's names: gravity, dt, substeps, radius, friction, damping, maxSpeed,
+    rotationIterations."""
+
+    def __init__(self, root: Root, particles, capacity: int, bodies, max_bodies: int, world: TracedField,
+                 options: dict | None = None):
+        o = N.SolverOpts()
+        for key, val in (options or {}).items():
+            if key not in N.SOLVER:
+                raise ClayError(N.CLAY_EINVAL, f"ClaySolver: unknown option '{key}'")
+            o.set |= N.SOLVER[key]
+            if key == "gravity":
+                o.gravity[:] = [float(x) for x in val]
+            elif key in ("substeps", "rotationIterations"):
+                setattr(o, "substeps" if key == "substeps" else "rotation_iterations", int(val))
+            else:
+                setattr(o, {"maxSpeed": "max_speed"}.get(key, key), float(val))
+        h = C.c_void_p()
+        check(lib().clay_solver_create(root.handle, world.handle, _dev_ptr(particles), int(capacity),
+                                       _dev_ptr(bodies), int(max_bodies), C.byref(o), C.byref(h)))
+        self.handle = h.value
+        self.world = world
+        self._keep = (particles, bodies)
+
+    def setForce(self, body: int, accel, impulse=(0.0, 0.0, 0.0)):
+        a = (C.c_double * 3)(*[float(x) for x in accel])
+        i = (C.c_double * 3)(*[float(x) for x in impulse])
+        check(lib().clay_solver_set_force(self.handle, int(body) & 0xFFFFFFFF, a, i))
+
+    def step(self, body_count: int, pass_=None):
+        check(lib().clay_solver_step(self.handle, int(body_count), stream_handle(pass_)))
+
+    def destroy(self):
+        if self.handle:
+            lib().clay_solver_destroy(self.handle)
+        self.handle = None
+
+
 @dataclass
 class ParticleCloud:
     """`ParticleCloud` (splat.ts:15-38) as device arrays.

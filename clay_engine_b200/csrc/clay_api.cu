@@ -1992,3 +1992,120 @@ int clay_field_offset_device(const clay_field* f, const float* device_offset, cl
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------------------------------
+// ClaySolver (pbd.ts:78-424).
+struct clay_solver {
+  clay_ctx* ctx = nullptr;
+  const clay_field* world = nullptr;
+  SolveDev h{};
+  SolveDev* d = nullptr;
+  int substeps = 2;
+  bool dirty = true;
+  bool kicking = false;
+};
+
+extern "C" {
+
+int clay_solver_create(clay_ctx* ctx, const clay_field* world, void* particles, int64_t capacity, void* bodies,
+                       int32_t max_bodies, const clay_solver_opts* opts, clay_solver** out) {
+  if (!ctx || !world || !particles || !bodies || !out) return fail(CLAY_EINVAL, "clay_solver_create: NULL argument");
+  if (world->ctx != ctx) return fail(CLAY_EINVAL, "ClaySolver: the world field belongs to another context");
+  if (world->leaves.empty()) return fail(CLAY_EINVAL, "ClaySolver: the world field has no volume");
+  if (capacity <= 0 || capacity > (1ll << 30) || max_bodies <= 0)
+    return fail(CLAY_EINVAL, "ClaySolver: capacity and max_bodies must be positive");
+  if ((reinterpret_cast<uintptr_t>(particles) & 15) || (reinterpret_cast<uintptr_t>(bodies) & 15))
+    return fail(CLAY_EINVAL, "ClaySolver: particle and body buffers must be 16-byte aligned");
+  clay_solver_opts o{};
+  if (opts) o = *opts;
+  // ClaySolverOptions defaults (pbd.ts:101-118)
+  const double dt = (o.set & CLAY_SOLVER_DT) ? o.dt : 1.0 / 60;
+  const int substeps = (o.set & CLAY_SOLVER_SUBSTEPS) ? o.substeps : 2;
+  const int iters = (o.set & CLAY_SOLVER_ROTATION_ITERATIONS) ? o.rotation_iterations : 2;
+  if (!(dt > 0) || substeps < 1 || iters < 0) return fail(CLAY_EINVAL, "ClaySolver: dt > 0, substeps >= 1, iterations >= 0");
+  clay_solver* sv = new clay_solver();
+  sv->ctx = ctx;
+  sv->world = world;
+  sv->substeps = substeps;
+  SolveDev& h = sv->h;
+  h.particles = static_cast<unsigned char*>(particles);
+  h.bodies = static_cast<unsigned char*>(bodies);
+  double g[3] = {0, -9.81, 0};
+  if (o.set & CLAY_SOLVER_GRAVITY)
+    for (int k = 0; k < 3; k++) g[k] = o.gravity[k];
+  for (int k = 0; k < 3; k++) {
+    h.gravity[k] = static_cast<float>(g[k]);
+    h.push[k] = 0.0f;
+    h.kick[k] = 0.0f;
+  }
+  h.h = static_cast<float>(dt / substeps);
+  h.radius = static_cast<float>((o.set & CLAY_SOLVER_RADIUS) ? o.radius : 0.1);
+  h.friction = static_cast<float>((o.set & CLAY_SOLVER_FRICTION) ? o.friction : 0.35);
+  h.damping = static_cast<float>((o.set & CLAY_SOLVER_DAMPING) ? o.damping : 0.995);
+  h.max_speed = static_cast<float>((o.set & CLAY_SOLVER_MAX_SPEED) ? o.max_speed : 40);
+  h.push_body = 0xffffffffu;
+  h.capacity = static_cast<int32_t>(capacity);
+  h.max_bodies = max_bodies;
+  h.rot_iters = iters;
+  void* p = nullptr;
+  int rc = ctx->dev_alloc(&p, sizeof(SolveDev));
+  if (rc) {
+    delete sv;
+    return rc;
+  }
+  sv->d = static_cast<SolveDev*>(p);
+  *out = sv;
+  return CLAY_OK;
+}
+
+void clay_solver_destroy(clay_solver* sv) {
+  if (!sv) return;
+  sv->ctx->dev_free(sv->d, sizeof(SolveDev));
+  delete sv;
+}
+
+int clay_solver_set_force(clay_solver* sv, uint32_t body, const double accel[3], const double impulse[3]) {
+  if (!sv || !accel) return fail(CLAY_EINVAL, "clay_solver_set_force: NULL argument");
+  bool kick = false;
+  for (int k = 0; k < 3; k++) {
+    sv->h.push[k] = static_cast<float>(accel[k]);
+    sv->h.kick[k] = impulse ? static_cast<float>(impulse[k]) : 0.0f;
+    kick = kick || (impulse && impulse[k] != 0.0);
+  }
+  sv->h.push_body = body;
+  sv->kicking = kick;
+  sv->dirty = true;
+  return CLAY_OK;
+}
+
+int clay_solver_step(clay_solver* sv, int32_t body_count, void* stream) {
+  if (!sv) return fail(CLAY_EINVAL, "clay_solver_step: NULL solver");
+  if (body_count < 0 || body_count > sv->h.max_bodies)
+    return fail(CLAY_EINVAL, "clay_solver_step: body count %d outside 0..%d", body_count, sv->h.max_bodies);
+  if (body_count == 0) return CLAY_OK;  // pbd.ts:401-404
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = const_cast<clay_field*>(sv->world)->flush(s);
+  if (rc) return rc;
+  if (sv->h.world != sv->world->d) {  // the field rebuilt its device table
+    sv->h.world = sv->world->d;
+    sv->dirty = true;
+  }
+  if (sv->dirty) {
+    if ((rc = sv->ctx->upload(sv->d, &sv->h, sizeof(SolveDev), s))) return rc;
+    sv->dirty = false;
+  }
+  const int blocks = (sv->h.capacity + kSolveThreads - 1) / kSolveThreads;
+  if (sv->kicking) {
+    CK(L_pbd_kick(sv->d, blocks, s));
+    sv->kicking = false;
+  }
+  for (int sub = 0; sub < sv->substeps; sub++) {
+    CK(L_pbd_predict(sv->d, blocks, s));
+    CK(L_pbd_match(sv->d, body_count, s));
+    CK(L_pbd_apply(sv->d, blocks, s));
+    CK(L_pbd_finalize(sv->d, blocks, s));
+  }
+  return CLAY_OK;
+}
+
+}  // extern "C"

@@ -194,6 +194,24 @@ struct __align__(16) ExtractDev {
 };
 constexpr int kExtractThreads = 256;  // cells (lattice points) per block of the grid passes
 
+// A ClaySolver (sim/pbd.ts:78-424) as the kernels see it: the caller's ParticleSet records,
+// the world field and the SolveParams uniform (pbd.ts:12-41).
+struct __align__(16) SolveDev {
+  unsigned char* particles;
+  unsigned char* bodies;
+  const FieldDev* world;
+  float gravity[3];
+  float h;  // substep length
+  float radius, friction, damping, max_speed;
+  float push[3];
+  uint32_t push_body;
+  float kick[3];
+  int32_t capacity, max_bodies, rot_iters, pad_;
+};
+constexpr int kSolveThreads = 64;    // particle passes (pbd.ts:10)
+constexpr int kSolveReduce = 256;    // threads per body in the match pass (pbd.ts:8)
+constexpr uint32_t kBodyKinematic = 1u, kBodyWeightless = 2u;  // BodyFlags (particles.ts:38-43)
+
 // The brush record (brush.ts:52-78), 80 bytes.
 struct BrushDev {
   float pos[3];
@@ -2201,6 +2219,307 @@ __global__ void __launch_bounds__(kExtractThreads) k_ext_finish(const ExtractDev
   E.draw_args[1] = 1u;
   E.draw_args[2] = 0u;
   E.draw_args[3] = 0u;
+}
+
+// ---------------------------------------------------------------------------------------
+// ClaySolver (sim/pbd.ts:78-424): shape-matched particle bodies of a ParticleSet colliding
+// against a field. Particle records are 96 bytes (pos 0, body 12, prev 16, material 28,
+// vel 32, velPrev 48, rest 64, restNormal 80), Body records 64 (com 0, first 12, rot 16,
+// restCom 32, count 44, stiffness 48, plasticity 52, material 56, flags 60).
+
+// sin and cos of one angle, identical on the device and in the CPU restatement (WGSL leaves
+// their precision to the implementation): Cody-Waite reduction by pi/2 split in three f32
+// parts (the first two of 12 significant bits, so k times them is exact for |k| < 4096), then
+// Taylor polynomials through x^9 (sin) and x^10 (cos) on [-pi/4, pi/4], where the truncation
+// error is far below half an f32 ulp.
+__host__ __device__ inline void clay_sincos(float x, float& s, float& c) {
+  const float k = rintf(x * 0.636619746685028076171875f);
+  const float r = ((x - k * 1.57080078125f) - k * -4.453584551811218e-06f) - k * -8.705515752716053e-10f;
+  const float r2 = r * r;
+  const float ps = r + r * (r2 * (-0.16666667163372039794921875f +
+                                 r2 * (0.008333333767950534820556640625f +
+                                       r2 * (-0.000198412701138295233249664306640625f + r2 * 2.7557318844628753140568733215332031e-06f))));
+  const float pc = 1.0f + r2 * (-0.5f + r2 * (0.041666667908430099487304687500f +
+                                            r2 * (-0.0013888889225199818611145019531f +
+                                                  r2 * (2.4801587642286904156208038330078e-05f + r2 * -2.7557319981497130356729030609131e-07f))));
+  const int q = static_cast<int>(k) & 3;
+  s = q == 0 ? ps : q == 1 ? pc : q == 2 ? -ps : -pc;
+  c = q == 0 ? pc : q == 1 ? -ps : q == 2 ? -pc : ps;
+}
+
+struct Q4 {
+  float x, y, z, w;
+};
+// quatMul, quatRotate, quatConj, quatToMat3 (math/gpu.ts:5-44), in their operation order.
+__device__ __forceinline__ Q4 quat_mul(Q4 a, Q4 b) {
+  return {((a.w * b.x + a.x * b.w) + a.y * b.z) - a.z * b.y, ((a.w * b.y - a.x * b.z) + a.y * b.w) + a.z * b.x,
+          ((a.w * b.z + a.x * b.y) - a.y * b.x) + a.z * b.w, ((a.w * b.w - a.x * b.x) - a.y * b.y) - a.z * b.z};
+}
+__device__ __forceinline__ void cross3(float ax, float ay, float az, float bx, float by, float bz, float& cx, float& cy,
+                                       float& cz) {
+  cx = ay * bz - az * by;
+  cy = az * bx - ax * bz;
+  cz = ax * by - ay * bx;
+}
+__device__ __forceinline__ void quat_rotate(Q4 q, float vx, float vy, float vz, float& ox, float& oy, float& oz) {
+  float tx, ty, tz;
+  cross3(q.x, q.y, q.z, vx, vy, vz, tx, ty, tz);
+  tx = tx * 2.0f;
+  ty = ty * 2.0f;
+  tz = tz * 2.0f;
+  float ux, uy, uz;
+  cross3(q.x, q.y, q.z, tx, ty, tz, ux, uy, uz);
+  ox = (vx + tx * q.w) + ux;
+  oy = (vy + ty * q.w) + uy;
+  oz = (vz + tz * q.w) + uz;
+}
+
+// extractRotation (math/gpu.ts:55-77, Müller et al. 2016): warm-started quaternion iterations
+// towards the rotational part of A (columns a0, a1, a2).
+__device__ __forceinline__ Q4 extract_rotation(const float a[9], Q4 q, int iters) {
+  for (int it = 0; it < iters; it++) {
+    const float x = q.x, y = q.y, z = q.z, w = q.w;
+    // quatToMat3 columns
+    const float c0[3] = {1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y + z * w), 2.0f * (x * z - y * w)};
+    const float c1[3] = {2.0f * (x * y - z * w), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z + x * w)};
+    const float c2[3] = {2.0f * (x * z + y * w), 2.0f * (y * z - x * w), 1.0f - 2.0f * (x * x + y * y)};
+    const float d = (dot3(c0[0], c0[1], c0[2], a[0], a[1], a[2]) + dot3(c1[0], c1[1], c1[2], a[3], a[4], a[5])) +
+                    dot3(c2[0], c2[1], c2[2], a[6], a[7], a[8]);
+    const float denom = fabsf(d) + 1e-9f;
+    float e0x, e0y, e0z, e1x, e1y, e1z, e2x, e2y, e2z;
+    cross3(c0[0], c0[1], c0[2], a[0], a[1], a[2], e0x, e0y, e0z);
+    cross3(c1[0], c1[1], c1[2], a[3], a[4], a[5], e1x, e1y, e1z);
+    cross3(c2[0], c2[1], c2[2], a[6], a[7], a[8], e2x, e2y, e2z);
+    const float inv = __fdiv_rn(1.0f, denom);
+    const float ox = ((e0x + e1x) + e2x) * inv, oy = ((e0y + e1y) + e2y) * inv, oz = ((e0z + e1z) + e2z) * inv;
+    const float wl = len3(ox, oy, oz);
+    if (wl < 1e-9f) break;
+    const float iw = __fdiv_rn(1.0f, wl);
+    // quatFromAxisAngle(omega * (1 / w), w)
+    float sh, ch;
+    clay_sincos(wl * 0.5f, sh, ch);
+    const Q4 r = {(ox * iw) * sh, (oy * iw) * sh, (oz * iw) * sh, ch};
+    const Q4 m = quat_mul(r, q);
+    // normalize: v / length(v)
+    const float l = __fsqrt_rn(((m.x * m.x + m.y * m.y) + m.z * m.z) + m.w * m.w);
+    q = {__fdiv_rn(m.x, l), __fdiv_rn(m.y, l), __fdiv_rn(m.z, l), __fdiv_rn(m.w, l)};
+  }
+  return q;
+}
+
+// ownerOf (pbd.ts:126-142): the particle's body when the slot lies in that body's slice,
+// else max_bodies.
+__device__ __forceinline__ uint32_t pbd_owner(const SolveDev& S, uint32_t i) {
+  const uint32_t b = *reinterpret_cast<const uint32_t*>(S.particles + static_cast<size_t>(i) * 96 + 12);
+  if (b >= static_cast<uint32_t>(S.max_bodies)) return static_cast<uint32_t>(S.max_bodies);
+  const unsigned char* bd = S.bodies + static_cast<size_t>(b) * 64;
+  const uint32_t first = *reinterpret_cast<const uint32_t*>(bd + 12), count = *reinterpret_cast<const uint32_t*>(bd + 44);
+  if (i < first || i >= first + count) return static_cast<uint32_t>(S.max_bodies);
+  return b;
+}
+__device__ __forceinline__ uint32_t pbd_flags(const SolveDev& S, uint32_t b) {
+  return *reinterpret_cast<const uint32_t*>(S.bodies + static_cast<size_t>(b) * 64 + 60);
+}
+
+// kick (pbd.ts:144-170): the one-shot velocity change of the pushed body.
+__global__ void __launch_bounds__(kSolveThreads) k_pbd_kick(const SolveDev* __restrict__ sd) {
+  const SolveDev& S = *sd;
+  const uint32_t i = blockIdx.x * kSolveThreads + threadIdx.x;
+  if (i >= static_cast<uint32_t>(S.capacity)) return;
+  const uint32_t b = pbd_owner(S, i);
+  if (b != S.push_body || b >= static_cast<uint32_t>(S.max_bodies)) return;
+  if (pbd_flags(S, b) & kBodyKinematic) return;
+  float* p = reinterpret_cast<float*>(S.particles + static_cast<size_t>(i) * 96);
+  for (int k = 0; k < 3; k++) {
+    const float dv = S.kick[k];
+    const float vel = p[8 + k], vp = p[12 + k], prev = p[4 + k];
+    p[8 + k] = vel + dv;
+    p[12 + k] = vp + dv;
+    p[4 + k] = prev - dv * S.h;
+  }
+}
+
+// predict (pbd.ts:172-222): BDF2 predictor, then the world collision with positional friction.
+__global__ void __launch_bounds__(kSolveThreads) k_pbd_predict(const SolveDev* __restrict__ sd) {
+  const SolveDev& S = *sd;
+  const uint32_t i = blockIdx.x * kSolveThreads + threadIdx.x;
+  if (i >= static_cast<uint32_t>(S.capacity)) return;
+  const uint32_t b = pbd_owner(S, i);
+  if (b >= static_cast<uint32_t>(S.max_bodies)) return;
+  const uint32_t flags = pbd_flags(S, b);
+  if (flags & kBodyKinematic) return;
+  float* p = reinterpret_cast<float*>(S.particles + static_cast<size_t>(i) * 96);
+  float acc[3];
+  for (int k = 0; k < 3; k++) {
+    acc[k] = (flags & kBodyWeightless) ? 0.0f : S.gravity[k];
+    if (b == S.push_body) acc[k] = acc[k] + S.push[k];
+  }
+  const float third = 0.3333333432674407958984375f;  // f32(1 / 3)
+  const float h23 = __fdiv_rn(2.0f * S.h, 3.0f);
+  float q[3];
+  for (int k = 0; k < 3; k++) {
+    const float vpred = (p[8 + k] * 4.0f - p[12 + k]) * third + acc[k] * h23;
+    q[k] = (p[k] * 4.0f - p[4 + k]) * third + vpred * h23;
+  }
+  float prev[3] = {p[0], p[1], p[2]};
+  float sx, sy;
+  const int child = field_pick(S.world, q[0], q[1], q[2], sx, sy);
+  if (sx < S.radius) {
+    float nx, ny, nz;
+    field_normal(S.world, child, q[0], q[1], q[2], nx, ny, nz);
+    const float push = S.radius - sx;
+    q[0] = q[0] + nx * push;
+    q[1] = q[1] + ny * push;
+    q[2] = q[2] + nz * push;
+    prev[0] = p[0] + nx * push;
+    prev[1] = p[1] + ny * push;
+    prev[2] = p[2] + nz * push;
+    const float dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
+    const float dn = dot3(dx, dy, dz, nx, ny, nz);
+    q[0] = q[0] - (dx - nx * dn) * S.friction;
+    q[1] = q[1] - (dy - ny * dn) * S.friction;
+    q[2] = q[2] - (dz - nz * dn) * S.friction;
+  }
+  for (int k = 0; k < 3; k++) {
+    p[4 + k] = prev[k];
+    p[k] = q[k];
+  }
+}
+
+// match (pbd.ts:224-297): per body, the current and rest centroids and the covariance
+// A = sum (p - com)(r - restCom)^T by per-thread strided sums and a tree, then the rotation.
+__global__ void __launch_bounds__(kSolveReduce) k_pbd_match(const SolveDev* __restrict__ sd) {
+  const SolveDev& S = *sd;
+  const uint32_t b = blockIdx.x, li = threadIdx.x;
+  unsigned char* bd = S.bodies + static_cast<size_t>(b) * 64;
+  const uint32_t first = *reinterpret_cast<const uint32_t*>(bd + 12), count = *reinterpret_cast<const uint32_t*>(bd + 44);
+  // the slice clipped to the set: a record reaching past the capacity reads no further
+  const uint32_t cap = static_cast<uint32_t>(S.capacity);
+  const uint32_t live = first >= cap ? 0u : min(count, cap - first);
+  __shared__ float g[kSolveReduce][9];
+  auto reduce = [&]() {
+    for (uint32_t s = kSolveReduce / 2; s > 0; s >>= 1) {
+      if (li < s)
+        for (int k = 0; k < 9; k++) g[li][k] = g[li][k] + g[li + s][k];
+      __syncthreads();
+    }
+  };
+  float sp[3] = {0.0f, 0.0f, 0.0f}, sr[3] = {0.0f, 0.0f, 0.0f};
+  for (uint32_t t = li; t < live; t += kSolveReduce) {
+    const float* p = reinterpret_cast<const float*>(S.particles + static_cast<size_t>(first + t) * 96);
+    for (int k = 0; k < 3; k++) {
+      sp[k] = sp[k] + p[k];
+      sr[k] = sr[k] + p[16 + k];
+    }
+  }
+  for (int k = 0; k < 3; k++) {
+    g[li][k] = sp[k];
+    g[li][3 + k] = sr[k];
+    g[li][6 + k] = 0.0f;
+  }
+  __syncthreads();
+  reduce();
+  const float inv = __fdiv_rn(1.0f, fmaxf(static_cast<float>(count), 1.0f));
+  const float com[3] = {g[0][0] * inv, g[0][1] * inv, g[0][2] * inv};
+  const float rcom[3] = {g[0][3] * inv, g[0][4] * inv, g[0][5] * inv};
+  __syncthreads();
+  float a[9] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  for (uint32_t t = li; t < live; t += kSolveReduce) {
+    const float* p = reinterpret_cast<const float*>(S.particles + static_cast<size_t>(first + t) * 96);
+    const float pr[3] = {p[0] - com[0], p[1] - com[1], p[2] - com[2]};
+    const float rr[3] = {p[16] - rcom[0], p[17] - rcom[1], p[18] - rcom[2]};
+    for (int c = 0; c < 3; c++)
+      for (int k = 0; k < 3; k++) a[3 * c + k] = a[3 * c + k] + pr[k] * rr[c];
+  }
+  for (int k = 0; k < 9; k++) g[li][k] = a[k];
+  __syncthreads();
+  reduce();
+  if (li == 0 && count > 0) {
+    float* f = reinterpret_cast<float*>(bd);
+    const Q4 q0 = {f[4], f[5], f[6], f[7]};
+    float A[9];
+    for (int k = 0; k < 9; k++) A[k] = g[0][k];
+    const Q4 r = extract_rotation(A, q0, S.rot_iters);
+    f[0] = com[0];
+    f[1] = com[1];
+    f[2] = com[2];
+    f[8] = rcom[0];
+    f[9] = rcom[1];
+    f[10] = rcom[2];
+    f[4] = r.x;
+    f[5] = r.y;
+    f[6] = r.z;
+    f[7] = r.w;
+  }
+}
+
+// apply (pbd.ts:299-340): the pull towards the matched shape, a final projection out of the
+// world, and plasticity letting the rest shape follow.
+__global__ void __launch_bounds__(kSolveThreads) k_pbd_apply(const SolveDev* __restrict__ sd) {
+  const SolveDev& S = *sd;
+  const uint32_t i = blockIdx.x * kSolveThreads + threadIdx.x;
+  if (i >= static_cast<uint32_t>(S.capacity)) return;
+  const uint32_t b = pbd_owner(S, i);
+  if (b >= static_cast<uint32_t>(S.max_bodies)) return;
+  const float* bf = reinterpret_cast<const float*>(S.bodies + static_cast<size_t>(b) * 64);
+  const uint32_t flags = *reinterpret_cast<const uint32_t*>(bf + 15);
+  if (flags & kBodyKinematic) return;
+  float* p = reinterpret_cast<float*>(S.particles + static_cast<size_t>(i) * 96);
+  const Q4 rot = {bf[4], bf[5], bf[6], bf[7]};
+  float tx, ty, tz;
+  quat_rotate(rot, p[16] - bf[8], p[17] - bf[9], p[18] - bf[10], tx, ty, tz);
+  const float target[3] = {bf[0] + tx, bf[1] + ty, bf[2] + tz};
+  const float st = clampf(bf[12], 0.0f, 1.0f), om = 1.0f - st;
+  float q[3];
+  for (int k = 0; k < 3; k++) q[k] = p[k] * om + target[k] * st;  // mix(pos, target, st)
+  float sx, sy;
+  const int child = field_pick(S.world, q[0], q[1], q[2], sx, sy);
+  if (sx < S.radius) {
+    float nx, ny, nz;
+    field_normal(S.world, child, q[0], q[1], q[2], nx, ny, nz);
+    const float push = S.radius - sx;
+    q[0] = q[0] + nx * push;
+    q[1] = q[1] + ny * push;
+    q[2] = q[2] + nz * push;
+    p[4] = p[4] + nx * push;
+    p[5] = p[5] + ny * push;
+    p[6] = p[6] + nz * push;
+  }
+  const float r0[3] = {p[16], p[17], p[18]};
+  p[0] = q[0];
+  p[1] = q[1];
+  p[2] = q[2];
+  if (bf[13] > 0.0f) {
+    const Q4 cj = {-rot.x, -rot.y, -rot.z, rot.w};
+    float rx, ry, rz;
+    quat_rotate(cj, q[0] - bf[0], q[1] - bf[1], q[2] - bf[2], rx, ry, rz);
+    const float rest[3] = {rx + bf[8], ry + bf[9], rz + bf[10]};
+    const float pl = clampf(bf[13], 0.0f, 1.0f), om2 = 1.0f - pl;
+    for (int k = 0; k < 3; k++) p[16 + k] = r0[k] * om2 + rest[k] * pl;
+  }
+}
+
+// finalize (pbd.ts:342-372): first-order velocity from the positions, damping, speed cap.
+__global__ void __launch_bounds__(kSolveThreads) k_pbd_finalize(const SolveDev* __restrict__ sd) {
+  const SolveDev& S = *sd;
+  const uint32_t i = blockIdx.x * kSolveThreads + threadIdx.x;
+  if (i >= static_cast<uint32_t>(S.capacity)) return;
+  const uint32_t b = pbd_owner(S, i);
+  if (b >= static_cast<uint32_t>(S.max_bodies)) return;
+  if (pbd_flags(S, b) & kBodyKinematic) return;
+  float* p = reinterpret_cast<float*>(S.particles + static_cast<size_t>(i) * 96);
+  const float ih = __fdiv_rn(1.0f, fmaxf(S.h, 1e-6f));
+  float v[3];
+  for (int k = 0; k < 3; k++) v[k] = ((p[k] - p[4 + k]) * ih) * S.damping;
+  const float speed = len3(v[0], v[1], v[2]);
+  if (speed > S.max_speed) {
+    const float sc = __fdiv_rn(S.max_speed, speed);
+    for (int k = 0; k < 3; k++) v[k] = v[k] * sc;
+  }
+  for (int k = 0; k < 3; k++) {
+    p[12 + k] = p[8 + k];
+    p[8 + k] = v[k];
+  }
 }
 
 // Gathers the ContactList of every scene of a batch into one array (one readback).

@@ -69,6 +69,15 @@ cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t
 cudaError_t L_field_query_mip(const FieldDev* f, const float* pts, int n, int mip, float* sxy, float* fxy, cudaStream_t st) {
   CLAY_LAUNCH(k_field_query_mip, (n + 255) / 256, 256, st, f, pts, n, mip, sxy, fxy);
 }
+cudaError_t L_pbd_kick(const SolveDev* s, int blocks, cudaStream_t st) { CLAY_LAUNCH(k_pbd_kick, blocks, kSolveThreads, st, s); }
+cudaError_t L_pbd_predict(const SolveDev* s, int blocks, cudaStream_t st) {
+  CLAY_LAUNCH(k_pbd_predict, blocks, kSolveThreads, st, s);
+}
+cudaError_t L_pbd_match(const SolveDev* s, int bodies, cudaStream_t st) { CLAY_LAUNCH(k_pbd_match, bodies, kSolveReduce, st, s); }
+cudaError_t L_pbd_apply(const SolveDev* s, int blocks, cudaStream_t st) { CLAY_LAUNCH(k_pbd_apply, blocks, kSolveThreads, st, s); }
+cudaError_t L_pbd_finalize(const SolveDev* s, int blocks, cudaStream_t st) {
+  CLAY_LAUNCH(k_pbd_finalize, blocks, kSolveThreads, st, s);
+}
 cudaError_t L_ext_reset(const ExtractDev* e, cudaStream_t st) { CLAY_LAUNCH(k_ext_reset, 1, kExtractThreads, st, e); }
 cudaError_t L_ext_cells(const ExtractDev* e, int blocks, cudaStream_t st) {
   CLAY_LAUNCH(k_ext_cells, blocks, kExtractThreads, st, e);

@@ -39,6 +39,12 @@ cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, 
 cudaError_t L_resolve(const SplatDev* d, const Work* w, int blocks, cudaStream_t st);
 // SurfaceExtractor passes (grid passes: `blocks` blocks of kExtractThreads lattice cells).
 cudaError_t L_field_query_mip(const FieldDev* f, const float* pts, int n, int mip, float* sxy, float* fxy, cudaStream_t st);
+// ClaySolver passes.
+cudaError_t L_pbd_kick(const SolveDev* s, int blocks, cudaStream_t st);
+cudaError_t L_pbd_predict(const SolveDev* s, int blocks, cudaStream_t st);
+cudaError_t L_pbd_match(const SolveDev* s, int bodies, cudaStream_t st);
+cudaError_t L_pbd_apply(const SolveDev* s, int blocks, cudaStream_t st);
+cudaError_t L_pbd_finalize(const SolveDev* s, int blocks, cudaStream_t st);
 cudaError_t L_ext_reset(const ExtractDev* e, cudaStream_t st);
 cudaError_t L_ext_cells(const ExtractDev* e, int blocks, cudaStream_t st);
 cudaError_t L_ext_scan(const ExtractDev* e, int which, cudaStream_t st);

@@ -496,6 +496,46 @@ int clay_extractor_read_indices_async(clay_extractor* x, uint32_t* host_indices,
 int clay_field_offset_device(const clay_field* f, const float* device_offset, clay_field** out);
 
 /* ------------------------------------------------------------------------------------
+ * ClaySolver (lib/src/sim/pbd.ts:78-424): shape-matched bodies of a ParticleSet colliding
+ * against a field. Per step: the one-shot kick, then `substeps` x (BDF2 predict with world
+ * collision and positional friction, per-body shape match with the polar rotation of
+ * math/gpu.ts:55-77, pull and projection with plasticity, velocity finalize). Particles and
+ * bodies are the caller's device buffers (96- and 64-byte records, particles.ts:18-68).
+ * ---------------------------------------------------------------------------------- */
+typedef struct clay_solver clay_solver;
+#define CLAY_SOLVER_GRAVITY (1u << 0)
+#define CLAY_SOLVER_DT (1u << 1)
+#define CLAY_SOLVER_SUBSTEPS (1u << 2)
+#define CLAY_SOLVER_RADIUS (1u << 3)
+#define CLAY_SOLVER_FRICTION (1u << 4)
+#define CLAY_SOLVER_DAMPING (1u << 5)
+#define CLAY_SOLVER_MAX_SPEED (1u << 6)
+#define CLAY_SOLVER_ROTATION_ITERATIONS (1u << 7)
+/* ClaySolverOptions (pbd.ts:44-55); unset options take the reference's defaults: gravity
+ * (0,-9.81,0), dt 1/60, substeps 2, radius 0.1, friction 0.35, damping 0.995, maxSpeed 40,
+ * rotationIterations 2 (pbd.ts:101-118). */
+typedef struct clay_solver_opts {
+  uint32_t set;
+  int32_t substeps;
+  double gravity[3];
+  double dt;
+  double radius;
+  double friction;
+  double damping;
+  double max_speed;
+  int32_t rotation_iterations;
+  int32_t pad;
+} clay_solver_opts;
+int clay_solver_create(clay_ctx* ctx, const clay_field* world, void* particles, int64_t capacity, void* bodies,
+                       int32_t max_bodies, const clay_solver_opts* opts, clay_solver** out);
+void clay_solver_destroy(clay_solver* s);
+/* setForce (pbd.ts:376-398): a uniform acceleration of one body for the next steps and a
+ * one-shot velocity change (`impulse`, may be NULL) applied once by the next step. */
+int clay_solver_set_force(clay_solver* s, uint32_t body, const double accel[3], const double impulse[3]);
+/* step (pbd.ts:396-416) over the set's first `body_count` bodies, on `stream`. */
+int clay_solver_step(clay_solver* s, int32_t body_count, void* stream);
+
+/* ------------------------------------------------------------------------------------
  * Continuous-batching server (no reference counterpart: the reference steps the scenes of
  * one game). Serves requests "advance scene i by k frames" (each frame: FluidSim.step with
  * its bake) over many registered scenes. Each frame it launches one clay_batch_step_subset

@@ -1440,3 +1440,262 @@ void orc_extract(const orc_extract_cfg* cfg, const orc_field* field, float* moti
   draw_args[2] = 0;
   draw_args[3] = 0;
 }
+
+
+// ----------------------------------------------------------------------------------------
+// ClaySolver.step (sim/pbd.ts:144-416) in f32, particle passes in index order (each touches
+// only its own record), the match pass as the reference's 256-thread workgroup per body:
+// per-thread strided sums, then a tree.
+namespace {
+// sin and cos by Cody-Waite reduction by pi/2 and Taylor polynomials on [-pi/4, pi/4]: the
+// same steps as the CUDA path, so both sides round alike (WGSL leaves sin/cos precision open).
+void orc_sincos(float x, float& s, float& c) {
+  const float k = std::nearbyint(x * 0.636619746685028076171875f);
+  const float r = ((x - k * 1.57080078125f) - k * -4.453584551811218e-06f) - k * -8.705515752716053e-10f;
+  const float r2 = r * r;
+  const float ps = r + r * (r2 * (-0.16666667163372039794921875f +
+                                 r2 * (0.008333333767950534820556640625f +
+                                       r2 * (-0.000198412701138295233249664306640625f + r2 * 2.7557318844628753140568733215332031e-06f))));
+  const float pc = 1.0f + r2 * (-0.5f + r2 * (0.041666667908430099487304687500f +
+                                            r2 * (-0.0013888889225199818611145019531f +
+                                                  r2 * (2.4801587642286904156208038330078e-05f + r2 * -2.7557319981497130356729030609131e-07f))));
+  const int q = static_cast<int>(k) & 3;
+  s = q == 0 ? ps : q == 1 ? pc : q == 2 ? -ps : -pc;
+  c = q == 0 ? pc : q == 1 ? -ps : q == 2 ? -pc : ps;
+}
+
+struct Qf {
+  float x, y, z, w;
+};
+Qf qmul(Qf a, Qf b) {
+  return {((a.w * b.x + a.x * b.w) + a.y * b.z) - a.z * b.y, ((a.w * b.y - a.x * b.z) + a.y * b.w) + a.z * b.x,
+          ((a.w * b.z + a.x * b.y) - a.y * b.x) + a.z * b.w, ((a.w * b.w - a.x * b.x) - a.y * b.y) - a.z * b.z};
+}
+void cross3f(float ax, float ay, float az, float bx, float by, float bz, float& cx, float& cy, float& cz) {
+  cx = ay * bz - az * by;
+  cy = az * bx - ax * bz;
+  cz = ax * by - ay * bx;
+}
+void qrot(Qf q, float vx, float vy, float vz, float& ox, float& oy, float& oz) {
+  float tx, ty, tz, ux, uy, uz;
+  cross3f(q.x, q.y, q.z, vx, vy, vz, tx, ty, tz);
+  tx = tx * 2.0f;
+  ty = ty * 2.0f;
+  tz = tz * 2.0f;
+  cross3f(q.x, q.y, q.z, tx, ty, tz, ux, uy, uz);
+  ox = (vx + tx * q.w) + ux;
+  oy = (vy + ty * q.w) + uy;
+  oz = (vz + tz * q.w) + uz;
+}
+float dot3f(float ax, float ay, float az, float bx, float by, float bz) { return (ax * bx + ay * by) + az * bz; }
+float len3f(float x, float y, float z) { return std::sqrt(dot3f(x, y, z, x, y, z)); }
+float clampf_(float x, float lo, float hi) { return std::min(std::max(x, lo), hi); }
+
+// extractRotation (math/gpu.ts:55-77)
+Qf extract_rot(const float a[9], Qf q, int iters) {
+  for (int it = 0; it < iters; it++) {
+    const float x = q.x, y = q.y, z = q.z, w = q.w;
+    const float c0[3] = {1.0f - 2.0f * (y * y + z * z), 2.0f * (x * y + z * w), 2.0f * (x * z - y * w)};
+    const float c1[3] = {2.0f * (x * y - z * w), 1.0f - 2.0f * (x * x + z * z), 2.0f * (y * z + x * w)};
+    const float c2[3] = {2.0f * (x * z + y * w), 2.0f * (y * z - x * w), 1.0f - 2.0f * (x * x + y * y)};
+    const float d = (dot3f(c0[0], c0[1], c0[2], a[0], a[1], a[2]) + dot3f(c1[0], c1[1], c1[2], a[3], a[4], a[5])) +
+                    dot3f(c2[0], c2[1], c2[2], a[6], a[7], a[8]);
+    const float denom = std::fabs(d) + 1e-9f;
+    float e0x, e0y, e0z, e1x, e1y, e1z, e2x, e2y, e2z;
+    cross3f(c0[0], c0[1], c0[2], a[0], a[1], a[2], e0x, e0y, e0z);
+    cross3f(c1[0], c1[1], c1[2], a[3], a[4], a[5], e1x, e1y, e1z);
+    cross3f(c2[0], c2[1], c2[2], a[6], a[7], a[8], e2x, e2y, e2z);
+    const float inv = 1.0f / denom;
+    const float ox = ((e0x + e1x) + e2x) * inv, oy = ((e0y + e1y) + e2y) * inv, oz = ((e0z + e1z) + e2z) * inv;
+    const float wl = len3f(ox, oy, oz);
+    if (wl < 1e-9f) break;
+    const float iw = 1.0f / wl;
+    float sh, ch;
+    orc_sincos(wl * 0.5f, sh, ch);
+    const Qf r = {(ox * iw) * sh, (oy * iw) * sh, (oz * iw) * sh, ch};
+    const Qf m = qmul(r, q);
+    const float l = std::sqrt(((m.x * m.x + m.y * m.y) + m.z * m.z) + m.w * m.w);
+    q = {m.x / l, m.y / l, m.z / l, m.w / l};
+  }
+  return q;
+}
+}  // namespace
+
+void orc_sincos_f32(float x, float sc[2]) { orc_sincos(x, sc[0], sc[1]); }
+
+void orc_solver_step(const orc_solve_cfg* cfg, const orc_field* world, unsigned char* particles, unsigned char* bodies,
+                     int body_count) {
+  if (body_count == 0) return;
+  const FieldU<float> f = make_field<float>(world);
+  const uint32_t maxb = static_cast<uint32_t>(cfg->max_bodies);
+  auto P = [&](uint32_t i) { return reinterpret_cast<float*>(particles + static_cast<size_t>(i) * 96); };
+  auto B = [&](uint32_t b) { return reinterpret_cast<float*>(bodies + static_cast<size_t>(b) * 64); };
+  auto U = [](const float* p, int k) {
+    uint32_t u;
+    std::memcpy(&u, p + k, 4);
+    return u;
+  };
+  auto owner = [&](uint32_t i) -> uint32_t {
+    const uint32_t b = U(P(i), 3);
+    if (b >= maxb) return maxb;
+    const float* bd = B(b);
+    const uint32_t first = U(bd, 3), count = U(bd, 11);
+    if (i < first || i >= first + count) return maxb;
+    return b;
+  };
+  auto sample = [&](const float q[3], float& dw, float n[3]) {
+    float s[2];
+    const int child = field_pick(f, v3(q[0], q[1], q[2]), s);
+    dw = s[0];
+    const V3<float> nn = field_normal(f, v3(q[0], q[1], q[2]), child);
+    n[0] = nn.x;
+    n[1] = nn.y;
+    n[2] = nn.z;
+  };
+  const uint32_t cap = static_cast<uint32_t>(cfg->capacity);
+  if (cfg->kicking)
+    for (uint32_t i = 0; i < cap; i++) {
+      const uint32_t b = owner(i);
+      if (b != cfg->push_body || b >= maxb || (U(B(b), 15) & 1u)) continue;
+      float* p = P(i);
+      for (int k = 0; k < 3; k++) {
+        const float dv = cfg->kick[k];
+        const float vel = p[8 + k], vp = p[12 + k], prev = p[4 + k];
+        p[8 + k] = vel + dv;
+        p[12 + k] = vp + dv;
+        p[4 + k] = prev - dv * cfg->h;
+      }
+    }
+  for (int sub = 0; sub < cfg->substeps; sub++) {
+    // predict
+    for (uint32_t i = 0; i < cap; i++) {
+      const uint32_t b = owner(i);
+      if (b >= maxb) continue;
+      const uint32_t flags = U(B(b), 15);
+      if (flags & 1u) continue;
+      float* p = P(i);
+      float acc[3];
+      for (int k = 0; k < 3; k++) {
+        acc[k] = (flags & 2u) ? 0.0f : cfg->gravity[k];
+        if (b == cfg->push_body) acc[k] = acc[k] + cfg->push[k];
+      }
+      const float third = 0.3333333432674407958984375f;
+      const float h23 = (2.0f * cfg->h) / 3.0f;
+      float q[3];
+      for (int k = 0; k < 3; k++) {
+        const float vpred = (p[8 + k] * 4.0f - p[12 + k]) * third + acc[k] * h23;
+        q[k] = (p[k] * 4.0f - p[4 + k]) * third + vpred * h23;
+      }
+      float prev[3] = {p[0], p[1], p[2]};
+      float dw, n[3];
+      sample(q, dw, n);
+      if (dw < cfg->radius) {
+        const float push = cfg->radius - dw;
+        for (int k = 0; k < 3; k++) q[k] = q[k] + n[k] * push;
+        for (int k = 0; k < 3; k++) prev[k] = p[k] + n[k] * push;
+        const float dx = q[0] - p[0], dy = q[1] - p[1], dz = q[2] - p[2];
+        const float dn = dot3f(dx, dy, dz, n[0], n[1], n[2]);
+        q[0] = q[0] - (dx - n[0] * dn) * cfg->friction;
+        q[1] = q[1] - (dy - n[1] * dn) * cfg->friction;
+        q[2] = q[2] - (dz - n[2] * dn) * cfg->friction;
+      }
+      for (int k = 0; k < 3; k++) {
+        p[4 + k] = prev[k];
+        p[k] = q[k];
+      }
+    }
+    // match
+    constexpr int T = 256;
+    for (int b = 0; b < body_count; b++) {
+      float* bd = B(static_cast<uint32_t>(b));
+      const uint32_t first = U(bd, 3), count = U(bd, 11);
+      // the slice clipped to the set: a record reaching past the capacity reads no further
+      const uint32_t live = first >= cap ? 0u : std::min(count, cap - first);
+      std::vector<float> g(static_cast<size_t>(T) * 9, 0.0f);
+      for (int li = 0; li < T; li++)
+        for (uint32_t t = li; t < live; t += T) {
+          const float* p = P(first + t);
+          for (int k = 0; k < 3; k++) {
+            g[li * 9 + k] = g[li * 9 + k] + p[k];
+            g[li * 9 + 3 + k] = g[li * 9 + 3 + k] + p[16 + k];
+          }
+        }
+      auto reduce = [&]() {
+        for (int h = T / 2; h > 0; h >>= 1)
+          for (int li = 0; li < h; li++)
+            for (int k = 0; k < 9; k++) g[li * 9 + k] = g[li * 9 + k] + g[(li + h) * 9 + k];
+      };
+      reduce();
+      const float inv = 1.0f / std::max(static_cast<float>(count), 1.0f);
+      const float com[3] = {g[0] * inv, g[1] * inv, g[2] * inv};
+      const float rcom[3] = {g[3] * inv, g[4] * inv, g[5] * inv};
+      std::fill(g.begin(), g.end(), 0.0f);
+      for (int li = 0; li < T; li++)
+        for (uint32_t t = li; t < live; t += T) {
+          const float* p = P(first + t);
+          const float pr[3] = {p[0] - com[0], p[1] - com[1], p[2] - com[2]};
+          const float rr[3] = {p[16] - rcom[0], p[17] - rcom[1], p[18] - rcom[2]};
+          for (int c = 0; c < 3; c++)
+            for (int k = 0; k < 3; k++) g[li * 9 + 3 * c + k] = g[li * 9 + 3 * c + k] + pr[k] * rr[c];
+        }
+      reduce();
+      if (count > 0) {
+        const Qf q0 = {bd[4], bd[5], bd[6], bd[7]};
+        const Qf r = extract_rot(&g[0], q0, cfg->rot_iters);
+        bd[0] = com[0], bd[1] = com[1], bd[2] = com[2];
+        bd[8] = rcom[0], bd[9] = rcom[1], bd[10] = rcom[2];
+        bd[4] = r.x, bd[5] = r.y, bd[6] = r.z, bd[7] = r.w;
+      }
+    }
+    // apply
+    for (uint32_t i = 0; i < cap; i++) {
+      const uint32_t b = owner(i);
+      if (b >= maxb) continue;
+      const float* bf = B(b);
+      if (U(bf, 15) & 1u) continue;
+      float* p = P(i);
+      const Qf rot = {bf[4], bf[5], bf[6], bf[7]};
+      float tx, ty, tz;
+      qrot(rot, p[16] - bf[8], p[17] - bf[9], p[18] - bf[10], tx, ty, tz);
+      const float target[3] = {bf[0] + tx, bf[1] + ty, bf[2] + tz};
+      const float st = clampf_(bf[12], 0.0f, 1.0f), om = 1.0f - st;
+      float q[3];
+      for (int k = 0; k < 3; k++) q[k] = p[k] * om + target[k] * st;
+      float dw, n[3];
+      sample(q, dw, n);
+      if (dw < cfg->radius) {
+        const float push = cfg->radius - dw;
+        for (int k = 0; k < 3; k++) q[k] = q[k] + n[k] * push;
+        for (int k = 0; k < 3; k++) p[4 + k] = p[4 + k] + n[k] * push;
+      }
+      const float r0[3] = {p[16], p[17], p[18]};
+      for (int k = 0; k < 3; k++) p[k] = q[k];
+      if (bf[13] > 0.0f) {
+        const Qf cj = {-rot.x, -rot.y, -rot.z, rot.w};
+        float rx, ry, rz;
+        qrot(cj, q[0] - bf[0], q[1] - bf[1], q[2] - bf[2], rx, ry, rz);
+        const float rest[3] = {rx + bf[8], ry + bf[9], rz + bf[10]};
+        const float pl = clampf_(bf[13], 0.0f, 1.0f), om2 = 1.0f - pl;
+        for (int k = 0; k < 3; k++) p[16 + k] = r0[k] * om2 + rest[k] * pl;
+      }
+    }
+    // finalize
+    for (uint32_t i = 0; i < cap; i++) {
+      const uint32_t b = owner(i);
+      if (b >= maxb || (U(B(b), 15) & 1u)) continue;
+      float* p = P(i);
+      const float ih = 1.0f / std::max(cfg->h, 1e-6f);
+      float v[3];
+      for (int k = 0; k < 3; k++) v[k] = ((p[k] - p[4 + k]) * ih) * cfg->damping;
+      const float speed = len3f(v[0], v[1], v[2]);
+      if (speed > cfg->max_speed) {
+        const float sc = cfg->max_speed / speed;
+        for (int k = 0; k < 3; k++) v[k] = v[k] * sc;
+      }
+      for (int k = 0; k < 3; k++) {
+        p[12 + k] = p[8 + k];
+        p[8 + k] = v[k];
+      }
+    }
+  }
+}

@@ -202,6 +202,21 @@ typedef struct orc_extract_cfg {
 void orc_extract(const orc_extract_cfg* cfg, const orc_field* f, float* motion, unsigned char* particles,
                  unsigned char* bodies, uint32_t* indices, uint32_t* draw_args, uint32_t* counters, uint32_t* id_grid);
 
+/* ---- sim/pbd.ts: ClaySolver.step (f32) ---- */
+typedef struct orc_solve_cfg {
+  float gravity[3];
+  float h;
+  float radius, friction, damping, max_speed;
+  float push[3];
+  uint32_t push_body;
+  float kick[3];
+  int32_t capacity, max_bodies, rot_iters, substeps, kicking;
+} orc_solve_cfg;
+void orc_solver_step(const orc_solve_cfg* cfg, const orc_field* world, unsigned char* particles, unsigned char* bodies,
+                     int body_count);
+/* the sin/cos shared with the CUDA path: sc = (sin x, cos x) */
+void orc_sincos_f32(float x, float sc[2]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -108,6 +108,15 @@ class ExtractCfg(C.Structure):
     ]
 
 
+class SolveCfg(C.Structure):
+    _fields_ = [
+        ("gravity", C.c_float * 3), ("h", C.c_float), ("radius", C.c_float), ("friction", C.c_float),
+        ("damping", C.c_float), ("max_speed", C.c_float), ("push", C.c_float * 3), ("push_body", C.c_uint32),
+        ("kick", C.c_float * 3), ("capacity", C.c_int32), ("max_bodies", C.c_int32), ("rot_iters", C.c_int32),
+        ("substeps", C.c_int32), ("kicking", C.c_int32),
+    ]
+
+
 BRUSH_DTYPE = np.dtype([
     ("pos", np.float32, 3), ("scale", np.float32), ("rot", np.float32, 4),
     ("size", np.float32, 3), ("radius", np.float32), ("material", np.float32),
@@ -163,6 +172,8 @@ def _declare(L):
     L.orc_build_brushes.argtypes = [C.POINTER(Volume), C.c_void_p, C.c_int32, u16p, u16p, C.c_int32]
     L.orc_eval_brush.argtypes = [C.c_void_p, f32p, C.c_int32, f32p]
     L.orc_field_query_mip_f32.argtypes = [C.POINTER(Field), f32p, C.c_int32, f32p, f32p]
+    L.orc_solver_step.argtypes = [C.POINTER(SolveCfg), C.POINTER(Field), C.c_void_p, C.c_void_p, C.c_int32]
+    L.orc_sincos_f32.argtypes = [C.c_float, f32p]
     L.orc_extract.argtypes = [C.POINTER(ExtractCfg), C.POINTER(Field), C.c_void_p, C.c_void_p, C.c_void_p, u32p,
                               u32p, u32p, u32p]
 
@@ -422,3 +433,36 @@ def extract(field: Field, particles: np.ndarray, bodies: np.ndarray, res: int, b
     lib().orc_extract(C.byref(cfg), C.byref(field), None if motion is None else motion.ctypes.data,
                       particles.ctypes.data, bodies.ctypes.data, idx, draw, cnt, grid)
     return idx, draw, cnt
+
+
+def solver_cfg(capacity, max_bodies, gravity=(0.0, -9.81, 0.0), dt=1 / 60, substeps=2, radius=0.1, friction=0.35,
+               damping=0.995, max_speed=40.0, rotation_iterations=2) -> SolveCfg:
+    """ClaySolverOptions after defaults (sim/pbd.ts:101-118) as the f32 SolveParams uniform."""
+    c = SolveCfg(h=float(np.float32(dt / substeps)), radius=float(np.float32(radius)),
+                 friction=float(np.float32(friction)), damping=float(np.float32(damping)),
+                 max_speed=float(np.float32(max_speed)), push_body=0xFFFFFFFF, capacity=capacity,
+                 max_bodies=max_bodies, rot_iters=rotation_iterations, substeps=substeps, kicking=0)
+    c.gravity[:] = [float(np.float32(g)) for g in gravity]
+    return c
+
+
+def solver_set_force(cfg: SolveCfg, body, accel, impulse=(0.0, 0.0, 0.0)):
+    cfg.push[:] = [float(np.float32(a)) for a in accel]
+    cfg.kick[:] = [float(np.float32(a)) for a in impulse]
+    cfg.push_body = int(body) & 0xFFFFFFFF
+    cfg.kicking = 1 if any(x != 0 for x in impulse) else 0
+
+
+def solver_step(cfg: SolveCfg, field: Field, particles: np.ndarray, bodies: np.ndarray, body_count: int):
+    """ClaySolver.step (sim/pbd.ts:396-416) in place on the ParticleSet records; the kick is
+    applied once (the flag is cleared, as the reference's `kicking`)."""
+    assert particles.flags["C_CONTIGUOUS"] and bodies.flags["C_CONTIGUOUS"]
+    lib().orc_solver_step(C.byref(cfg), C.byref(field), particles.ctypes.data, bodies.ctypes.data, int(body_count))
+    if body_count > 0:
+        cfg.kicking = 0
+
+
+def sincos(x: float):
+    out = np.zeros(2, np.float32)
+    lib().orc_sincos_f32(float(x), out)
+    return float(out[0]), float(out[1])
