@@ -22,6 +22,8 @@ constexpr int kSplatWarps = 8;  // warps per block of the splat pass
 constexpr int kSplatItems = 2048;  // compacted (brick, slice) items of the sphere block walk
 constexpr int kSplatAccVoxels = 4096;   // shared-memory minimum tile of the splat pass (spheres)
 constexpr int kSplatAccVoxelsDiscs = 4096;  // the same for oriented-disc clouds
+// the tile walk decodes items (< tile voxels x warps) by multiplication, exact below 2^16
+static_assert(kSplatAccVoxels <= 4096 && kSplatAccVoxels * kSplatWarps <= 65536, "item decode range");
 
 // FluidParticle (fluid.ts:20-26): (pos, density), (vel, pressure), (nvel, pad).
 struct __align__(16) ParticleDev {
@@ -1286,13 +1288,21 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       if (threadIdx.x == 0) s_nitems = 0u;
       __syncthreads();
       const uint32_t nall = ngroups * nsl;
+      // Item decode by multiplication: for x < 2^16 and 1 <= d < 2^15, floor(x * ceil(2^32 / d)
+      // / 2^32) == x / d (the excess x * (ceil - 2^32 / d) / 2^32 stays below 2^-16 < 1 / d).
+      // Items number below ngroups * nsl <= 4096 * 8, so every operand is in range.
+      const uint64_t m_groups = static_cast<uint64_t>(0xffffffffu / ngroups) + 1u;
+      const uint64_t m_gx = static_cast<uint64_t>(0xffffffffu / ngx) + 1u;
+      const uint64_t m_gy = static_cast<uint64_t>(0xffffffffu / ngy) + 1u;
+      auto divm = [](uint32_t x, uint64_t m) { return static_cast<uint32_t>((static_cast<uint64_t>(x) * m) >> 32); };
       auto brick_of = [&](uint32_t it, uint32_t& sl, uint32_t& lx0, uint32_t& ly0, uint32_t& lz0) {
-        sl = it / ngroups;
+        sl = divm(it, m_groups);
         const uint32_t g = it - sl * ngroups;
-        const uint32_t rest = g / ngx;
+        const uint32_t rest = divm(g, m_gx);
         lx0 = (g - rest * ngx) * 4u;  // brick corner in the union box
-        ly0 = (rest % ngy) * 2u;
-        lz0 = (rest / ngy) * 2u;
+        const uint32_t rz = divm(rest, m_gy);
+        ly0 = (rest - rz * ngy) * 2u;
+        lz0 = rz * 2u;
       };
       // a brick farther than the reach from a slice's bounding box: nothing to lower
       auto culled = [&](uint32_t sl, uint32_t lx0, uint32_t ly0, uint32_t lz0) {
@@ -1342,13 +1352,15 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
           cy[k] = (static_cast<float>(y0 + k) + 0.5f) * voxel;
           cz[k] = (static_cast<float>(z0 + k) + 0.5f) * voxel;
         }
-        float b[16];
+        // Minima of squared lengths as float bits (non-negative floats order like their bit
+        // patterns), two particles per step: the squared lengths keep the reference's rounding
+        // order (dx*dx + dy*dy) + dz*dz, and one three-input minimum folds both particles into
+        // a voxel's running minimum.
+        uint32_t b[16];
 #pragma unroll
-        for (int k = 0; k < 16; k++) b[k] = __int_as_float(0x7f800000);
-        const uint32_t j1 = min(nlive, (sl + 1u) * per);
-#pragma unroll 2
-        for (uint32_t j = sl * per; j < j1; j++) {
-          const float4 q = s_cp[j];
+        for (int k = 0; k < 16; k++) b[k] = 0x7f800000u;
+        // the 16 squared lengths of one particle, indexed xx + 4 * yy + 8 * zz
+        auto lengths = [&](const float4 q, uint32_t (&u)[16]) {
           float dx2[4], dy2[2], dz2[2];
 #pragma unroll
           for (int k = 0; k < 4; k++) {
@@ -1367,8 +1379,23 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
             for (int xx = 0; xx < 4; xx++) {
               const float t = dx2[xx] + dy2[yy];
 #pragma unroll
-              for (int zz = 0; zz < 2; zz++) b[xx + 4 * yy + 8 * zz] = fminf(b[xx + 4 * yy + 8 * zz], t + dz2[zz]);
+              for (int zz = 0; zz < 2; zz++) u[xx + 4 * yy + 8 * zz] = __float_as_uint(t + dz2[zz]);
             }
+        };
+        const uint32_t j1 = min(nlive, (sl + 1u) * per);
+        uint32_t j = sl * per;
+        for (; j + 1u < j1; j += 2u) {
+          uint32_t ua[16], ub[16];
+          lengths(s_cp[j], ua);
+          lengths(s_cp[j + 1u], ub);
+#pragma unroll
+          for (int k = 0; k < 16; k++) b[k] = __vimin3_u32(b[k], ua[k], ub[k]);
+        }
+        if (j < j1) {
+          uint32_t ua[16];
+          lengths(s_cp[j], ua);
+#pragma unroll
+          for (int k = 0; k < 16; k++) b[k] = min(b[k], ua[k]);
         }
 #pragma unroll
         for (int zz = 0; zz < 2; zz++)
@@ -1377,9 +1404,8 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
 #pragma unroll
             for (int xx = 0; xx < 4; xx++) {
               const uint32_t lx = lx0 + xx, ly = ly0 + yy, lz = lz0 + zz;
-              const float v = b[xx + 4 * yy + 8 * zz];
-              if (lx < ux && ly < uy && lz < uz && v < __int_as_float(0x7f800000))
-                atomicMin(&s_tile[lx + ux * (ly + uy * lz)], __float_as_uint(v));
+              const uint32_t v = b[xx + 4 * yy + 8 * zz];
+              if (lx < ux && ly < uy && lz < uz && v < 0x7f800000u) atomicMin(&s_tile[lx + ux * (ly + uy * lz)], v);
             }
       }
       __syncthreads();
@@ -1485,8 +1511,10 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     }
   }
   // Warp walks. When the block's union box fits in shared memory the minima are taken there
-  // first (shared-memory atomicMin) and written out with one global atomicMin per touched voxel;
-  // otherwise every hit goes to the key grid directly.
+  // first (shared-memory atomicMin of the distance as an order-preserving integer, so the key,
+  // a division, is taken once per voxel) and written out with one global atomicMin per touched
+  // voxel; otherwise every hit goes to the key grid directly. The key is monotone in the
+  // distance, so the key of the minimum is the minimum of the keys.
   extern __shared__ uint32_t s_acc[];  // acc_cap voxels of dynamic shared memory
   const int ax0 = s_box[0], ay0 = s_box[1], az0 = s_box[2];
   const uint32_t anx = static_cast<uint32_t>(s_box[3] - ax0 + 1), any = static_cast<uint32_t>(s_box[4] - ay0 + 1),
@@ -1494,15 +1522,17 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   const uint64_t an = static_cast<uint64_t>(anx) * any * anz;
   const bool use_acc = an <= static_cast<uint64_t>(acc_cap);
   if (use_acc) {
-    for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) s_acc[v] = 65535u;
+    for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) s_acc[v] = 0xffffffffu;
     __syncthreads();
   }
-  auto emit = [&](int x, int y, int z, uint32_t key) {
+  auto emit = [&](int x, int y, int z, float sd) {  // sd < bandWorld
     if (use_acc) {
       uint32_t a = static_cast<uint32_t>(x - ax0) + anx * (static_cast<uint32_t>(y - ay0) + any * static_cast<uint32_t>(z - az0));
-      atomicMin(&s_acc[a], key);
+      const uint32_t u = __float_as_uint(sd);
+      atomicMin(&s_acc[a], (u & 0x80000000u) ? ~u : (u | 0x80000000u));
     } else {
-      atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)), key);
+      atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
+                enc_key(sd, bw));
     }
   };
   const float reach2_hi = (bw + radius) * (bw + radius) * 1.00001f;
@@ -1551,7 +1581,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
             }
           }
         }
-        if (v < nu && best < bw) emit(x, y, z, enc_key(best, bw));
+        if (v < nu && best < bw) emit(x, y, z, best);
       }
     } else {
       uint32_t rem = active;
@@ -1580,7 +1610,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
           float t = (dx * dx + dy * dy) + dz * dz;
           if (t >= reach2_hi) continue;
           float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
-          if (sd < bw) emit(x, y, z, enc_key(sd, bw));
+          if (sd < bw) emit(x, y, z, sd);
         }
       }
     }
@@ -1588,12 +1618,14 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   if (use_acc) {
     __syncthreads();
     for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) {
-      uint32_t key = s_acc[v];
-      if (key < 65535u) {
+      const uint32_t u = s_acc[v];
+      if (u != 0xffffffffu) {
+        const float sd = __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
         int x = ax0 + static_cast<int>(v % anx);
         int y = ay0 + static_cast<int>((v / anx) % any);
         int z = az0 + static_cast<int>(v / (anx * any));
-        atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)), key);
+        atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
+                  enc_key(sd, bw));
       }
     }
   }
