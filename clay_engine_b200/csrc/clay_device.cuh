@@ -20,6 +20,7 @@ constexpr int kMaxMips = 8;
 constexpr uint32_t kMaxNbr = 64;  // neighbour-list slots per particle
 constexpr int kSplatWarps = 8;  // warps per block of the splat pass
 constexpr int kSplatItems = 2048;  // compacted (brick, slice) items of the sphere block walk
+constexpr int kSplatStencil = 2048;  // voxel offsets of the own-box walk's stencil (8 KB of shared memory)
 constexpr int kSplatAccVoxels = 4096;   // shared-memory minimum tile of the splat pass (spheres)
 constexpr int kSplatAccVoxelsDiscs = 4096;  // the same for oriented-disc clouds
 // the tile walk decodes items (< tile voxels x warps) by multiplication, exact below 2^16
@@ -1536,6 +1537,49 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     }
   };
   const float reach2_hi = (bw + radius) * (bw + radius) * 1.00001f;
+  // The own-box walk visits a stencil instead of a particle's whole box: the voxel offsets,
+  // relative to the voxel holding the particle, that lie within the reach of some point of
+  // one octant of that voxel (mirrored per axis to the particle's octant). Every voxel the
+  // particle can lower (squared length below reach2_hi, i.e. within the reach to 1e-5) is in
+  // it: the octant is widened by 0.02 voxel and the reach by 0.02 voxel, far above the f32
+  // rounding of the particle's voxel coordinates. With a band of 4 voxels it holds about half
+  // of the box's voxels, so lanes spend fewer steps outside the reach. Offsets are packed in
+  // 4 bits per axis; a reach beyond 6 voxels keeps the box walk.
+  __shared__ uint32_t s_st[kSplatStencil];
+  __shared__ uint32_t s_nst;
+  const float rv = reach * inv_voxel;
+  const int sn = static_cast<int>(ceilf(rv)) + 1;  // candidate offsets in [-sn, sn]
+  bool use_st = rv > 0.0f && sn <= 7;
+  if (use_st) {
+    if (threadIdx.x == 0) s_nst = 0u;
+    __syncthreads();
+    const uint32_t side = static_cast<uint32_t>(2 * sn + 1), cand = side * side * side;
+    const float lim = (rv + 0.02f) * (rv + 0.02f);
+    auto gap = [](int o) {  // distance from the centre at offset o to the widened octant [-0.02, 0.52]
+      const float f = static_cast<float>(o);
+      return f > 0.52f ? f - 0.52f : (f < -0.02f ? -0.02f - f : 0.0f);
+    };
+    for (uint32_t c0 = 0; c0 < cand; c0 += blockDim.x) {
+      const uint32_t c = c0 + threadIdx.x;
+      bool keep = false;
+      uint32_t e = 0;
+      if (c < cand) {
+        const int ox = static_cast<int>(c % side) - sn, oy = static_cast<int>((c / side) % side) - sn,
+                  oz = static_cast<int>(c / (side * side)) - sn;
+        const float gx = gap(ox), gy = gap(oy), gz = gap(oz);
+        keep = gx * gx + gy * gy + gz * gz < lim;
+        e = static_cast<uint32_t>(ox + 8) | (static_cast<uint32_t>(oy + 8) << 4) | (static_cast<uint32_t>(oz + 8) << 8);
+      }
+      const uint32_t m = __ballot_sync(0xffffffffu, keep);
+      uint32_t o = 0;
+      if (lane == 0 && m) o = atomicAdd(&s_nst, static_cast<uint32_t>(__popc(m)));
+      o = __shfl_sync(0xffffffffu, o, 0);
+      const uint32_t pos = o + __popc(m & ((1u << lane) - 1u));
+      if (keep && pos < static_cast<uint32_t>(kSplatStencil)) s_st[pos] = e;
+    }
+    __syncthreads();
+    use_st = s_nst <= static_cast<uint32_t>(kSplatStencil);
+  }
   if (active != 0u) {
     const uint32_t nux = static_cast<uint32_t>(uhx - ulx + 1), nuy = static_cast<uint32_t>(uhy - uly + 1),
                    nuz = static_cast<uint32_t>(uhz - ulz + 1);
@@ -1591,27 +1635,41 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
         float4 q = s_p[wid][j];
         float4 nn = s_n[wid][j];
         int4 lo = s_lo[wid][j], hi = s_hi[wid][j];
-        uint32_t bxn = static_cast<uint32_t>(hi.x - lo.x + 1), byn = static_cast<uint32_t>(hi.y - lo.y + 1),
-                 bzn = static_cast<uint32_t>(hi.z - lo.z + 1);
-        uint32_t nb = bxn * byn * bzn;
-        BoxWalk bw_;
-        bw_.init(lane, bxn, byn);
-        for (uint32_t v = lane; v < nb; v += 32, bw_.next()) {
-          int x = lo.x + bw_.x;
-          int y = lo.y + bw_.y;
-          int z = lo.z + bw_.z;
+        auto visit = [&](int x, int y, int z) {
           float dx = (static_cast<float>(x) + 0.5f) * voxel - q.x;
           float dy = (static_cast<float>(y) + 0.5f) * voxel - q.y;
           float dz = (static_cast<float>(z) + 0.5f) * voxel - q.z;
           // a voxel whose plane term or squared length already puts it at or beyond the band
           // cannot pass sd < bandWorld: skip its square root
           float pl = has_n ? dot3(dx, dy, dz, nn.x, nn.y, nn.z) : -__int_as_float(0x7f800000);
-          if (pl >= bw) continue;
+          if (pl >= bw) return;
           float t = (dx * dx + dy * dy) + dz * dz;
-          if (t >= reach2_hi) continue;
+          if (t >= reach2_hi) return;
           float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
           if (sd < bw) emit(x, y, z, sd);
+        };
+        if (use_st) {
+          const float fx = q.x * inv_voxel, fy = q.y * inv_voxel, fz = q.z * inv_voxel;
+          const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
+          const int cxv = f2i(flx), cyv = f2i(fly), czv = f2i(flz);
+          const int sx = fx - flx >= 0.5f ? 1 : -1, sy = fy - fly >= 0.5f ? 1 : -1, sz = fz - flz >= 0.5f ? 1 : -1;
+          const uint32_t ns = s_nst;
+          for (uint32_t v = lane; v < ns; v += 32) {
+            const uint32_t e = s_st[v];
+            const int x = cxv + sx * (static_cast<int>(e & 15u) - 8);
+            const int y = cyv + sy * (static_cast<int>((e >> 4) & 15u) - 8);
+            const int z = czv + sz * (static_cast<int>((e >> 8) & 15u) - 8);
+            if (x < lo.x || x > hi.x || y < lo.y || y > hi.y || z < lo.z || z > hi.z) continue;
+            visit(x, y, z);
+          }
+          continue;
         }
+        uint32_t bxn = static_cast<uint32_t>(hi.x - lo.x + 1), byn = static_cast<uint32_t>(hi.y - lo.y + 1),
+                 bzn = static_cast<uint32_t>(hi.z - lo.z + 1);
+        uint32_t nb = bxn * byn * bzn;
+        BoxWalk bw_;
+        bw_.init(lane, bxn, byn);
+        for (uint32_t v = lane; v < nb; v += 32, bw_.next()) visit(lo.x + bw_.x, lo.y + bw_.y, lo.z + bw_.z);
       }
     }
   }

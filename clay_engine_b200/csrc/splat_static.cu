@@ -83,6 +83,10 @@ int static_keys_address(uint32_t** out) {
     e = cudaGetSymbolAddress(&p, g_static_keys);
     if (e != cudaSuccess || !p)
       return report_error(CLAY_ECUDA, "clay_splat_bake_static: cudaGetSymbolAddress of the scratch keys failed");
+    // the splat's static shared memory plus its tile exceed the default 48 KB per block
+    e = cudaFuncSetAttribute(k_static_splat, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSplatAccVoxels * static_cast<int>(sizeof(uint32_t)));
+    if (e != cudaSuccess) return report_error(CLAY_ECUDA, "clay_splat_bake_static: cudaFuncSetAttribute failed");
     g_addr[dev] = static_cast<uint32_t*>(p);
   }
   *out = g_addr[dev];
