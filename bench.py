@@ -406,8 +406,8 @@ BYTES_PER_PARTICLE = {
 }
 # DRAM bytes (read + written) per particle of one k_splat launch over the fluid surfaces (3
 # levels), from the ncu capture summarised in profiles/k_splat_batched_128_scenes.md:
-# 107,436,288 + 5,356,032 bytes for 1,940,550 particles.
-SPLAT_TRAFFIC_PER_PARTICLE = (107436288 + 5356032) / 1940550
+# 107,385,856 + 4,627,712 bytes for 1,940,550 particles.
+SPLAT_TRAFFIC_PER_PARTICLE = (107385856 + 4627712) / 1940550
 
 
 def main():
@@ -548,7 +548,7 @@ def main():
         roof.update({"achieved": achieved, "frac": achieved / peak,
                      "traffic": SPLAT_TRAFFIC_PER_PARTICLE * particles,
                      "algorithmic_bytes_per_launch": splat_bytes, "avg_launch_ms": avg_ms,
-                     "limiter": "instruction issue (ncu: ~82% issue active, DRAM ~1% of peak)"})
+                     "limiter": "instruction issue (ncu: ~80% issue active, DRAM ~1% of peak)"})
     # the neighbour passes against the same peak (one launch per block-size group and substep)
     others = {}
     for name, per in BYTES_PER_PARTICLE.items():
