@@ -1291,10 +1291,13 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       const uint32_t nall = ngroups * nsl;
       // Item decode by multiplication: for x < 2^16 and 1 <= d < 2^15, floor(x * ceil(2^32 / d)
       // / 2^32) == x / d (the excess x * (ceil - 2^32 / d) / 2^32 stays below 2^-16 < 1 / d).
-      // Items number below ngroups * nsl <= 4096 * 8, so every operand is in range.
+      // Items number below ngroups * nsl <= 4096 * 8 and tile voxels below 4096, so every
+      // operand is in range.
       const uint64_t m_groups = static_cast<uint64_t>(0xffffffffu / ngroups) + 1u;
       const uint64_t m_gx = static_cast<uint64_t>(0xffffffffu / ngx) + 1u;
       const uint64_t m_gy = static_cast<uint64_t>(0xffffffffu / ngy) + 1u;
+      const uint64_t m_ux = static_cast<uint64_t>(0xffffffffu / ux) + 1u;
+      const uint64_t m_uy = static_cast<uint64_t>(0xffffffffu / uy) + 1u;
       auto divm = [](uint32_t x, uint64_t m) { return static_cast<uint32_t>((static_cast<uint64_t>(x) * m) >> 32); };
       auto brick_of = [&](uint32_t it, uint32_t& sl, uint32_t& lx0, uint32_t& ly0, uint32_t& lz0) {
         sl = divm(it, m_groups);
@@ -1345,13 +1348,16 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
         brick_of(it, sl, lx0, ly0, lz0);
         if (!compact && culled(sl, lx0, ly0, lz0)) continue;
         const int x0 = bx0 + static_cast<int>(lx0), y0 = by0 + static_cast<int>(ly0), z0 = bz0 + static_cast<int>(lz0);
+        // voxel centres (x + 0.5) * voxel: one conversion per axis, since float(x0) + (k + 0.5)
+        // equals float(x0 + k) + 0.5 exactly for grid coordinates (integers far below 2^23)
         float cx[4], cy[2], cz[2];
+        const float fx0 = static_cast<float>(x0), fy0 = static_cast<float>(y0), fz0 = static_cast<float>(z0);
 #pragma unroll
-        for (int k = 0; k < 4; k++) cx[k] = (static_cast<float>(x0 + k) + 0.5f) * voxel;
+        for (int k = 0; k < 4; k++) cx[k] = (fx0 + (static_cast<float>(k) + 0.5f)) * voxel;
 #pragma unroll
         for (int k = 0; k < 2; k++) {
-          cy[k] = (static_cast<float>(y0 + k) + 0.5f) * voxel;
-          cz[k] = (static_cast<float>(z0 + k) + 0.5f) * voxel;
+          cy[k] = (fy0 + (static_cast<float>(k) + 0.5f)) * voxel;
+          cz[k] = (fz0 + (static_cast<float>(k) + 0.5f)) * voxel;
         }
         // Minima of squared lengths as float bits (non-negative floats order like their bit
         // patterns), two particles per step: the squared lengths keep the reference's rounding
@@ -1415,8 +1421,8 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
         if (bits == 0x7f800000u) continue;
         const float sd = __fsqrt_rn(__uint_as_float(bits)) - radius;
         if (sd < bw) {
-          const int x = bx0 + static_cast<int>(v % ux), y = by0 + static_cast<int>((v / ux) % uy),
-                    z = bz0 + static_cast<int>(v / (ux * uy));
+          const uint32_t vy = divm(v, m_ux), vz = divm(vy, m_uy);  // v < 4096: decode by multiplication
+          const int x = bx0 + static_cast<int>(v - vy * ux), y = by0 + static_cast<int>(vy - vz * uy), z = bz0 + static_cast<int>(vz);
           atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
                     enc_key(sd, bw));
         }
@@ -1547,6 +1553,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   // 4 bits per axis; a reach beyond 6 voxels keeps the box walk.
   __shared__ uint32_t s_st[kSplatStencil];
   __shared__ uint32_t s_nst;
+  __shared__ float2 s_dt[kSplatWarps][3][16];  // per warp: the current particle's per-axis terms
   const float rv = reach * inv_voxel;
   const int sn = static_cast<int>(ceilf(rv)) + 1;  // candidate offsets in [-sn, sn]
   bool use_st = rv > 0.0f && sn <= 7;
@@ -1653,15 +1660,36 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
           const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
           const int cxv = f2i(flx), cyv = f2i(fly), czv = f2i(flz);
           const int sx = fx - flx >= 0.5f ? 1 : -1, sy = fy - fly >= 0.5f ? 1 : -1, sz = fz - flz >= 0.5f ? 1 : -1;
+          // Per axis, the 15 voxel offsets the stencil can reach (-7..7) as (d * n, d * d) with
+          // d = centre - particle: the same operations visit() does per voxel, done once per
+          // particle; a voxel then adds them as (dx*nx + dy*ny) + dz*nz and (dx*dx + dy*dy) +
+          // dz*dz, the reference's rounding order.
+          if (lane < 30) {
+            const int axis = lane >= 15 ? 1 : 0, o = static_cast<int>(lane) - 15 * axis - 7;
+            const float d = (static_cast<float>((axis ? cyv : cxv) + o) + 0.5f) * voxel - (axis ? q.y : q.x);
+            s_dt[wid][axis][o + 7] = make_float2(d * (axis ? nn.y : nn.x), d * d);
+          }
+          if (lane < 15) {
+            const float d = (static_cast<float>(czv + static_cast<int>(lane) - 7) + 0.5f) * voxel - q.z;
+            s_dt[wid][2][lane] = make_float2(d * nn.z, d * d);
+          }
+          __syncwarp();
           const uint32_t ns = s_nst;
           for (uint32_t v = lane; v < ns; v += 32) {
             const uint32_t e = s_st[v];
-            const int x = cxv + sx * (static_cast<int>(e & 15u) - 8);
-            const int y = cyv + sy * (static_cast<int>((e >> 4) & 15u) - 8);
-            const int z = czv + sz * (static_cast<int>((e >> 8) & 15u) - 8);
+            const int mx = sx * (static_cast<int>(e & 15u) - 8), my = sy * (static_cast<int>((e >> 4) & 15u) - 8),
+                      mz = sz * (static_cast<int>((e >> 8) & 15u) - 8);
+            const int x = cxv + mx, y = cyv + my, z = czv + mz;
             if (x < lo.x || x > hi.x || y < lo.y || y > hi.y || z < lo.z || z > hi.z) continue;
-            visit(x, y, z);
+            const float2 tx = s_dt[wid][0][mx + 7], ty = s_dt[wid][1][my + 7], tz = s_dt[wid][2][mz + 7];
+            const float pl = has_n ? (tx.x + ty.x) + tz.x : -__int_as_float(0x7f800000);
+            if (pl >= bw) continue;
+            const float t = (tx.y + ty.y) + tz.y;
+            if (t >= reach2_hi) continue;
+            const float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
+            if (sd < bw) emit(x, y, z, sd);
           }
+          __syncwarp();  // the tables are rewritten for the next particle
           continue;
         }
         uint32_t bxn = static_cast<uint32_t>(hi.x - lo.x + 1), byn = static_cast<uint32_t>(hi.y - lo.y + 1),
