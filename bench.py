@@ -49,6 +49,7 @@ def parse():
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="requests per second")
     ap.add_argument("--serve-pool", type=int, default=1024, help="resident scenes of the serving pool")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-next", action="store_true", help="skip the measurements of the rows after the frame")
     ap.add_argument("--workload", default="batched", choices=["batched", "tap"],
                     help="batched: the 256-scene batch (+plain, served); tap: one 262,144-particle scene fed by a tap")
     return ap.parse_args()
@@ -318,6 +319,176 @@ def cpu_sample(n_scenes, seed, max_particles, threads, frames=1):
     return total * frames / dt, total * frames, dt, desc
 
 
+def _event_ms(stream, fn, reps):
+    """Device time of `reps` calls of fn() on `stream` (CUDA events on that stream), in ms."""
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def _cpu_s(fn):
+    t = time.perf_counter()
+    fn()
+    return time.perf_counter() - t
+
+
+def body_set(shell, normals, centers, capacity=None):
+    """A ParticleSet holding one surface-net shell per centre: 96-byte Particle and 64-byte Body
+    records (particles.ts:18-68), rest shape relative to the body centre."""
+    from clay_engine_b200 import scenes
+
+    n = len(shell)
+    cap = capacity or n * len(centers)
+    parts = np.zeros(cap, scenes.PARTICLE_RECORD)
+    bodies = np.zeros(len(centers), scenes.BODY_RECORD)
+    for b, c in enumerate(centers):
+        sl = slice(b * n, (b + 1) * n)
+        parts["pos"][sl] = shell + np.asarray(c, np.float32)
+        parts["prev"][sl] = parts["pos"][sl]
+        parts["rest"][sl] = shell
+        parts["restNormal"][sl] = normals
+        parts["body"][sl] = b
+        parts["material"][sl] = 0.5
+        bodies["com"][b], bodies["first"][b], bodies["count"][b] = c, b * n, n
+        bodies["rot"][b] = (0.0, 0.0, 0.0, 1.0)
+        bodies["stiffness"][b] = 0.8
+    return parts, bodies
+
+
+def measure_next_rows(root, stream, threads):
+    """The rows after the frame, each measured as the frame is: device throughput with CUDA
+    events on the launching stream, achieved GB/s from algorithmic bytes, and the oracle on the
+    host cores on the same inputs (a bounded sample where the full case would take long)."""
+    import torch
+
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import brushes as B
+    from clay_engine_b200 import scenes
+    from oracle import oracle
+
+    oracle.build()
+    out = {}
+    origin = (-12.0, -4.0, -12.0)
+
+    # 1. collider build (SdfBuilder brush fold): config 2's 192^3 world volume from 64 brushes
+    br = scenes.random_brushes(64, seed=2024)
+    vol = ce.SdfVolume(root, resolution=192, worldSize=24.0, origin=origin)
+    vol.build(br, stream)
+    ms = _event_ms(stream, lambda: vol.build(br, stream), 5) / 5
+    vox = vol.totalVoxels
+    cpu_vd = oracle.VolumeData(96, 3, origin, 24.0, 4.0)
+    cpu_vox = oracle.total_voxels(96, 3)
+    cs = _cpu_s(lambda: oracle.build_brushes(cpu_vd, br, threads=threads))
+    out["collider_build"] = {
+        "workload": f"192^3 x {vol.mipLevels} levels from 64 brushes", "value": vox / (ms / 1e3), "unit": "voxels/s",
+        "ms_per_build": ms, "achieved_gbs": vox * 4 / (ms / 1e3) / 1e9, "bytes_per_voxel": 4,
+        "bound": "fp32 (the brush fold per voxel)",
+        "cpu_baseline": {"value": cpu_vox / cs, "unit": "voxels/s", "cores": threads, "kind": "port",
+                         "sample": "the same 64 brushes into a 96^3 x 3 volume"}}
+
+    # 2. level sampling: sample(p, mip) and field(p, mip) of that volume at 4M device points
+    field = ce.volumeField(vol)
+    n = 1 << 22
+    g = torch.Generator(device="cuda").manual_seed(7)
+    lo = torch.tensor(origin, device="cuda")
+    pts = (torch.rand(n, 3, device="cuda", generator=g) * 24.0 + lo).contiguous()
+    sxy = torch.empty(n, 2, device="cuda")
+    fxy = torch.empty(n, 2, device="cuda")
+    dist, mat = vol.download()
+    ovd = oracle.VolumeData(192, vol.mipLevels, origin, 24.0, 4.0, dist=dist, mat=mat)
+    ofield = oracle.make_field([ovd])
+    hp = pts[: 1 << 18].cpu().numpy()
+    levels = {}
+    for m in range(vol.mipLevels):
+        field.query_mip_device(pts, sxy, fxy, m, stream)
+        ms = _event_ms(stream, lambda: field.query_mip_device(pts, sxy, fxy, m, stream), 5) / 5
+        cs = _cpu_s(lambda: oracle.field_query_mip_batch(ofield, hp, m, threads=threads))
+        levels[str(m)] = {"value": n / (ms / 1e3), "ms": ms, "achieved_gbs": n * 28 / (ms / 1e3) / 1e9,
+                          "cpu_value": len(hp) / cs}
+    out["field_sample_mip"] = {
+        "workload": f"4,194,304 uniform points over the 192^3 volume, levels 0..{vol.mipLevels - 1}",
+        "unit": "samples/s", "bytes_per_sample": 28, "bound": "L2/L1 latency of the trilinear gathers",
+        "levels": levels, "cpu_baseline": {"unit": "samples/s", "cores": threads, "kind": "port",
+                                           "sample": "262,144 of the points per level"}}
+
+    # 3. SurfaceExtractor: the config-3 clay body (sphere r = 0.95) from a 64^3 bake of it, at the
+    # game's lattice (32^3) and at 128^3
+    box = 32 * 0.083
+    bo = (-box / 2,) * 3
+    sv = ce.SdfVolume(root, resolution=64, worldSize=box, origin=bo, mipLevels=1)
+    sv.build(B.make_brush("sphere", pos=(0.0, 0.0, 0.0), size=0.95))
+    sfield = ce.volumeField(sv)
+    sd, smat = sv.download()
+    sofield = oracle.make_field([oracle.VolumeData(64, 1, bo, box, 4.0, dist=sd, mat=smat)])
+    ext = {}
+    for res in (32, 128):
+        cap = 65536
+        parts = torch.zeros(cap * 96, dtype=torch.uint8, device="cuda")
+        bodies = torch.zeros(64, dtype=torch.uint8, device="cuda")
+        x = ce.SurfaceExtractor(root, parts, cap, bodies, 1, sfield, 0, 0, cap, resolution=res)
+        x.setRegion(bo, box)
+        x.extract(stream)
+        reps = 50 if res == 32 else 10
+        ms = _event_ms(stream, lambda: x.extract(stream), reps) / reps
+        nv = int(x.counts(stream)[0])
+        hpart = np.zeros(cap, scenes.PARTICLE_RECORD)
+        hbody = np.zeros(1, scenes.BODY_RECORD)
+        cs = _cpu_s(lambda: oracle.extract(sofield, hpart, hbody, res, 0, 0, cap, bo, box))
+        ext[str(res)] = {"cells": res ** 3, "particles": nv, "ms_per_extract": ms, "value": res ** 3 / (ms / 1e3),
+                         "achieved_gbs": (nv * 96 + res ** 3 * 36) / (ms / 1e3) / 1e9, "cpu_value": res ** 3 / cs}
+        x.destroy()
+    out["extract"] = {"workload": "surface nets of the clay-body sphere (r 0.95) over its 2.656 m box",
+                      "unit": "lattice cells/s", "bytes": "96 B per particle + 36 B scratch per cell",
+                      "bound": "field samples (8 + 9 per vertex cell, 4 per lattice point)", "lattices": ext,
+                      "cpu_baseline": {"unit": "lattice cells/s", "cores": 1, "kind": "port", "sample": "the same"}}
+
+    # 4. ClaySolver: 86 clay bodies (config 3's shell, 3,800 particles each) over a config-3
+    # collider, default options (2 substeps)
+    shell, shell_n = scenes.surface_net_sphere(0.95, 0.067)
+    wv = ce.SdfVolume(root, resolution=64, worldSize=24.0, origin=scenes.WORLD_ORIGIN)
+    wbr = scenes.random_brushes(8, seed=99, lo=(-10, -3.5, -10), hi=(10, 1.0, 10))
+    wv.build(wbr)
+    world = ce.volumeField(wv)
+    rng = np.random.default_rng(5)
+    centers = [(float(a), 2.5, float(c)) for a, c in rng.uniform(-9, 9, (86, 2))]
+    hparts, hbodies = body_set(shell, shell_n, centers)
+    dparts = torch.from_numpy(hparts.view(np.uint8).copy()).cuda()
+    dbodies = torch.from_numpy(hbodies.view(np.uint8).copy()).cuda()
+    solver = ce.ClaySolver(root, dparts, len(hparts), dbodies, len(hbodies), world)
+    for _ in range(3):
+        solver.step(len(hbodies), stream)
+    frames = 20
+    ms = _event_ms(stream, lambda: solver.step(len(hbodies), stream), frames) / frames
+    npart = len(hparts)
+    wd, wm = wv.download()
+    wfield = oracle.make_field([oracle.VolumeData(64, wv.mipLevels, scenes.WORLD_ORIGIN, 24.0, 4.0, dist=wd, mat=wm)])
+    sp, sb = body_set(shell, shell_n, centers[:8])
+    cfg = oracle.solver_cfg(len(sp), len(sb))
+    cs = _cpu_s(lambda: oracle.solver_step(cfg, wfield, sp, sb, len(sb)))
+    # per particle and substep: predict reads the record (96 B) and writes pos + prev (24 B),
+    # match reads pos + rest twice (48 B), apply reads the record and writes pos (+ prev) (120 B),
+    # finalize reads pos, prev, vel (36 B) and writes vel, velPrev (24 B)
+    per = 96 + 24 + 48 + 96 + 24 + 36 + 24
+    out["solver"] = {"workload": f"86 bodies x {len(shell)} particles, 2 substeps, 2 rotation iterations",
+                     "value": npart / (ms / 1e3), "unit": "particle-steps/s", "ms_per_step": ms,
+                     "achieved_gbs": npart * 2 * per / (ms / 1e3) / 1e9, "bytes_per_particle_substep": per,
+                     "launches_per_step": 8,
+                     "cpu_baseline": {"value": len(sp) / cs, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+                                      "sample": f"8 of the bodies ({len(sp)} particles), 1 step"}}
+    solver.destroy()
+    for f in (world, sfield, field):
+        f.destroy()
+    for v in (wv, sv, vol):
+        v.destroy()
+    return out
+
+
 def run_tap(root, args, stream, seed):
     """The plain method at scale: one scene of capacity 262,144 over a 192^3 collider of 64
     seeded brushes, baked into 128^3 x 4 (band 4), fed each frame by spawn(4096) at a tap with
@@ -569,6 +740,9 @@ def main():
     served = None
     if not args.no_serve and not args.small:
         served = run_serving(root, args, seed + 50, stream)
+    next_rows = None
+    if rank == 0 and ws == 1 and not args.small and not args.no_next:
+        next_rows = measure_next_rows(root, stream, os.cpu_count() or 1)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, total, dt, desc = cpu_sample(n_scenes, seed, 1_500_000, os.cpu_count() or 1, frames=2)
@@ -601,6 +775,7 @@ def main():
             "frame_ms_unfused": frame_ms,
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
+            "next_rows": next_rows,
         }
         print(json.dumps(line), flush=True)
 

@@ -166,6 +166,7 @@ SIGNATURES = {
     "clay_field_destroy": (None, [P]),
     "clay_field_query": (I, [P, P, I, P, P, P]),
     "clay_field_query_mip": (I, [P, P, I, I, P, P, P]),
+    "clay_field_query_mip_device": (I, [P, P, I, I, P, P, P]),
     "clay_field_band_voxel": (I, [P, I, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "clay_splat_create": (I, [P, C.POINTER(CloudDesc), C.POINTER(SplatOpts), C.POINTER(P)]),
     "clay_splat_destroy": (None, [P]),

@@ -184,6 +184,18 @@ class TracedField:
                                          f.ctypes.data, None))
         return s, f
 
+    def query_mip_device(self, points, sample_xy, field_xy, mip: int, stream=None):
+        """sample(p, mip) and field(p, mip) at device points into device (x, y) pairs: CUDA
+        tensors (n x 3 and n x 2 float32), asynchronous on `stream`, nothing allocated."""
+        import torch
+
+        n = int(points.shape[0])
+        for t, w in ((points, 3), (sample_xy, 2), (field_xy, 2)):
+            if not t.is_cuda or t.dtype != torch.float32 or tuple(t.shape) != (n, w) or not t.is_contiguous():
+                raise ValueError("query_mip_device: contiguous float32 CUDA tensors of n x 3, n x 2, n x 2")
+        check(lib().clay_field_query_mip_device(self.handle, points.data_ptr(), n, int(mip), sample_xy.data_ptr(),
+                                                field_xy.data_ptr(), stream_handle(stream)))
+
     def bandWorld(self, mip: int) -> float:
         return self._band_voxel(mip)[0]
 

@@ -759,6 +759,19 @@ int clay_field_query_mip(const clay_field* f, const float* pts, int n, int mip, 
   return CLAY_OK;
 }
 
+int clay_field_query_mip_device(const clay_field* f, const float* pts, int n, int mip, float* sample_xy, float* field_xy,
+                                void* stream) {
+  if (!f || n < 0 || (n > 0 && (!pts || !sample_xy || !field_xy)))
+    return fail(CLAY_EINVAL, "clay_field_query_mip_device: bad argument");
+  if (mip < 0) return fail(CLAY_EINVAL, "clay_field_query_mip_device: mip %d < 0", mip);
+  if (n == 0) return CLAY_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = const_cast<clay_field*>(f)->flush(s);
+  if (rc) return rc;
+  CK(L_field_query_mip(f->d, pts, n, mip, sample_xy, field_xy, s));
+  return CLAY_OK;
+}
+
 int clay_field_band_voxel(const clay_field* f, int mip, float* band_world, float* voxel_world) {
   if (!f || !band_world || !voxel_world || mip < 0) return fail(CLAY_EINVAL, "clay_field_band_voxel: bad argument");
   if (f->leaves.empty()) return fail(CLAY_ESTATE, "clay_field_band_voxel: empty field");

@@ -166,6 +166,11 @@ int clay_field_query(const clay_field* f, const float* points_xyz, int n, float*
  * (distance, raw) and (distance, material) pairs. Test and tool hook (allocates). */
 int clay_field_query_mip(const clay_field* f, const float* pts, int n, int mip, float* sample_xy, float* field_xy,
                          void* stream);
+/* The same with every pointer in device memory, asynchronous on `stream`, allocating nothing:
+ * sampling by a device-side consumer of the baked volume (the reference's tracer samples the
+ * same way from its shaders). */
+int clay_field_query_mip_device(const clay_field* f, const float* pts, int n, int mip, float* sample_xy,
+                                float* field_xy, void* stream);
 /* bandWorld(mip) and voxelWorld(mip) of the field (trace/field.ts:151-155, 294-305): the
  * smallest band and the largest voxel over the union's volumes, each at its capped level. */
 int clay_field_band_voxel(const clay_field* f, int mip, float* band_world, float* voxel_world);

@@ -1237,6 +1237,15 @@ void orc_field_query_mip_f32(const orc_field* f, const float p[3], int mip, floa
   field_xy[1] = best[2];
 }
 
+void orc_field_query_mip_batch(const orc_field* f, const float* pts, int64_t n, int mip, float* sample_xy,
+                               float* field_xy, int threads) {
+#ifdef _OPENMP
+  omp_set_num_threads(threads > 0 ? threads : 1);
+#endif
+#pragma omp parallel for schedule(static) if (threads > 1)
+  for (int64_t i = 0; i < n; i++) orc_field_query_mip_f32(f, pts + 3 * i, mip, sample_xy + 2 * i, field_xy + 2 * i);
+}
+
 // ----------------------------------------------------------------------------------------
 // SurfaceExtractor.extract (sim/extract.ts:194-436) in f32, with the slot order of the CUDA
 // path: dual vertices in lattice order, quads by lattice point then +x, +y, +z edge (the

@@ -185,6 +185,9 @@ float orc_f16_to_f32(uint16_t h);
 
 /* ---- trace/field.ts: sample(p, mip) and field(p, mip), level capped (f32) ---- */
 void orc_field_query_mip_f32(const orc_field* f, const float p[3], int mip, float sample_xy[2], float field_xy[2]);
+/* the same over n points (xyz triples), OpenMP over points: the CPU leg of the sampling measurement */
+void orc_field_query_mip_batch(const orc_field* f, const float* pts, int64_t n, int mip, float* sample_xy,
+                               float* field_xy, int threads);
 
 /* ---- sim/extract.ts: SurfaceExtractor.extract (f32) ---- */
 typedef struct orc_extract_cfg {

@@ -172,6 +172,7 @@ def _declare(L):
     L.orc_build_brushes.argtypes = [C.POINTER(Volume), C.c_void_p, C.c_int32, u16p, u16p, C.c_int32]
     L.orc_eval_brush.argtypes = [C.c_void_p, f32p, C.c_int32, f32p]
     L.orc_field_query_mip_f32.argtypes = [C.POINTER(Field), f32p, C.c_int32, f32p, f32p]
+    L.orc_field_query_mip_batch.argtypes = [C.POINTER(Field), f32p, C.c_int64, C.c_int32, f32p, f32p, C.c_int32]
     L.orc_solver_step.argtypes = [C.POINTER(SolveCfg), C.POINTER(Field), C.c_void_p, C.c_void_p, C.c_int32]
     L.orc_sincos_f32.argtypes = [C.c_float, f32p]
     L.orc_extract.argtypes = [C.POINTER(ExtractCfg), C.POINTER(Field), C.c_void_p, C.c_void_p, C.c_void_p, u32p,
@@ -261,6 +262,15 @@ def field_query_mip_f32(field: Field, pts: np.ndarray, mip: int):
     for i, p in enumerate(pts):
         lib().orc_field_query_mip_f32(C.byref(field), np.ascontiguousarray(p), int(mip), o2, o2b)
         s[i], f[i] = o2, o2b
+    return s, f
+
+
+def field_query_mip_batch(field: Field, pts: np.ndarray, mip: int, threads=1):
+    """field_query_mip_f32 over all points in one call (OpenMP over points)."""
+    pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+    s = np.zeros((len(pts), 2), np.float32)
+    f = np.zeros((len(pts), 2), np.float32)
+    lib().orc_field_query_mip_batch(C.byref(field), pts, len(pts), int(mip), s, f, int(threads))
     return s, f
 
 

@@ -61,3 +61,29 @@ def test_levels_capped_union_offset(root, oracle):
         assert np.abs(s[:, 0]).max() < 8.0 / 128 * 2 ** mip, mip
     for x in (ws, fu, world, body):
         x.destroy()
+
+
+def test_device_points_match_the_host_hook(root, oracle):
+    """clay_field_query_mip_device (device pointers, nothing allocated) gives what the host hook
+    gives, at every level."""
+    import torch
+
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    v = ce.SdfVolume(root, resolution=64, worldSize=24.0, origin=scenes.WORLD_ORIGIN)
+    v.build(scenes.random_brushes(8, seed=31, lo=(-10, -3.5, -10), hi=(10, 1.0, 10)))
+    f = ce.volumeField(v)
+    pts = np.random.default_rng(3).uniform(-11.0, 11.0, (5000, 3)).astype(np.float32)
+    dp = torch.from_numpy(pts).cuda()
+    s = torch.empty(len(pts), 2, device="cuda")
+    g = torch.empty(len(pts), 2, device="cuda")
+    for m in range(v.mipLevels + 1):
+        hs, hf = f.query_mip(pts, m)
+        f.query_mip_device(dp, s, g, m)
+        torch.cuda.synchronize()
+        assert np.array_equal(hs, s.cpu().numpy()) and np.array_equal(hf, g.cpu().numpy())
+    with pytest.raises(ValueError):
+        f.query_mip_device(dp.cpu(), s, g, 0)
+    f.destroy()
+    v.destroy()
