@@ -435,10 +435,9 @@ int make_splat(clay_ctx* ctx, const clay_cloud_desc* cloud, const clay_splat_opt
   void* p = nullptr;
   if ((rc = ctx->dev_alloc(&p, sizeof(uint32_t) * vol->total))) goto fail_out;
   s->keys = static_cast<uint32_t*>(p);
-  // The key grid holds 65535 between bakes (see k_resolve).
+  // The key grid holds kNoHit (all bits set) between bakes (see k_resolve).
   {
-    std::vector<uint32_t> sat(static_cast<size_t>(vol->total), 65535u);
-    cudaMemcpy(s->keys, sat.data(), sizeof(uint32_t) * vol->total, cudaMemcpyHostToDevice);
+    cudaMemset(s->keys, 0xff, sizeof(uint32_t) * vol->total);
     // The material channel is the constant `material` (splat.ts:273): written once here.
     uint16_t mh;
     __half hm = __float2half_rn(static_cast<float>(material));

@@ -1029,6 +1029,19 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
 // `sd < bandWorld` (splat.ts:246). For spheres the minimum is taken over squared lengths:
 // sqrt and the subtraction of the radius are both monotone in f32.
 
+// The key grid holds, per voxel, the smallest distance lowered into it so far as an
+// order-preserving integer of its f32 bits (negative values flipped whole, positive ones with
+// the sign bit set): kNoHit until a particle reaches the voxel. The reference's key is a
+// monotone function of the distance, so the key of the smallest distance, taken once per
+// voxel by the resolve pass, equals the smallest of the keys the reference's atomicMin keeps;
+// the splat passes never divide.
+constexpr uint32_t kNoHit = 0xffffffffu;
+__device__ __forceinline__ uint32_t sd_bits(float sd) {
+  const uint32_t u = __float_as_uint(sd);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float bits_sd(uint32_t u) { return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u); }
+
 __device__ __forceinline__ uint32_t enc_key(float sd, float bw) {
   float v = clampf(__fdiv_rn(sd, bw), -1.0f, 1.0f);
   return static_cast<uint32_t>((v + 1.0f) * 32767.5f);
@@ -1424,7 +1437,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
           const uint32_t vy = divm(v, m_ux), vz = divm(vy, m_uy);  // v < 4096: decode by multiplication
           const int x = bx0 + static_cast<int>(v - vy * ux), y = by0 + static_cast<int>(vy - vz * uy), z = bz0 + static_cast<int>(vz);
           atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
-                    enc_key(sd, bw));
+                    sd_bits(sd));
         }
       }
       return;
@@ -1511,7 +1524,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
         for (int k = 0; k < 4; k++) {
           if (x0 + k <= bhx && b[k] < bw)
             atomicMin(keys + (static_cast<long long>(x0 + k) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
-                      enc_key(b[k], bw));
+                      sd_bits(b[k]));
         }
       }
       return;
@@ -1529,17 +1542,16 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   const uint64_t an = static_cast<uint64_t>(anx) * any * anz;
   const bool use_acc = an <= static_cast<uint64_t>(acc_cap);
   if (use_acc) {
-    for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) s_acc[v] = 0xffffffffu;
+    for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) s_acc[v] = kNoHit;
     __syncthreads();
   }
   auto emit = [&](int x, int y, int z, float sd) {  // sd < bandWorld
     if (use_acc) {
       uint32_t a = static_cast<uint32_t>(x - ax0) + anx * (static_cast<uint32_t>(y - ay0) + any * static_cast<uint32_t>(z - az0));
-      const uint32_t u = __float_as_uint(sd);
-      atomicMin(&s_acc[a], (u & 0x80000000u) ? ~u : (u | 0x80000000u));
+      atomicMin(&s_acc[a], sd_bits(sd));
     } else {
       atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
-                enc_key(sd, bw));
+                sd_bits(sd));
     }
   };
   const float reach2_hi = (bw + radius) * (bw + radius) * 1.00001f;
@@ -1660,34 +1672,45 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
           const float flx = floorf(fx), fly = floorf(fy), flz = floorf(fz);
           const int cxv = f2i(flx), cyv = f2i(fly), czv = f2i(flz);
           const int sx = fx - flx >= 0.5f ? 1 : -1, sy = fy - fly >= 0.5f ? 1 : -1, sz = fz - flz >= 0.5f ? 1 : -1;
-          // Per axis, the 15 voxel offsets the stencil can reach (-7..7) as (d * n, d * d) with
+          // Per axis, the voxel offsets the stencil can reach, indexed by the stencil's own 4-bit
+          // field i (offset i - 8, mirrored to the particle's octant), as (d * n, d * d) with
           // d = centre - particle: the same operations visit() does per voxel, done once per
           // particle; a voxel then adds them as (dx*nx + dy*ny) + dz*nz and (dx*dx + dy*dy) +
-          // dz*dz, the reference's rounding order.
-          if (lane < 30) {
-            const int axis = lane >= 15 ? 1 : 0, o = static_cast<int>(lane) - 15 * axis - 7;
-            const float d = (static_cast<float>((axis ? cyv : cxv) + o) + 0.5f) * voxel - (axis ? q.y : q.x);
-            s_dt[wid][axis][o + 7] = make_float2(d * (axis ? nn.y : nn.x), d * d);
+          // dz*dz, the reference's rounding order. Which offsets land inside the particle's box
+          // is kept as bits (ballots): x in the low half of vxy, y in the high half, z in vz.
+          bool in_box;
+          {
+            const int axis = lane >= 16 ? 1 : 0, i = static_cast<int>(lane & 15u);
+            const int c = (axis ? cyv : cxv) + (axis ? sy : sx) * (i - 8);
+            const float d = (static_cast<float>(c) + 0.5f) * voxel - (axis ? q.y : q.x);
+            s_dt[wid][axis][i] = make_float2(d * (axis ? nn.y : nn.x), d * d);
+            in_box = axis ? (c >= lo.y && c <= hi.y) : (c >= lo.x && c <= hi.x);
           }
-          if (lane < 15) {
-            const float d = (static_cast<float>(czv + static_cast<int>(lane) - 7) + 0.5f) * voxel - q.z;
-            s_dt[wid][2][lane] = make_float2(d * nn.z, d * d);
+          const uint32_t vxy = __ballot_sync(0xffffffffu, in_box);
+          {
+            const int i = static_cast<int>(lane & 15u), c = czv + sz * (i - 8);
+            if (lane < 16) {
+              const float d = (static_cast<float>(c) + 0.5f) * voxel - q.z;
+              s_dt[wid][2][i] = make_float2(d * nn.z, d * d);
+            }
+            in_box = lane < 16 && c >= lo.z && c <= hi.z;
           }
+          const uint32_t vz = __ballot_sync(0xffffffffu, in_box);
           __syncwarp();
           const uint32_t ns = s_nst;
           for (uint32_t v = lane; v < ns; v += 32) {
             const uint32_t e = s_st[v];
-            const int mx = sx * (static_cast<int>(e & 15u) - 8), my = sy * (static_cast<int>((e >> 4) & 15u) - 8),
-                      mz = sz * (static_cast<int>((e >> 8) & 15u) - 8);
-            const int x = cxv + mx, y = cyv + my, z = czv + mz;
-            if (x < lo.x || x > hi.x || y < lo.y || y > hi.y || z < lo.z || z > hi.z) continue;
-            const float2 tx = s_dt[wid][0][mx + 7], ty = s_dt[wid][1][my + 7], tz = s_dt[wid][2][mz + 7];
+            const uint32_t ex = e & 15u, ey = (e >> 4) & 15u, ez = (e >> 8) & 15u;
+            if (!((vxy >> ex) & (vxy >> (16u + ey)) & (vz >> ez) & 1u)) continue;
+            const float2 tx = s_dt[wid][0][ex], ty = s_dt[wid][1][ey], tz = s_dt[wid][2][ez];
             const float pl = has_n ? (tx.x + ty.x) + tz.x : -__int_as_float(0x7f800000);
             if (pl >= bw) continue;
             const float t = (tx.y + ty.y) + tz.y;
             if (t >= reach2_hi) continue;
             const float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
-            if (sd < bw) emit(x, y, z, sd);
+            if (sd < bw)
+              emit(cxv + sx * (static_cast<int>(ex) - 8), cyv + sy * (static_cast<int>(ey) - 8),
+                   czv + sz * (static_cast<int>(ez) - 8), sd);
           }
           __syncwarp();  // the tables are rewritten for the next particle
           continue;
@@ -1705,29 +1728,35 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     __syncthreads();
     for (uint32_t v = threadIdx.x; v < static_cast<uint32_t>(an); v += blockDim.x) {
       const uint32_t u = s_acc[v];
-      if (u != 0xffffffffu) {
-        const float sd = __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+      if (u != kNoHit) {
         int x = ax0 + static_cast<int>(v % anx);
         int y = ay0 + static_cast<int>((v / anx) % any);
         int z = az0 + static_cast<int>(v / (anx * any));
-        atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
-                  enc_key(sd, bw));
+        atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)), u);
       }
     }
   }
 }
 
-// resolve[m] (splat.ts:258-276): v = f32(key) * (1/32767.5) - 1 stored as f16 (round to
-// nearest even). The key is reset to 65535 behind the read, which is the clear of the
-// next bake (splat.ts:200-210): the grid holds 65535 everywhere between bakes.
+// resolve[m] (splat.ts:258-276): the voxel's key, u32((clamp(sd / bandWorld, -1, 1) + 1) *
+// 32767.5) of its smallest distance (65535 where no particle reached it), then
+// v = f32(key) * (1/32767.5) - 1 stored as f16 (round to nearest even). The grid is reset to
+// kNoHit behind the read, which is the clear of the next bake (splat.ts:200-210).
 __device__ __forceinline__ void resolve_block(const SplatDev& D, const Work w) {
   const long long base = static_cast<long long>(w.first) * 4;
   const long long v0 = base + static_cast<long long>(threadIdx.x) * 4;
   const float inv = 3.0518043793392844e-05f;  // f32(1/32767.5)
+  if (v0 >= D.total) return;
+  // the level of these voxels (level sizes are multiples of 4, so four share one)
+  int m = 0;
+  while (m + 1 < D.mips && v0 >= D.off[m + 1]) m++;
+  const float bw = D.bw[m];
+  auto key_of = [&](uint32_t u) { return u == kNoHit ? 65535u : enc_key(bits_sd(u), bw); };
   if (v0 + 3 < D.total) {
-    uint4 k4 = *reinterpret_cast<const uint4*>(D.keys + v0);
+    const uint4 u4 = *reinterpret_cast<const uint4*>(D.keys + v0);
+    const uint4 k4 = make_uint4(key_of(u4.x), key_of(u4.y), key_of(u4.z), key_of(u4.w));
     if (D.key_capture) *reinterpret_cast<uint4*>(D.key_capture + v0) = k4;
-    *reinterpret_cast<uint4*>(D.keys + v0) = make_uint4(65535u, 65535u, 65535u, 65535u);
+    *reinterpret_cast<uint4*>(D.keys + v0) = make_uint4(kNoHit, kNoHit, kNoHit, kNoHit);
     __half2 a = __halves2half2(__float2half_rn(static_cast<float>(k4.x) * inv - 1.0f),
                                __float2half_rn(static_cast<float>(k4.y) * inv - 1.0f));
     __half2 b = __halves2half2(__float2half_rn(static_cast<float>(k4.z) * inv - 1.0f),
@@ -1737,9 +1766,9 @@ __device__ __forceinline__ void resolve_block(const SplatDev& D, const Work w) {
     out[1] = b;
   } else {
     for (long long v = v0; v < D.total && v < v0 + 4; v++) {
-      uint32_t key = D.keys[v];
+      const uint32_t key = key_of(D.keys[v]);
       if (D.key_capture) D.key_capture[v] = key;
-      D.keys[v] = 65535u;
+      D.keys[v] = kNoHit;
       D.dist_out[v] = __float2half_rn(static_cast<float>(key) * inv - 1.0f);
     }
   }

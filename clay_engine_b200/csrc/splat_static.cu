@@ -40,7 +40,7 @@ __device__ __align__(256) uint32_t g_static_keys[kStaticKeys];
 
 __global__ void k_static_clear(uint32_t* __restrict__ keys, long long n) {
   long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (i < n) keys[i] = 65535u;
+  if (i < n) keys[i] = kNoHit;
 }
 
 __global__ void __launch_bounds__(32 * kSplatWarps) k_static_splat(const __grid_constant__ SplatDev D, float ox, float oy,
@@ -167,7 +167,7 @@ extern "C" int clay_splat_bake_static(const clay_cloud_desc* cloud, const clay_s
   }
   h.total = total;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  // The array keeps the last call's keys: start from the clear value 65535.
+  // The array keeps the last call's values: start from the clear value kNoHit.
   k_static_clear<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(keys, total);
   count_launch();
   if (cloud->capacity > 0) {
