@@ -624,7 +624,7 @@ def main():
     from clay_engine_b200 import autotune
 
     t_tune = time.perf_counter()
-    tuned, tune_report = autotune.tune(root, sims, bodies, stream, frames=5, use_cache=False)
+    tuned, tune_report = autotune.tune(root, sims, bodies, stream, frames=8, use_cache=False)
     t_tune = time.perf_counter() - t_tune
     batch = ce.Batch(root, sims, extra_splats=bodies, use_graph=True, sph_block=tuned["default"])
     autotune.apply(batch, tuned)

@@ -3,8 +3,9 @@
 Scenes are grouped by capacity into buckets. For each bucket in turn (coordinate descent,
 the other buckets held at their current choice), every candidate block size is timed over a
 few real batched frames (CUDA graph replays, CUDA events on the launching stream) and the
-fastest kept. The scenes' particle state is saved before tuning and restored after it, so
-tuning does not advance the simulation. Results are cached per bucket signature in a JSON
+fastest kept. The scenes' particle state is saved before tuning, restored before every
+candidate (so all are timed from the same state) and after tuning, so tuning does not advance
+the simulation. Results are cached per bucket signature in a JSON
 file next to the library.
 """
 from __future__ import annotations
@@ -48,7 +49,7 @@ def _time(batch, stream, frames):
     return a.elapsed_time(z) / frames
 
 
-def tune(root, sims, extra=(), stream=None, frames=5, use_cache=True, default=256, min_gain=0.02):
+def tune(root, sims, extra=(), stream=None, frames=8, use_cache=True, default=256, min_gain=0.02):
     """Returns ({"uppers": [...], "blocks": [...]}, report) for this set of scenes."""
     import torch
 
@@ -72,6 +73,10 @@ def tune(root, sims, extra=(), stream=None, frames=5, use_cache=True, default=25
             times = {}
             for cand in CANDIDATES:
                 choice[bi] = cand
+                # every candidate is timed from the same state (stepping moves the fluid, and a
+                # later, more spread-out state would cost more whatever the block size)
+                for s, snap in zip(sims, snaps):
+                    s.upload(snap)
                 batch = Batch(root, sims, extra_splats=extra, sph_block=choice[len(BUCKETS)], use_graph=True)
                 batch.set_bucket_blocks(list(BUCKETS), [choice[i] for i in range(len(BUCKETS))])
                 ms = _time(batch, stream, frames)
