@@ -1604,7 +1604,11 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
                    nuz = static_cast<uint32_t>(uhz - ulz + 1);
     const uint64_t nu64 = static_cast<uint64_t>(nux) * nuy * nuz;
     const uint32_t nact = __popc(active);
-    if (nu64 < (1ull << 31) && ((nu64 + 31) >> 5) * nact <= 2ull * cost_ind) {
+    // union walk when its lane-steps (each over every particle of the warp) cost less than the
+    // particles' own walks: a union step per particle costs about half an own-walk step for
+    // discs, a third for spheres (no plane term, no square root until the end)
+    const uint64_t own_steps = use_st ? static_cast<uint64_t>(nact) * ((s_nst + 31u) >> 5) : cost_ind;
+    if (nu64 < (1ull << 31) && ((nu64 + 31) >> 5) * nact <= (has_n ? 2ull : 3ull) * own_steps) {
       const uint32_t nu = static_cast<uint32_t>(nu64);
       BoxWalk bw_;
       bw_.init(lane, nux, nuy);
