@@ -250,8 +250,8 @@ int clay_splat_bake_static(const clay_cloud_desc* cloud, const clay_splat_opts* 
 clay_volume* clay_splat_volume(clay_splat* s);
 clay_field* clay_splat_field(clay_splat* s);
 /* Test hook: during the next bakes, copy each voxel's 16-bit key (the u32 the reference
- * `atomicMin`s, splat.ts:247-249) into `keys_device` (total_voxels u32) before resolving.
- * NULL turns it off. */
+ * `atomicMin`s, splat.ts:247-249) into `keys_device` (total_voxels u32) as the resolve pass
+ * computes it. NULL turns it off. */
 int clay_splat_capture_keys(clay_splat* s, uint32_t* keys_device);
 
 /* ------------------------------------------------------------------------------------
