@@ -668,7 +668,7 @@ def main():
     D.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_steps = max(2, args.steps // 2)
+    e2e_steps = max(2, args.steps)
     e0.record(stream)
     for i in range(e2e_steps):
         batch.step(stream)
