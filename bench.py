@@ -577,8 +577,8 @@ BYTES_PER_PARTICLE = {
 }
 # DRAM bytes (read + written) per particle of one k_splat launch over the fluid surfaces (3
 # levels), from the ncu capture summarised in profiles/k_splat_batched_128_scenes.md:
-# 107,385,856 + 4,627,712 bytes for 1,940,550 particles.
-SPLAT_TRAFFIC_PER_PARTICLE = (107385856 + 4627712) / 1940550
+# 107,440,128 + 6,127,360 bytes for 1,940,550 particles.
+SPLAT_TRAFFIC_PER_PARTICLE = (107440128 + 6127360) / 1940550
 
 
 def main():
