@@ -572,7 +572,7 @@ def load_peaks():
 # traffic if every input were read once and every output written once; neighbour re-reads
 # are cache reuse and the neighbour list is an intermediate, neither is counted).
 BYTES_PER_PARTICLE = {
-    "density": 16 + 16,                        # pos in; density, pressure, 1/density, count out
+    "density": 16 + 16 + 16 + 4,  # pos in; density record, neighbour view (pos, 1/density), pressure out
     "forces_integrate": 16 + 16 + 16 + 4 + 48,  # pos, vel, density record, id in; particle record out
 }
 # DRAM bytes (read + written) per particle of one k_splat launch over the fluid surfaces (3

@@ -133,6 +133,9 @@ struct __align__(16) SceneDev {
   float4* spos;
   float4* svel;
   float4* sdp;  // density, pressure, 1/density (the reference's per-pair `1 / other.density`), neighbours
+  // what the forces pass reads of a neighbour, in two 16-byte records: spx = position and
+  // 1/density (written by the density pass), svel = velocity and pressure (.w written by it)
+  float4* spx;
   uint4* nbr;  // accepted neighbours of the density pass, 4 per entry, slot-major: nbr[(j / 4) * capacity + k]
   uint32_t* counts;
   uint32_t* cell_start;
@@ -872,7 +875,11 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   if (kFast) rho = __fadd_rn(rho, comp);
   const float stiff = S.prm->stiffness;
   const float dens = fmaxf(rho, S.rest_floor);
-  S.sdp[k] = make_float4(dens, fmaxf(stiff * (rho - S.rest), 0.0f), __frcp_rn(dens), __uint_as_float(cnt));
+  const float pres = fmaxf(stiff * (rho - S.rest), 0.0f), inv = __frcp_rn(dens);
+  S.sdp[k] = make_float4(dens, pres, inv, __uint_as_float(cnt));
+  // the neighbour view of this particle for the forces pass (svel is not read in this pass)
+  S.spx[k] = make_float4(me.x, me.y, me.z, inv);
+  S.svel[k].w = pres;
 }
 
 // forces (fluid.ts:370-439) fused with integrate (fluid.ts:449-491). The neighbour pass
@@ -899,16 +906,15 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
   float fx = 0.0f, fy = 0.0f, fz = 0.0f;
   float vsx = mv.x * S.h6, vsy = mv.y * S.h6, vsz = mv.z * S.h6;
   float wsum = S.h6;
-  const float4* __restrict__ spos = S.spos;
+  const float4* __restrict__ spx = S.spx;
   const float4* __restrict__ svel = S.svel;
-  const float4* __restrict__ sdp = S.sdp;
-  // one neighbour q with its cell-ordered position, density record and velocity
-  auto accum = [&](uint32_t q, const float4 o, const float4 odp, const float4 ov) {
+  // one neighbour q: o = position and 1/density, ov = velocity and pressure
+  auto accum = [&](uint32_t q, const float4 o, const float4 ov) {
     if (q == k) return;
     float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
     float r2 = (dx * dx + dy * dy) + dz * dz;
     if (r2 >= h2) return;
-    const float inv = odp.z;
+    const float inv = o.w;
     float w0 = h2 - r2;
     float wv = (w0 * w0) * w0;
     vsx = vsx + ov.x * wv;
@@ -920,7 +926,7 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
     const float r = kFast ? r2 * irs : __fsqrt_rn(r2);
     if (r > 1e-6f) {
       float hr = h - r;
-      float s = mass * (mp + odp.y) * 0.5f * inv * spiky * (hr * hr);
+      float s = mass * (mp + ov.w) * 0.5f * inv * spiky * (hr * hr);
       float ir = kFast ? irs : __frcp_rn(r);
       fx = fx - (dx * ir) * s;
       fy = fy - (dy * ir) * s;
@@ -929,10 +935,10 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
   };
   auto pair = [&](uint32_t q) {
     if (q == k) return;
-    const float4 o = __ldg(spos + q);
+    const float4 o = __ldg(spx + q);
     float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
     if ((dx * dx + dy * dy) + dz * dz >= h2) return;
-    accum(q, o, __ldg(sdp + q), __ldg(svel + q));
+    accum(q, o, __ldg(svel + q));
   };
   // The density pass of this substep stored the neighbours it accepted, in the same visiting
   // order, with the same squared lengths: the list replaces the scan of the 27 cells, and
@@ -949,18 +955,17 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
       const uint32_t qa[4] = {e.x, e.y, e.z, e.w};
 #pragma unroll
       for (int g = 0; g < 4; g += kForceLoads) {
-        float4 o[kForceLoads], d[kForceLoads], v[kForceLoads];
+        float4 o[kForceLoads], v[kForceLoads];
 #pragma unroll
         for (int u = 0; u < kForceLoads; u++) {
           if (j + g + u < cnt) {  // entries past the count hold no index
-            o[u] = __ldg(spos + qa[g + u]);
-            d[u] = __ldg(sdp + qa[g + u]);
+            o[u] = __ldg(spx + qa[g + u]);
             v[u] = __ldg(svel + qa[g + u]);
           }
         }
 #pragma unroll
         for (int u = 0; u < kForceLoads; u++)
-          if (j + g + u < cnt) accum(qa[g + u], o[u], d[u], v[u]);
+          if (j + g + u < cnt) accum(qa[g + u], o[u], v[u]);
       }
     }
   } else {
