@@ -1855,6 +1855,10 @@ struct clay_extractor {
   std::vector<DevBuf> bufs;
   bool dirty = true;
   int blocks = 0;
+  // the eight passes of one extraction, captured on the first extract and replayed after:
+  // every pass reads its parameters from `d`, so one graph serves every region and motion
+  cudaGraphExec_t graph = nullptr;
+  int64_t launches = 0;
 
   template <class T>
   int alloc(T** p, size_t count) {
@@ -1937,6 +1941,7 @@ int clay_extractor_create(clay_ctx* ctx, const clay_field* field, void* particle
 
 void clay_extractor_destroy(clay_extractor* x) {
   if (!x) return;
+  if (x->graph) cudaGraphExecDestroy(x->graph);
   for (auto& b : x->bufs) x->ctx->dev_free(b.p, b.n);
   delete x;
 }
@@ -1959,14 +1964,35 @@ int clay_extractor_extract(clay_extractor* x, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int rc = x->flush(s);
   if (rc) return rc;
-  CK(L_ext_reset(x->d, s));
-  CK(L_ext_cells(x->d, x->blocks, s));
-  CK(L_ext_scan(x->d, 0, s));
-  CK(L_ext_emit(x->d, x->blocks, s));
-  CK(L_ext_qcount(x->d, x->blocks, s));
-  CK(L_ext_scan(x->d, 1, s));
-  CK(L_ext_qemit(x->d, x->blocks, s));
-  CK(L_ext_finish(x->d, s));
+  // A small lattice (the game's 32^3 per body) is bound by launching its eight dependent
+  // passes, so they run as one CUDA graph, captured on a private stream at the first call.
+  if (!x->graph) {
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = launch_count();
+    cudaError_t e = L_ext_reset(x->d, cs);
+    if (e == cudaSuccess) e = L_ext_cells(x->d, x->blocks, cs);
+    if (e == cudaSuccess) e = L_ext_scan(x->d, 0, cs);
+    if (e == cudaSuccess) e = L_ext_emit(x->d, x->blocks, cs);
+    if (e == cudaSuccess) e = L_ext_qcount(x->d, x->blocks, cs);
+    if (e == cudaSuccess) e = L_ext_scan(x->d, 1, cs);
+    if (e == cudaSuccess) e = L_ext_qemit(x->d, x->blocks, cs);
+    if (e == cudaSuccess) e = L_ext_finish(x->d, cs);
+    x->launches = static_cast<int64_t>(launch_count() - before);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (e == cudaSuccess) e = ec;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&x->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      x->graph = nullptr;
+      return fail(CLAY_ECUDA, "SurfaceExtractor: capturing the extraction failed: %s", cudaGetErrorString(e));
+    }
+  }
+  CK(cudaGraphLaunch(x->graph, s));
+  count_launches(static_cast<uint64_t>(x->launches));
   return CLAY_OK;
 }
 

@@ -486,7 +486,10 @@ void clay_extractor_destroy(clay_extractor* x);
  * velocity into it at the next extraction. */
 int clay_extractor_set_region(clay_extractor* x, const double origin[3], double size, const double vel[3],
                               int preserve_motion);
-/* extract (extract.ts:469-475): reset, cells, quads, finish, on `stream`. */
+/* extract (extract.ts:469-475): reset, cells, quads, finish, on `stream`. The eight passes
+ * run as one CUDA graph that the first call captures (on a private stream) and later calls
+ * replay; every pass reads the region and motion from device memory, so setRegion between
+ * calls needs no new graph. */
 int clay_extractor_extract(clay_extractor* x, void* stream);
 /* Device views: the quad index list (quad_capacity * 6 u32) and the 4 draw arguments. */
 int clay_extractor_views(clay_extractor* x, uint32_t** indices, uint32_t** draw_args, int64_t* quad_capacity);
