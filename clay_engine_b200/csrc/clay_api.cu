@@ -2042,6 +2042,11 @@ struct clay_solver {
   int substeps = 2;
   bool dirty = true;
   bool kicking = false;
+  // the substeps' passes as one CUDA graph, captured for the body count they were last run
+  // with (it sets the match pass's grid); every pass reads its parameters from `d`
+  cudaGraphExec_t graph = nullptr;
+  int32_t graph_bodies = -1;
+  int64_t launches = 0;
 };
 
 extern "C" {
@@ -2099,6 +2104,7 @@ int clay_solver_create(clay_ctx* ctx, const clay_field* world, void* particles, 
 
 void clay_solver_destroy(clay_solver* sv) {
   if (!sv) return;
+  if (sv->graph) cudaGraphExecDestroy(sv->graph);
   sv->ctx->dev_free(sv->d, sizeof(SolveDev));
   delete sv;
 }
@@ -2138,12 +2144,37 @@ int clay_solver_step(clay_solver* sv, int32_t body_count, void* stream) {
     CK(L_pbd_kick(sv->d, blocks, s));
     sv->kicking = false;
   }
-  for (int sub = 0; sub < sv->substeps; sub++) {
-    CK(L_pbd_predict(sv->d, blocks, s));
-    CK(L_pbd_match(sv->d, body_count, s));
-    CK(L_pbd_apply(sv->d, blocks, s));
-    CK(L_pbd_finalize(sv->d, blocks, s));
+  // The substeps' 4 x substeps dependent passes run as one CUDA graph, captured on a private
+  // stream the first time and again when the body count changes.
+  if (!sv->graph || sv->graph_bodies != body_count) {
+    if (sv->graph) cudaGraphExecDestroy(sv->graph);
+    sv->graph = nullptr;
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    const uint64_t before = launch_count();
+    cudaError_t e = cudaSuccess;
+    for (int sub = 0; sub < sv->substeps && e == cudaSuccess; sub++) {
+      e = L_pbd_predict(sv->d, blocks, cs);
+      if (e == cudaSuccess) e = L_pbd_match(sv->d, body_count, cs);
+      if (e == cudaSuccess) e = L_pbd_apply(sv->d, blocks, cs);
+      if (e == cudaSuccess) e = L_pbd_finalize(sv->d, blocks, cs);
+    }
+    sv->launches = static_cast<int64_t>(launch_count() - before);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (e == cudaSuccess) e = ec;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&sv->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+      sv->graph = nullptr;
+      return fail(CLAY_ECUDA, "ClaySolver: capturing the substeps failed: %s", cudaGetErrorString(e));
+    }
+    sv->graph_bodies = body_count;
   }
+  CK(cudaGraphLaunch(sv->graph, s));
+  count_launches(static_cast<uint64_t>(sv->launches));
   return CLAY_OK;
 }
 

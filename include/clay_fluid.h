@@ -540,7 +540,9 @@ void clay_solver_destroy(clay_solver* s);
 /* setForce (pbd.ts:376-398): a uniform acceleration of one body for the next steps and a
  * one-shot velocity change (`impulse`, may be NULL) applied once by the next step. */
 int clay_solver_set_force(clay_solver* s, uint32_t body, const double accel[3], const double impulse[3]);
-/* step (pbd.ts:396-416) over the set's first `body_count` bodies, on `stream`. */
+/* step (pbd.ts:396-416) over the set's first `body_count` bodies, on `stream`. The substeps'
+ * passes run as one CUDA graph, captured (on a private stream) at the first step and again
+ * when `body_count` changes; the impulse of set_force is a separate launch before it. */
 int clay_solver_step(clay_solver* s, int32_t body_count, void* stream);
 
 /* ------------------------------------------------------------------------------------
