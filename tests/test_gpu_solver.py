@@ -193,3 +193,33 @@ def test_body_count_rules(root, oracle):
     sv.destroy()
     field.destroy()
     v.destroy()
+
+
+def test_body_count_changes_between_steps(root, oracle):
+    """One solver stepped with a body count that changes from step to step (the substeps'
+    graph is captured again for each new count) stays bit-exact to the oracle."""
+    import torch
+
+    import clay_engine_b200 as ce
+
+    v, vd = volume(root, oracle, [brushes.make_brush("box", pos=(0.0, -2.0, 0.0), size=(3.5, 1.0, 3.5))],
+                   32, (-4.0, -4.0, -4.0), 8.0)
+    field = ce.volumeField(v)
+    specs = [{"center": (-1.0, 0.0, 0.0), "vel": (0.5, 0.0, 0.0)}, {"center": (0.0, 0.5, 0.0), "stiffness": 0.7},
+             {"center": (1.0, 1.0, 0.0), "rot": quat((0, 0, 1), 20)}]
+    parts, bodies = particle_set(specs, 400, 3, 1 / 120, seed=3)
+    dp = torch.from_numpy(parts.view(np.uint8).copy()).cuda()
+    db = torch.from_numpy(bodies.view(np.uint8).copy()).cuda()
+    sv = ce.ClaySolver(root, dp, len(parts), db, len(bodies), field)
+    cfg = oracle.solver_cfg(len(parts), len(bodies))
+    ofield = oracle.make_field([vd])
+    hp, hb = parts.copy(), bodies.copy()
+    for f, count in enumerate((3, 3, 1, 2, 2, 3, 1, 3)):
+        sv.step(count)
+        oracle.solver_step(cfg, ofield, hp, hb, count)
+        torch.cuda.synchronize()
+        assert same(dp.cpu().numpy(), hp.view(np.uint8)), f"step {f} (bodies {count}): particle records differ"
+        assert same(db.cpu().numpy(), hb.view(np.uint8)), f"step {f} (bodies {count}): body records differ"
+    sv.destroy()
+    field.destroy()
+    v.destroy()
