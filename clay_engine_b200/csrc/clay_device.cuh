@@ -1765,7 +1765,9 @@ __device__ __forceinline__ void resolve_block(const SplatDev& D, const Work w) {
     const uint4 u4 = *reinterpret_cast<const uint4*>(D.keys + v0);
     const uint4 k4 = make_uint4(key_of(u4.x), key_of(u4.y), key_of(u4.z), key_of(u4.w));
     if (D.key_capture) *reinterpret_cast<uint4*>(D.key_capture + v0) = k4;
-    *reinterpret_cast<uint4*>(D.keys + v0) = make_uint4(kNoHit, kNoHit, kNoHit, kNoHit);
+    // most voxels of a bake volume are reached by no particle and hold kNoHit already
+    if ((u4.x & u4.y & u4.z & u4.w) != kNoHit)
+      *reinterpret_cast<uint4*>(D.keys + v0) = make_uint4(kNoHit, kNoHit, kNoHit, kNoHit);
     __half2 a = __halves2half2(__float2half_rn(static_cast<float>(k4.x) * inv - 1.0f),
                                __float2half_rn(static_cast<float>(k4.y) * inv - 1.0f));
     __half2 b = __halves2half2(__float2half_rn(static_cast<float>(k4.z) * inv - 1.0f),
