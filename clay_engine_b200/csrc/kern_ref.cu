@@ -51,12 +51,18 @@ cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threa
   CLAY_LAUNCH(k_forces_integrate<false>, blocks, threads, st, s, w, sub);
 }
 cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, uint32_t acc_voxels, cudaStream_t st) {
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_splat, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         kSplatAccVoxelsDiscs * static_cast<int>(sizeof(uint32_t)));
+  // The splat's shared memory exceeds the default per-block limit; the opt-in is a property
+  // of the function on each device, so it is set once per device (from any thread).
+  constexpr int kDevices = 64;
+  static std::atomic<bool> attr_set[kDevices];
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kDevices || !attr_set[dev].load(std::memory_order_acquire)) {
+    e = cudaFuncSetAttribute(k_splat, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kSplatAccVoxelsDiscs * static_cast<int>(sizeof(uint32_t)));
     if (e != cudaSuccess) return e;
-    attr_set = true;
+    if (dev >= 0 && dev < kDevices) attr_set[dev].store(true, std::memory_order_release);
   }
   dim3 g(blocks, w ? 1 : blocks_y);
   k_splat<<<g, kSplatThreads, acc_voxels * sizeof(uint32_t), st>>>(d, w, acc_voxels);
