@@ -9,6 +9,14 @@ unioned into its collider), all advanced one frame per batched launch captured i
 graph. The same scenes stepped one scene per launch sequence give the plain rate reported
 beside it. Inputs are seeded synthetic data (no dataset): jittered lattices of spacing 0.1.
 
+Beside the headline the line carries: `e2e` (the same frames through the public API, inputs up
+from and results down to pinned host memory every frame), `served` (a native continuous-batching
+server under Poisson arrivals of step-and-bake requests, p50/p99 latency, and a second stream
+below capacity when the first one outruns the GPU), `roofline` (the dominant kernel against the
+measured HBM peak, with the neighbour passes), `cpu_baseline` (the f32 oracle on the host cores),
+`next_rows` (collider build, level sampling, surface nets and the ClaySolver, each against the
+oracle on the same inputs), `clocks` and `gpu_launches`.
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Multi-GPU: one process per GPU under torchrun; each rank steps its own 256 scenes (weak
 scaling, no collective on the data path); timings are the max over ranks.
