@@ -233,12 +233,15 @@ class VolumeData:
 
 
 def make_field(volumes, offsets=None) -> Field:
+    """A union of volumes as the oracle's field. The field holds raw pointers into the volumes'
+    planes, so it keeps the volumes alive for as long as it exists."""
     f = Field()
     f.n = len(volumes)
     for i, v in enumerate(volumes):
         f.vol[i] = v.c()
         off = offsets[i] if offsets is not None else (0.0, 0.0, 0.0)
         f.offset[i][:] = off
+    f._volumes = list(volumes)
     return f
 
 

@@ -121,3 +121,30 @@ def test_kinematic_still_and_impulse_once(oracle):
     assert abs(v1 - 3.0 * 0.995 ** 2) < 0.05 and cfg.kicking == 0
     oracle.solver_step(cfg, field, parts, bodies, 1)
     assert parts["vel"][:k, 1].mean() < v1  # no second kick: only damping
+
+
+def test_body_count_limits_the_match_only(oracle):
+    """step(bodyCount) dispatches the match pass over the first bodyCount bodies (pbd.ts:400-416):
+    a body past the count keeps its record, while its particles still go through the other
+    passes (they only ask whether a particle's body index is below maxBodies). At stiffness 1 the
+    pull lands them exactly on the pose of the record they still carry."""
+    field, _ = floor(oracle, top=-3.5)
+    cfg = oracle.solver_cfg(512, 2)
+    a, ba, ka = lattice_body((0.0, 1.0, 0.0), vel=(0.5, 0.0, 0.0), h=cfg.h, capacity=512)
+    b, bb, kb = lattice_body((1.0, 1.0, 0.0), vel=(0.0, 0.0, 1.0), h=cfg.h, capacity=512)
+    parts = a.copy()
+    parts[ka:ka + kb] = b[:kb]
+    parts["body"][ka:ka + kb] = 1
+    bodies = np.zeros(2, scenes.BODY_RECORD)
+    bodies[0] = ba[0]
+    bodies[1] = bb[0]
+    bodies["first"][1] = ka
+    before = bodies.copy()
+    rec0 = parts[ka:ka + kb].copy()
+    oracle.solver_step(cfg, field, parts, bodies, 1)
+    assert np.array_equal(bodies[1:].view(np.uint8), before[1:].view(np.uint8))
+    assert not np.array_equal(bodies[:1].view(np.uint8), before[:1].view(np.uint8))
+    assert not np.array_equal(parts[ka:ka + kb]["vel"], rec0["vel"])  # predicted and finalized
+    # the unmatched record has rotation 1, so its pose is com + (rest - restCom)
+    target = bodies["com"][1] + (parts["rest"][ka:ka + kb] - bodies["restCom"][1])
+    assert np.abs(parts["pos"][ka:ka + kb] - target).max() < 1e-6
