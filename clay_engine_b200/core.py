@@ -456,7 +456,6 @@ class SplatField:
             check(lib().clay_splat_create(root.handle, C.byref(desc), C.byref(o), C.byref(h)))
             self.handle = h.value
             self._owned = True
-            self.cloud = cloud  # the library reads the cloud's device arrays at every bake
         else:
             self.handle = _handle
             self._owned = False
