@@ -76,39 +76,17 @@ def fluid_opts(n):
 
 def build_scenes(root, n_scenes, seed, with_bodies=True):
     """The batched configuration on this GPU. Returns (sims, bodies, keepalive)."""
-    import torch
-
-    import clay_engine_b200 as ce
     from clay_engine_b200 import scenes
 
     cfg = scenes.CONFIG3
     counts = scenes.log_uniform_counts(n_scenes, cfg["n_lo"], cfg["n_hi"], seed)
     sims, bodies, keep = [], [], []
-    bcfg = cfg["body"]
-    shell, shell_n = scenes.surface_net_sphere(bcfg["radius"], bcfg["cell"])
     for i, n in enumerate(counts):
-        vol = ce.SdfVolume(root, resolution=cfg["collider"]["resolution"], worldSize=24.0, origin=scenes.WORLD_ORIGIN)
-        vol.build(scenes.random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10), hi=(10, 1.0, 10)))
-        world = ce.volumeField(vol)
-        keep += [vol, world]
-        if with_bodies and i % cfg["body_every"] == 0:
-            center = (2.0, -1.4, 1.0)
-            parts, body = scenes.body_records(shell + np.array(center, np.float32), shell_n, center)
-            dp = torch.from_numpy(parts.view(np.uint8)).cuda()
-            db = torch.from_numpy(body.view(np.uint8)).cuda()
-            cloud = ce.bodyCloud(dp, db, 0)
-            box = bcfg["bake_box"]
-            splat = ce.SplatField(root, cloud, radius=(box / bcfg["bake_res"]) * 1.15, resolution=bcfg["bake_res"],
-                                  band=bcfg["band"], worldSize=box)
-            splat.setCenter(center)
-            bodies.append(splat)
-            world = ce.unionField(world, splat.field)
-            keep += [dp, db, splat, world]
-        sim = ce.FluidSim(root, world, fluid_opts(n))
-        side = math.ceil(n ** (1 / 3)) * 0.1
-        p = scenes.lattice_block(int(n), 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i)
-        sim.upload(p)
-        sims.append(sim)
+        sc = scenes.config3_scene(root, i, int(n), seed, with_body=with_bodies)
+        sims.append(sc["sim"])
+        if sc["body"] is not None:
+            bodies.append(sc["body"])
+        keep += sc["keep"]
     return sims, bodies, keep
 
 
@@ -288,43 +266,51 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------
 # CPU baseline: the oracle (the f32 restatement of the reference WGSL) on host cores.
 
-def cpu_sample(n_scenes, seed, max_particles, threads, frames=1):
-    """Runs the oracle on a bounded sample of the batched scenes, one frame each, and returns
-    (particle-steps/s, particles, seconds, sample description)."""
-    from clay_engine_b200 import brushes as _b  # noqa: F401  (brush records for the colliders)
-    from clay_engine_b200 import scenes
-    from oracle import oracle
-    from oracle.fluid_frame import OracleFluid
+class CpuSample:
+    """The oracle (the f32 restatement of the reference WGSL) on a bounded sample of the
+    batched scenes: the scenes nearest the median size, up to `max_particles` particles, each
+    with its own collider, built once. One rep = every scene of the sample advanced one frame
+    from its initial state (the states are put back before each rep, untimed), so every rep,
+    in this arm and in the reference arm, times the same work."""
 
-    oracle.build()
-    cfg = scenes.CONFIG3
-    counts = scenes.log_uniform_counts(n_scenes, cfg["n_lo"], cfg["n_hi"], seed)
-    order = np.argsort(np.abs(np.log(counts) - np.median(np.log(counts))))
-    chosen, total = [], 0
-    for i in order:
-        if total + counts[i] > max_particles and chosen:
-            break
-        chosen.append(int(i))
-        total += int(counts[i])
-    sims = []
-    for i in chosen:
-        vd = oracle.VolumeData(64, 3, scenes.WORLD_ORIGIN, 24.0, 4.0)
-        d, m = oracle.build_brushes(vd, scenes.random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10),
-                                                               hi=(10, 1.0, 10)), threads=threads)
-        vd.dist[:], vd.mat[:] = d, m
-        o = dict(fluid_opts(counts[i]))
-        ref = OracleFluid(oracle, [vd], threads=threads, **o)
-        side = math.ceil(counts[i] ** (1 / 3)) * 0.1
-        ref.upload(scenes.lattice_block(int(counts[i]), 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i))
-        sims.append(ref)
-    t0 = time.perf_counter()
-    for _ in range(frames):
-        for ref in sims:
+    def __init__(self, n_scenes, seed, max_particles, threads):
+        from clay_engine_b200 import scenes
+        from oracle import oracle
+        from oracle.fluid_frame import OracleFluid
+
+        oracle.build()
+        cfg = scenes.CONFIG3
+        counts = scenes.log_uniform_counts(n_scenes, cfg["n_lo"], cfg["n_hi"], seed)
+        order = np.argsort(np.abs(np.log(counts) - np.median(np.log(counts))))
+        chosen, total = [], 0
+        for i in order:
+            if total + counts[i] > max_particles and chosen:
+                break
+            chosen.append(int(i))
+            total += int(counts[i])
+        self.sims, self.starts = [], []
+        for i in chosen:
+            vd = oracle.VolumeData(64, 3, scenes.WORLD_ORIGIN, 24.0, 4.0)
+            d, m = oracle.build_brushes(vd, scenes.random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10),
+                                                                   hi=(10, 1.0, 10)), threads=threads)
+            vd.dist[:], vd.mat[:] = d, m
+            ref = OracleFluid(oracle, [vd], threads=threads, **fluid_opts(counts[i]))
+            side = math.ceil(counts[i] ** (1 / 3)) * 0.1
+            self.starts.append(scenes.lattice_block(int(counts[i]), 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i))
+            self.sims.append(ref)
+        self.particles = total
+        self.threads = threads
+        self.desc = (f"{len(chosen)} of the {n_scenes} batched scenes nearest the median size, {total} particles, "
+                     f"one frame each from their initial state per rep, f32 oracle, {threads} thread(s)")
+
+    def rep(self) -> float:
+        """Seconds of one rep."""
+        for ref, p in zip(self.sims, self.starts):
+            ref.upload(p)
+        t0 = time.perf_counter()
+        for ref in self.sims:
             ref.step()
-    dt = time.perf_counter() - t0
-    desc = (f"{len(chosen)} of the {n_scenes} batched scenes nearest the median size, {total} particles, "
-            f"{frames} frame(s) each, f32 oracle, {threads} thread(s)")
-    return total * frames / dt, total * frames, dt, desc
+        return time.perf_counter() - t0
 
 
 def _event_ms(stream, fn, reps):
@@ -497,70 +483,166 @@ def measure_next_rows(root, stream, threads):
     return out
 
 
-def run_tap(root, args, stream, seed):
-    """The plain method at scale: one scene of capacity 262,144 over a 192^3 collider of 64
-    seeded brushes, baked into 128^3 x 4 (band 4), fed each frame by spawn(4096) at a tap with
-    a downward speed ~ N(2, 0.3) (one speed per spawn, as the reference emits one velocity per
-    spawn). Every frame is one FluidSim.step on one stream (no graph)."""
-    import torch
-
+def _tap_world(root, seed):
     import clay_engine_b200 as ce
     from clay_engine_b200 import scenes
 
     cfg = scenes.CONFIG2
     vol = ce.SdfVolume(root, resolution=cfg["collider"]["resolution"], worldSize=24.0, origin=scenes.WORLD_ORIGIN)
     vol.build(scenes.random_brushes(64, seed=seed))
-    world = ce.volumeField(vol)
-    sim = ce.FluidSim(root, world, cfg["fluid"])
-    rng = np.random.default_rng(seed)
-    tap = cfg["tap"]
-    live_sum = 0
+    return vol, ce.volumeField(vol)
 
-    def frame():
+
+def run_tap(root, stream, seed, frames, warmup):
+    """The plain method at scale (one scene of capacity 262,144 over a 192^3 collider of 64
+    seeded brushes, baked into 128^3 x 4, band 4), fed each frame by spawn(4096) at a tap with
+    a downward speed ~ N(2, 0.3) (one speed per spawn: the reference emits one velocity per
+    spawn). `frames` timed frames from an empty ring (it fills at frame 64, then wraps), each one
+    FluidSim.step on one stream (no graph), after `warmup` frames of a separate sim."""
+    import torch
+
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    cfg = scenes.CONFIG2
+    tap = cfg["tap"]
+    vol, world = _tap_world(root, seed)
+    rng = np.random.default_rng(seed)
+
+    def frame(sim):
         sim.spawn(tap["n"], tap["pos"], (0.0, -float(rng.normal(*tap["speed"])), 0.0))
         sim.step(stream)
         return sim.particleCount
 
-    for _ in range(args.warmup):
-        frame()
+    warm = ce.FluidSim(root, world, cfg["fluid"])
+    for _ in range(warmup):
+        frame(warm)
     stream.synchronize()
+    warm.destroy()
+    sim = ce.FluidSim(root, world, cfg["fluid"])
     a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(stream)
     l0 = ce.kernel_launch_count()
-    for _ in range(args.steps):
-        live_sum += frame()
+    live_sum = 0
+    a.record(stream)
+    for _ in range(frames):
+        live_sum += frame(sim)
     z.record(stream)
     z.synchronize()
     ms = a.elapsed_time(z)
-    launches = ce.kernel_launch_count() - l0
-    out = {"value": live_sum / (ms / 1000), "ms_per_step": ms / args.steps, "gpu_launches": launches,
-           "live_at_end": sim.particleCount}
+    out = {"value": live_sum / (ms / 1000), "ms_per_step": ms / frames, "frames": frames,
+           "gpu_launches": ce.kernel_launch_count() - l0, "live_at_end": sim.particleCount,
+           "particle_steps": live_sum}
     sim.destroy()
     world.destroy()
     vol.destroy()
     return out
 
 
+def run_small(root, stream, frames, warmup):
+    """The plain method, small: 4,096 particles (a 16^3 jittered lattice of spacing 0.1 at
+    y = 3, seed 1) over the 96^3 rounded-box collider, 2 substeps, a 64^3 x 3 bake, one
+    FluidSim.step per frame on one stream."""
+    import torch
+
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    cfg = scenes.CONFIG1
+    vol = ce.SdfVolume(root, resolution=cfg["collider"]["resolution"], worldSize=24.0, origin=scenes.WORLD_ORIGIN)
+    vol.build(scenes.config1_collider_brushes())
+    world = ce.volumeField(vol)
+    sim = ce.FluidSim(root, world, cfg["fluid"])
+    sim.upload(scenes.jittered_lattice(16, 0.1, (0.0, 3.0, 0.0), 1))
+    for _ in range(warmup):
+        sim.step(stream)
+    stream.synchronize()
+    a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(frames):
+        sim.step(stream)
+    z.record(stream)
+    z.synchronize()
+    ms = a.elapsed_time(z)
+    out = {"value": 4096 * frames / (ms / 1000), "ms_per_step": ms / frames, "frames": frames}
+    sim.destroy()
+    world.destroy()
+    vol.destroy()
+    return out
+
+
+def cpu_small(threads, frames=20):
+    """The oracle on the small configuration: the same 4,096 particles, `frames` frames."""
+    from clay_engine_b200 import scenes
+    from oracle import oracle
+    from oracle.fluid_frame import OracleFluid
+
+    oracle.build()
+    cfg = scenes.CONFIG1
+    vd = oracle.VolumeData(96, 3, scenes.WORLD_ORIGIN, 24.0, 4.0)
+    d, m = oracle.build_brushes(vd, scenes.config1_collider_brushes(), threads=threads)
+    vd.dist[:], vd.mat[:] = d, m
+    ref = OracleFluid(oracle, [vd], threads=threads, **cfg["fluid"])
+    ref.upload(scenes.jittered_lattice(16, 0.1, (0.0, 3.0, 0.0), 1))
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        ref.step()
+    sec = time.perf_counter() - t0
+    return {"value": 4096 * frames / sec, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"the same 4,096 particles, {frames} frames"}
+
+
+def cpu_tap(threads, seed, frames=2):
+    """The oracle on the tap at scale with its ring full: 262,144 - 2,048 particles piled on the
+    same 64-brush collider, then `frames` frames of spawn(4096) + step (the first one wraps)."""
+    from clay_engine_b200 import scenes
+    from oracle import oracle
+    from oracle.fluid_frame import OracleFluid
+
+    oracle.build()
+    cfg = scenes.CONFIG2
+    tap = cfg["tap"]
+    vd = oracle.VolumeData(192, 4, scenes.WORLD_ORIGIN, 24.0, 4.0)
+    d, m = oracle.build_brushes(vd, scenes.random_brushes(64, seed=seed), threads=threads)
+    vd.dist[:], vd.mat[:] = d, m
+    ref = OracleFluid(oracle, [vd], threads=threads, **cfg["fluid"])
+    p = scenes.lattice_block(262144 - 2048, 0.1, (0.0, -1.0, 0.0), 21)
+    p["vel"] = (0.0, -tap["speed"][0], 0.0)
+    ref.upload(p)
+    rng = np.random.default_rng(seed)
+    steps = 0
+    t0 = time.perf_counter()
+    for _ in range(frames):
+        ref.spawn(tap["n"], tap["pos"], (0.0, -float(rng.normal(*tap["speed"])), 0.0))
+        ref.step()
+        steps += ref.live
+    sec = time.perf_counter() - t0
+    return {"value": steps / sec, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{frames} frames of the full ring (262,144 particles), spawn(4096) each"}
+
+
+# The CPU sample both arms time: the 131 batched scenes nearest the median size (1.48 M
+# particles at the benchmark's seed), ~1.8 s per rep on 16 host cores.
+CPU_SAMPLE_PARTICLES = 1_500_000
+
+
 def reference_arm(args, ws, rank):
     """--impl reference: the oracle (the reference's algorithm restated on the CPU; the reference
-    itself is WebGPU/TypeScript and cannot run here) timed on host cores."""
+    itself is WebGPU/TypeScript and cannot run here) timed on all host cores, on the same sample
+    the other arm's cpu_baseline times: W untimed reps, then K timed ones."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    vals = []
-    for s in range(args.warmup + args.steps):
-        v, total, dt, desc = cpu_sample(args.scenes, 3, 150_000, threads)
-        if s >= args.warmup:
-            vals.append((total, dt))
-    tot = sum(t for t, _ in vals)
-    sec = sum(d for _, d in vals)
-    value = tot / sec
+    sample = CpuSample(args.scenes, 3, CPU_SAMPLE_PARTICLES, threads)
+    for _ in range(args.warmup):
+        sample.rep()
+    sec = sum(sample.rep() for _ in range(args.steps))
+    value = sample.particles * args.steps / sec
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sec / max(len(vals), 1),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sec / max(args.steps, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batched-256-scenes (bounded CPU sample)", "scenes": args.scenes,
                        "parallelism": "host threads"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": desc},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample.desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -602,6 +684,7 @@ def main():
     import torch
 
     import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
 
     torch.cuda.set_device(local)
     root = ce.init(local)
@@ -609,7 +692,7 @@ def main():
         stream = torch.cuda.Stream()
         with ClockSampler(local) as clocks:
             clocks.mark()
-            r = run_tap(root, args, stream, D.rank_seed(11, rank))
+            r = run_tap(root, stream, D.rank_seed(11, rank), args.steps, args.warmup)
             clocks.stop()
         value = D.reduce_sum(r["value"])
         if rank == 0:
@@ -713,6 +796,16 @@ def main():
         plain_value = total_particles * args.plain_steps / (plain_ms / 1000)
 
     clocks.__exit__(None, None, None)
+    clk = clocks.summary()
+    # ---- census of the frame's algorithmic work (untimed): neighbour candidates and accepted
+    # pairs of the last substep, the bake's in-band (particle, voxel) pairs, per scene
+    cand = acc = pairs = 0
+    for s in sims:
+        c = s.census(stream)
+        cand += c["candidates"]
+        acc += c["accepted"]
+        pairs += c["splat_pairs"]
+    body_pairs = sum(b.census(stream) for b in bodies)
     # algorithmic bytes of the bake: each (particle, level) reads its 16-byte position once; each
     # voxel the bake lowers is read and written once in the key grid (8 B)
     touched = 0
@@ -725,24 +818,46 @@ def main():
     # ---- roofline of the dominant kernel, k_splat (its fluid-surface launch "splat": the
     # SplatField bake of every fluid), from the per-launch event times of one frame
     peak, peak_kind = load_peaks()
+    # FP32 issue peak at the clock seen during the timed frames: 148 SMs x 128 FP32 lanes
+    mhz = clk.get("sm_mhz") or clk.get("sm_max_mhz") or 1965.0
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    lane_peak = sms * 128 * mhz * 1e6
     splat_ms, splat_launches = prof.get("splat", (None, 0))
     roof = {"bound": "hbm", "kernel": "k_splat (fluid surfaces)", "achieved": None, "peak": peak, "unit": "GB/s",
             "frac": None, "traffic": None, "peak_source": peak_kind}
     if splat_ms:
         avg_ms = splat_ms / splat_launches
         achieved = splat_bytes / (avg_ms / 1000) / 1e9
-        roof.update({"achieved": achieved, "frac": achieved / peak,
+        roof.update({"achieved": round(achieved, 2), "frac": achieved / peak,
                      "traffic": SPLAT_TRAFFIC_PER_PARTICLE * particles,
-                     "algorithmic_bytes_per_launch": splat_bytes, "avg_launch_ms": avg_ms,
-                     "limiter": "instruction issue (ncu: ~80% issue active, DRAM ~1% of peak)"})
-    # the neighbour passes against the same peak (one launch per block-size group and substep)
+                     "algorithmic_bytes_per_launch": splat_bytes, "avg_launch_ms": round(avg_ms, 4)})
+    # compute roofline (the kernels are issue-bound): algorithmic FP32 operations of the
+    # reference's work per second against the FP32 lane-issue peak. k_splat: 9 per in-band pair
+    # (3 sub, 3 mul, 2 add, 1 compare); k_density: 9 per candidate + 13 per accepted pair (the
+    # kernel term and the sum), over both substeps (the census counts the last one)
+    comp = {"unit": "FP32 lane-ops/s", "peak": lane_peak, "peak_source": f"{sms} SMs x 128 lanes x {mhz:.0f} MHz"}
+    if splat_ms:
+        ops = 9 * pairs
+        comp["k_splat"] = {"pairs": pairs, "pairs_per_s": pairs / (splat_ms / 1000), "ops_per_pair": 9,
+                           "frac": ops / (splat_ms / 1000) / lane_peak}
+    body_ms = prof.get("body_splat", (None, 0))[0]
+    if body_ms and body_pairs:
+        comp["k_splat_bodies"] = {"pairs": body_pairs, "pairs_per_s": body_pairs / (body_ms / 1000),
+                                  "frac": 12 * body_pairs / (body_ms / 1000) / lane_peak, "ops_per_pair": 12}
+    if "density" in prof:
+        dms = prof["density"][0]
+        ops = 2 * (9 * cand + 13 * acc)
+        comp["k_density"] = {"candidates": 2 * cand, "accepted": 2 * acc, "candidates_per_s": 2 * cand / (dms / 1000),
+                             "frac": ops / (dms / 1000) / lane_peak}
+    roof["compute"] = comp
+    # the neighbour passes against the HBM peak (one launch per block-size group and substep)
     others = {}
     for name, per in BYTES_PER_PARTICLE.items():
         if name in prof:
             ms_k, n_k = prof[name]
             byt = per * particles * 2 / max(n_k, 1)  # 2 substeps spread over the launches
-            others[name] = {"achieved_gbs": byt / (ms_k / n_k / 1000) / 1e9, "avg_launch_ms": ms_k / n_k,
-                            "algorithmic_bytes_per_launch": byt}
+            others[name] = {"achieved_gbs": round(byt / (ms_k / n_k / 1000) / 1e9, 2),
+                            "avg_launch_ms": round(ms_k / n_k, 4)}
     roof["neighbour_passes"] = others
 
     # ---- serving: free the batched scenes first, then a resident pool under Poisson arrivals
@@ -755,42 +870,77 @@ def main():
     served = None
     if not args.no_serve and not args.small:
         served = run_serving(root, args, seed + 50, stream)
+    threads = os.cpu_count() or 1
+    # ---- the plain configurations (small, and the tap at scale over its 120 frames)
+    configs = None
+    if rank == 0 and ws == 1 and not args.small:
+        small = run_small(root, stream, 120, max(args.warmup, 3))
+        tap = run_tap(root, stream, 11, scenes.CONFIG2["steps"], max(args.warmup, 3))
+        configs = {"small_4096": small, "tap_262144": tap}
+        if not args.no_cpu:
+            small["cpu_baseline"] = cpu_small(threads)
+            tap["cpu_baseline"] = cpu_tap(threads, 11)
     next_rows = None
     if rank == 0 and ws == 1 and not args.small and not args.no_next:
-        next_rows = measure_next_rows(root, stream, os.cpu_count() or 1)
+        next_rows = measure_next_rows(root, stream, threads)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        v, total, dt, desc = cpu_sample(n_scenes, seed, 1_500_000, os.cpu_count() or 1, frames=2)
-        cpu = {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port", "sample": desc}
+        sample = CpuSample(n_scenes, seed, CPU_SAMPLE_PARTICLES, threads)
+        sample.rep()  # warm
+        reps = 2
+        sec = sum(sample.rep() for _ in range(reps))
+        cpu = {"value": sample.particles * reps / sec, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": sample.desc + f", {reps} reps"}
         # the same oracle on one core, on a smaller sample (~10 s)
-        v1, _, _, desc1 = cpu_sample(n_scenes, seed, 120_000, 1, frames=1)
-        cpu["one_core"] = {"value": v1, "unit": UNIT, "cores": 1, "sample": desc1}
+        one = CpuSample(n_scenes, seed, 120_000, 1)
+        cpu["one_core"] = {"value": one.particles / one.rep(), "cores": 1, "sample": f"{one.particles} particles"}
 
     if rank == 0:
+        # The details first, on a line of their own that is not JSON (the rows after the frame,
+        # the per-kernel times, the full serving and tuning records) ...
+        detail = {"kernels_ms_per_frame": {k: round(v[0], 4) for k, v in prof.items()},
+                  "frame_ms_unfused": frame_ms, "served": served, "next_rows": next_rows,
+                  "autotune_trials": tune_report.get("trials", []), "census": {
+                      "particles": particles, "candidates_last_substep": cand, "accepted_last_substep": acc,
+                      "splat_pairs": pairs, "body_splat_pairs": body_pairs}}
+        print("# detail " + json.dumps(detail), flush=True)
+        # ... then the one JSON line, kept short enough to be read whole from the tail of the
+        # output, with the metric's own terms (plain, served) at its end
+        def r3(x):
+            return None if x is None else float(f"{x:.4g}")
+
+        srv = None
+        if served:
+            srv = {"throughput": r3(served["throughput"]), "p50_ms": r3(served["p50_ms"]),
+                   "p99_ms": r3(served["p99_ms"]), "rate_req_s": served["rate_req_s"],
+                   "demand": r3(served["demand_particle_steps_s"]), "completed": served["completed"]}
+            if "below_capacity" in served:
+                bc = served["below_capacity"]
+                srv["below_capacity"] = {"rate_req_s": r3(bc["rate_req_s"]), "throughput": r3(bc["throughput"]),
+                                         "p50_ms": r3(bc["p50_ms"]), "p99_ms": r3(bc["p99_ms"])}
+        cfgs = None
+        if configs:
+            cfgs = {k: {"value": r3(v["value"]), "ms_per_step": r3(v["ms_per_step"]), "frames": v["frames"],
+                        "cpu": r3(v.get("cpu_baseline", {}).get("value"))} for k, v in configs.items()}
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batched-256-scenes" if not args.small else "batched-16-scenes",
                        "scenes_per_gpu": n_scenes, "particles_per_gpu": particles, "substeps": 2,
-                       "bake": "64^3 x 3 mips band 4 (+32^3 x 2 body bakes)", "collider": "64^3 from 8 brushes",
-                       "parallelism": f"{ws} GPU(s), independent scenes per GPU", "cuda_graph": True,
-                       "l2": "working set larger than L2 (no flush needed)"},
-            "plain": {"value": plain_value, "unit": UNIT, "ratio_batched_over_plain":
-                      (value / plain_value) if plain_value else None},
-            "served": served,
-            "autotune": {"buckets_capacity_below": tuned["uppers"], "blocks": tuned["blocks"],
-                         "default_block": tuned["default"], "seconds": t_tune,
-                         "trials": len(tune_report.get("trials", []))},
+                       "bake": "64^3x3 band 4 (+32^3x2 bodies)", "collider": "64^3, 8 brushes",
+                       "parallelism": f"{ws} GPU(s), independent scenes", "cuda_graph": True,
+                       "l2": "working set > L2, no flush"},
+            "gpu_launches": int(launches),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 80 * n_sims * ws,
                     "d2h_bytes_per_step": 528 * n_sims * ws},
-            "gpu_launches": int(launches),
-            "roofline": roof,
-            "kernels_ms_per_frame": {k: round(v[0], 4) for k, v in prof.items()},
-            "frame_ms_unfused": frame_ms,
-            "clocks": clocks.summary(),
+            "clocks": clk,
             "cpu_baseline": cpu,
-            "next_rows": next_rows,
+            "roofline": roof,
+            "autotune": {"blocks": tuned["blocks"], "default": tuned["default"]},
+            "configs": cfgs,
+            "plain": {"value": plain_value, "ratio_batched_over_plain": (value / plain_value) if plain_value else None},
+            "served": srv,
         }
         print(json.dumps(line), flush=True)
 

@@ -66,6 +66,11 @@ class CloudDesc(C.Structure):
                 ("rotation", C.c_void_p)]
 
 
+class Census(C.Structure):
+    _fields_ = [("particles", C.c_uint64), ("candidates", C.c_uint64), ("accepted", C.c_uint64),
+                ("splat_pairs", C.c_uint64)]
+
+
 class SplatOpts(C.Structure):
     _fields_ = [("set", C.c_uint32), ("radius", C.c_double), ("material", C.c_double),
                 ("resolution", C.c_int32), ("mip_levels", C.c_int32), ("band", C.c_double),
@@ -189,6 +194,8 @@ SIGNATURES = {
     "clay_fluid_upload": (I, [P, P, C.c_int64, P]),
     "clay_fluid_download": (I, [P, P, C.c_int64, P]),
     "clay_fluid_cell_indices": (I, [P, P, P]),
+    "clay_fluid_census": (I, [P, P, C.POINTER(Census)]),
+    "clay_splat_census": (I, [P, P, C.POINTER(C.c_uint64)]),
     "clay_fluid_surface": (P, [P]),
     "clay_fluid_field": (P, [P]),
     "clay_fluid_get_info": (I, [P, C.POINTER(FluidInfo)]),

@@ -470,6 +470,12 @@ class SplatField:
     def bake(self, pass_=None):
         check(lib().clay_splat_bake(self.handle, stream_handle(pass_)))
 
+    def census(self, pass_=None) -> int:
+        """Measurement hook: the (particle, voxel) pairs a bake of the cloud as it is now lowers."""
+        v = C.c_uint64()
+        check(lib().clay_splat_census(self.handle, stream_handle(pass_), C.byref(v)))
+        return int(v.value)
+
     def capture_keys(self, keys_device):
         """Test hook: subsequent bakes copy their 16-bit keys into `keys_device` (u32 tensor)."""
         check(lib().clay_splat_capture_keys(self.handle, None if keys_device is None else _ptr(keys_device)))
@@ -584,6 +590,13 @@ class FluidSim:
         check(lib().clay_fluid_download(self.handle, out.ctypes.data if n else None, n, stream_handle(stream)))
         _sync(stream)
         return out
+
+    def census(self, stream=None) -> dict:
+        """Measurement hook: the algorithmic work of the last frame (neighbour candidates and
+        accepted pairs of its last substep, the bake's in-band (particle, voxel) pairs)."""
+        c = N.Census()
+        check(lib().clay_fluid_census(self.handle, stream_handle(stream), C.byref(c)))
+        return {k: int(getattr(c, k)) for k, _ in N.Census._fields_}
 
     def cell_indices(self) -> np.ndarray:
         """Test hook: the reference's cellIndex of every live particle (0xffffffff outside)."""

@@ -63,6 +63,27 @@ namespace {
   } while (0)
 
 constexpr int TILE = 8;
+constexpr int kMaxResolution = 4096;  // 4096^3 voxels per level: far beyond device memory, far below int64 overflow
+
+// SplatField's default mip count, Math.max(1, Math.log2(res / TILE) | 0) (splat.ts:149):
+// 1 wherever the logarithm is not a positive number (resolution 0 or below included).
+int default_splat_mips(int res) {
+  if (res <= 0) return 1;
+  return std::max(1, static_cast<int>(std::log2(static_cast<double>(res) / TILE)));
+}
+
+// A temporary device buffer of a host query, freed on every return path (an error included).
+template <class T>
+struct TempDev {
+  T* p = nullptr;
+  TempDev() = default;
+  TempDev(const TempDev&) = delete;
+  TempDev& operator=(const TempDev&) = delete;
+  ~TempDev() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t alloc(size_t n) { return cudaMalloc(&p, sizeof(T) * n); }
+};
 
 }  // namespace
 
@@ -283,6 +304,10 @@ namespace {
 
 // SdfVolume mip rule (volume.ts:140-160).
 int volume_mips(int resolution, int requested, bool has_req, int* out) {
+  // Checked first: the halving loop below never ends for 0 (the reference's does not either,
+  // volume.ts:148), and the cube of a larger resolution would overflow the 64-bit voxel count.
+  if (resolution <= 0 || resolution > kMaxResolution)
+    return fail(CLAY_EINVAL, "SdfVolume: resolution %d is outside 1..%d", resolution, kMaxResolution);
   int mips = requested;
   if (!has_req) {
     int halvings = 0;
@@ -406,7 +431,7 @@ int make_splat(clay_ctx* ctx, const clay_cloud_desc* cloud, const clay_splat_opt
   // splat.ts:148-153
   int res = (o->set & CLAY_SPLAT_RESOLUTION) ? o->resolution : 64;
   bool has_m = (o->set & CLAY_SPLAT_MIP_LEVELS) != 0;
-  int mips = has_m ? o->mip_levels : std::max(1, static_cast<int>(std::log2(static_cast<double>(res) / TILE)));
+  int mips = has_m ? o->mip_levels : default_splat_mips(res);
   double band = (o->set & CLAY_SPLAT_BAND) ? o->band : 2.0;
   double material = (o->set & CLAY_SPLAT_MATERIAL) ? o->material : 0.0;
   double world = (o->set & CLAY_SPLAT_WORLD_SIZE) ? o->world_size : 24.0;
@@ -743,18 +768,15 @@ int clay_field_query_mip(const clay_field* f, const float* pts, int n, int mip, 
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int rc = const_cast<clay_field*>(f)->flush(s);
   if (rc) return rc;
-  float *dp = nullptr, *ds = nullptr, *df = nullptr;
-  CK(cudaMalloc(&dp, sizeof(float) * 3 * n));
-  CK(cudaMalloc(&ds, sizeof(float) * 2 * n));
-  CK(cudaMalloc(&df, sizeof(float) * 2 * n));
-  CK(cudaMemcpyAsync(dp, pts, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
-  CK(L_field_query_mip(f->d, dp, n, mip, ds, df, s));
-  CK(cudaMemcpyAsync(sample_xy, ds, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(field_xy, df, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
+  TempDev<float> dp, ds, df;
+  CK(dp.alloc(3 * static_cast<size_t>(n)));
+  CK(ds.alloc(2 * static_cast<size_t>(n)));
+  CK(df.alloc(2 * static_cast<size_t>(n)));
+  CK(cudaMemcpyAsync(dp.p, pts, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
+  CK(L_field_query_mip(f->d, dp.p, n, mip, ds.p, df.p, s));
+  CK(cudaMemcpyAsync(sample_xy, ds.p, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(field_xy, df.p, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  cudaFree(dp);
-  cudaFree(ds);
-  cudaFree(df);
   return CLAY_OK;
 }
 
@@ -796,18 +818,15 @@ int clay_field_query(const clay_field* f, const float* pts, int n, float* sxy, f
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   int rc = const_cast<clay_field*>(f)->flush(s);
   if (rc) return rc;
-  float *dp = nullptr, *ds = nullptr, *dn = nullptr;
-  CK(cudaMalloc(&dp, sizeof(float) * 3 * n));
-  CK(cudaMalloc(&ds, sizeof(float) * 2 * n));
-  CK(cudaMalloc(&dn, sizeof(float) * 3 * n));
-  CK(cudaMemcpyAsync(dp, pts, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
-  CK(L_field_query(f->d, dp, n, ds, dn, s));
-  CK(cudaMemcpyAsync(sxy, ds, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(nrm, dn, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
+  TempDev<float> dp, ds, dn;
+  CK(dp.alloc(3 * static_cast<size_t>(n)));
+  CK(ds.alloc(2 * static_cast<size_t>(n)));
+  CK(dn.alloc(3 * static_cast<size_t>(n)));
+  CK(cudaMemcpyAsync(dp.p, pts, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, s));
+  CK(L_field_query(f->d, dp.p, n, ds.p, dn.p, s));
+  CK(cudaMemcpyAsync(sxy, ds.p, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(nrm, dn.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  cudaFree(dp);
-  cudaFree(ds);
-  cudaFree(dn);
   return CLAY_OK;
 }
 
@@ -906,7 +925,7 @@ int fluid_options(const clay_fluid_opts& o, clay_fluid* f) {
   f->bake_res = (o.set & CLAY_FLUID_BAKE_RESOLUTION) ? o.bake_resolution : 64;
   f->bake_mips = (o.set & CLAY_FLUID_BAKE_MIP_LEVELS)
                      ? o.bake_mip_levels
-                     : std::max(1, static_cast<int>(std::log2(static_cast<double>(f->bake_res) / TILE)));
+                     : default_splat_mips(f->bake_res);
   f->band = (o.set & CLAY_FLUID_BAKE_BAND) ? o.bake_band : 2.0;
   f->world_size = (o.set & CLAY_FLUID_WORLD_SIZE) ? o.world_size : 24.0;
   double org[3] = {-12, -4, -12};
@@ -1225,8 +1244,8 @@ int clay_fluid_cell_indices(clay_fluid* f, uint32_t* host, void* stream) {
   if (!f || !host) return fail(CLAY_EINVAL, "clay_fluid_cell_indices: NULL argument");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (f->live == 0) return CLAY_OK;
-  uint32_t* d = nullptr;
-  CK(cudaMalloc(&d, sizeof(uint32_t) * f->live));
+  TempDev<uint32_t> d;
+  CK(d.alloc(static_cast<size_t>(f->live)));
   // the uniform's count must be current for the kernel
   clay_fluid_params p = f->frozen;
   p.count = static_cast<uint32_t>(f->live);
@@ -1238,10 +1257,58 @@ int clay_fluid_cell_indices(clay_fluid* f, uint32_t* host, void* stream) {
     f->written = p;
     f->written_valid = true;
   }
-  CK(L_cell_index(f->d_scene, d, static_cast<int>(f->live), s));
-  CK(cudaMemcpyAsync(host, d, sizeof(uint32_t) * f->live, cudaMemcpyDeviceToHost, s));
+  CK(L_cell_index(f->d_scene, d.p, static_cast<int>(f->live), s));
+  CK(cudaMemcpyAsync(host, d.p, sizeof(uint32_t) * f->live, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
-  cudaFree(d);
+  return CLAY_OK;
+}
+
+namespace {
+// The bake pairs of one splat over every level, added to *d_out (device) on stream s.
+int census_splat(clay_splat* sp, unsigned long long* d_out, cudaStream_t s) {
+  int rc = sp->flush(s);
+  if (rc) return rc;
+  const uint32_t cap = sp->cloud.capacity;
+  if (cap == 0) return CLAY_OK;
+  CK(L_census_splat(sp->d, static_cast<int>((cap + 255) / 256), sp->mips, d_out, s));
+  return CLAY_OK;
+}
+}  // namespace
+
+int clay_fluid_census(clay_fluid* f, void* stream, clay_census* out) {
+  if (!f || !out) return fail(CLAY_EINVAL, "clay_fluid_census: NULL argument");
+  std::memset(out, 0, sizeof(*out));
+  out->particles = static_cast<uint64_t>(f->live);
+  if (f->live == 0) return CLAY_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  TempDev<unsigned long long> d;
+  CK(d.alloc(3));
+  CK(cudaMemsetAsync(d.p, 0, 3 * sizeof(unsigned long long), s));
+  CK(L_census_nbr(f->d_scene, static_cast<int>(f->live), d.p, s));
+  int rc = census_splat(f->surface, d.p + 2, s);
+  if (rc) return rc;
+  unsigned long long h[3] = {0, 0, 0};
+  CK(cudaMemcpyAsync(h, d.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  out->candidates = h[0];
+  out->accepted = h[1];
+  out->splat_pairs = h[2];
+  return CLAY_OK;
+}
+
+int clay_splat_census(clay_splat* sp, void* stream, uint64_t* pairs_out) {
+  if (!sp || !pairs_out) return fail(CLAY_EINVAL, "clay_splat_census: NULL argument");
+  *pairs_out = 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  TempDev<unsigned long long> d;
+  CK(d.alloc(1));
+  CK(cudaMemsetAsync(d.p, 0, sizeof(unsigned long long), s));
+  int rc = census_splat(sp, d.p, s);
+  if (rc) return rc;
+  unsigned long long h = 0;
+  CK(cudaMemcpyAsync(&h, d.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  *pairs_out = h;
   return CLAY_OK;
 }
 

@@ -1987,6 +1987,90 @@ __global__ void k_cell_index(const SceneDev* __restrict__ scenes, uint32_t* __re
 }
 
 // ---------------------------------------------------------------------------------------
+// Census of the algorithmic work of a frame (a measurement hook, never part of a step): the
+// work the reference's own passes do, counted on the state the last step left.
+//  - k_census_nbr: over the cell-ordered copies of the last substep, the neighbour candidates
+//    the density pass tests (fluid.ts:346-364, with the bucket limit) and, of them, the pairs
+//    within the smoothing length (self included) that it sums (:357-361).
+//  - k_census_splat: the (particle, voxel) pairs of the bake whose distance passes
+//    sd < bandWorld (splat.ts:246), i.e. the reference's atomicMin count, over every level
+//    (blockIdx.y), with the reference's own arithmetic per voxel.
+// Counts go to out[] with one 64-bit atomic per warp.
+__device__ __forceinline__ void census_add(unsigned long long* out, uint32_t v) {
+  const uint32_t s = __reduce_add_sync(0xffffffffu, v);
+  if ((threadIdx.x & 31) == 0 && s) atomicAdd(out, static_cast<unsigned long long>(s));
+}
+
+__global__ void k_census_nbr(const SceneDev* __restrict__ scenes, unsigned long long* __restrict__ out) {
+  const SceneDev& S = scenes[0];
+  const uint32_t count = work_count(S);
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t cand = 0, acc = 0;
+  if (k < count) {
+    const BoxInfo b = box_from_state(S.gs);
+    const bool overflow = S.gs->overflow != 0u;
+    const float4 me = S.spos[k];
+    int cx, cy, cz;
+    cell_of(S, me.x, me.y, me.z, cx, cy, cz);
+    for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
+      const float4 o = S.spos[q];
+      const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+      cand++;
+      if ((dx * dx + dy * dy) + dz * dz < S.h2) acc++;
+    });
+  }
+  census_add(out, cand);
+  census_add(out + 1, acc);
+}
+
+__global__ void k_census_splat(const SplatDev* __restrict__ d, unsigned long long* __restrict__ out) {
+  const SplatDev& D = *d;
+  const int m = static_cast<int>(blockIdx.y);
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t i = 0, hits = 0;
+  if (cloud_live(D, idx, i)) {
+    const float voxel = D.voxel[m], bw = D.bw[m], reach = D.reach[m], inv_voxel = D.inv_voxel[m];
+    const int last = D.r[m] - 1;
+    const float* pp = reinterpret_cast<const float*>(D.pos + static_cast<size_t>(i) * D.pos_stride);
+    const float px = pp[0] - D.vp->origin[0], py = pp[1] - D.vp->origin[1], pz = pp[2] - D.vp->origin[2];
+    const bool has_n = D.nrm != nullptr;
+    float nx = 0.0f, ny = 0.0f, nz = 0.0f;
+    if (has_n) {
+      const float* nn = reinterpret_cast<const float*>(D.nrm + static_cast<size_t>(i) * D.nrm_stride);
+      nx = nn[0];
+      ny = nn[1];
+      nz = nn[2];
+      if (D.quat) {  // quatRotate (math/gpu.ts:21-25)
+        const float qx = D.quat[0], qy = D.quat[1], qz = D.quat[2], qw = D.quat[3];
+        const float tx = (qy * nz - qz * ny) * 2.0f, ty = (qz * nx - qx * nz) * 2.0f, tz = (qx * ny - qy * nx) * 2.0f;
+        const float rx = (nx + tx * qw) + (qy * tz - qz * ty);
+        const float ry = (ny + ty * qw) + (qz * tx - qx * tz);
+        const float rz = (nz + tz * qw) + (qx * ty - qy * tx);
+        nx = rx;
+        ny = ry;
+        nz = rz;
+      }
+    }
+    const int lx = max(f2i(floorf((px - reach) * inv_voxel)), 0), hx = min(f2i(floorf((px + reach) * inv_voxel)), last);
+    const int ly = max(f2i(floorf((py - reach) * inv_voxel)), 0), hy = min(f2i(floorf((py + reach) * inv_voxel)), last);
+    const int lz = max(f2i(floorf((pz - reach) * inv_voxel)), 0), hz = min(f2i(floorf((pz + reach) * inv_voxel)), last);
+    for (int z = lz; z <= hz; z++) {
+      const float dz = (static_cast<float>(z) + 0.5f) * voxel - pz;
+      for (int y = ly; y <= hy; y++) {
+        const float dy = (static_cast<float>(y) + 0.5f) * voxel - py;
+        for (int x = lx; x <= hx; x++) {
+          const float dx = (static_cast<float>(x) + 0.5f) * voxel - px;
+          float sd = sqrtf((dx * dx + dy * dy) + dz * dz) - D.radius;
+          if (has_n) sd = fmaxf(dot3(dx, dy, dz, nx, ny, nz), sd);
+          if (sd < bw) hits++;
+        }
+      }
+    }
+  }
+  census_add(out, hits);
+}
+
+// ---------------------------------------------------------------------------------------
 // SurfaceExtractor.extract (extract.ts:469-475): naive surface nets of the field's zero set
 // on a res^3 lattice. The reference hands out particle and quad slots with atomics, so their
 // order is unspecified; here a block scan gives them in lattice order (cells, then lattice

@@ -148,6 +148,9 @@ void drop_batch(clay_server* s) {
 }
 
 // Evicts an idle resident scene: its particle state goes to the host, its sim is freed.
+// Served scenes never emit (the server has no spawn request), so the particle records and
+// their count are the whole state: a re-admitted sim starts its emission ring at the count
+// (clay_fluid_upload), which is where it stood.
 int evict(clay_server* s, int32_t id) {
   Scene& sc = s->scenes[static_cast<size_t>(id)];
   // the batch references the sim: it is rebuilt before the next launch

@@ -106,6 +106,13 @@ cudaError_t L_build(const BuildLevelDev& lv, const BrushDev* brushes, int n, cud
 cudaError_t L_cell_index(const SceneDev* s, uint32_t* out, int n, cudaStream_t st) {
   CLAY_LAUNCH(k_cell_index, (n + 255) / 256, 256, st, s, out);
 }
+cudaError_t L_census_nbr(const SceneDev* s, int n, unsigned long long* out, cudaStream_t st) {
+  CLAY_LAUNCH(k_census_nbr, (n + 255) / 256, 256, st, s, out);
+}
+cudaError_t L_census_splat(const SplatDev* d, int blocks, int mips, unsigned long long* out, cudaStream_t st) {
+  dim3 g(blocks, mips);
+  CLAY_LAUNCH(k_census_splat, g, 256, st, d, out);
+}
 cudaError_t L_gather_contacts(const SceneDev* s, int n, ContactsDev* out, cudaStream_t st) {
   CLAY_LAUNCH(k_gather_contacts, n, 128, st, s, n, out);
 }

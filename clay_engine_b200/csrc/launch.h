@@ -54,6 +54,10 @@ cudaError_t L_ext_qemit(const ExtractDev* e, int blocks, cudaStream_t st);
 cudaError_t L_ext_finish(const ExtractDev* e, cudaStream_t st);
 cudaError_t L_build(const BuildLevelDev& lv, const BrushDev* brushes, int n, cudaStream_t st);
 cudaError_t L_cell_index(const SceneDev* s, uint32_t* out, int n, cudaStream_t st);
+// Census of a frame's algorithmic work (measurement hooks): out[0] += candidates, out[1] +=
+// accepted pairs over `n` cell-ordered particles; out[0] += bake pairs over `blocks` x `mips`.
+cudaError_t L_census_nbr(const SceneDev* s, int n, unsigned long long* out, cudaStream_t st);
+cudaError_t L_census_splat(const SplatDev* d, int blocks, int mips, unsigned long long* out, cudaStream_t st);
 cudaError_t L_gather_contacts(const SceneDev* s, int n, ContactsDev* out, cudaStream_t st);
 cudaError_t L_field_query(const FieldDev* f, const float* pts, int n, float* sxy, float* nrm, cudaStream_t st);
 

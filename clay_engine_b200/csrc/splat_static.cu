@@ -5,8 +5,10 @@
 // device and stall the frame, and plugin hosts that hand a library only buffers allocated
 // up front and forbid it to grow device memory afterwards. For them this file provides
 // clay_splat_bake_static: the caller passes the particle cloud (inputs) and the f16 output
-// plane(s); the bake's only scratch, the 16-bit key grid the splat takes the minimum into,
-// lives in a fixed file-scope device array instead of a per-object allocation.
+// plane(s); the bake's only scratch, one 32-bit word per voxel holding the smallest distance
+// lowered into it as an order-preserving integer of its f32 bits (the resolve pass turns it
+// into the reference's 16-bit key), lives in a fixed file-scope device array instead of a
+// per-object allocation.
 //
 // The array holds at most kStaticKeys keys (4 MiB) and every GPU that loads the library
 // keeps it until the process exits. All calls share it: each call clears the part it uses
@@ -22,6 +24,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 
@@ -101,6 +104,13 @@ using namespace clay;
 extern "C" int clay_splat_bake_static(const clay_cloud_desc* cloud, const clay_splat_opts* o, void* dist_out_f16,
                                       void* material_out_f16, void* stream) {
   if (!cloud || !o || !dist_out_f16) return report_error(CLAY_EINVAL, "clay_splat_bake_static: NULL argument");
+  // the resolve pass stores the distance plane two halves at a time, the material pass one half
+  if (reinterpret_cast<uintptr_t>(dist_out_f16) % 4 != 0)
+    return report_error(CLAY_EINVAL, "clay_splat_bake_static: dist_out_f16 must be 4-byte aligned");
+  if (material_out_f16 && reinterpret_cast<uintptr_t>(material_out_f16) % 2 != 0)
+    return report_error(CLAY_EINVAL, "clay_splat_bake_static: material_out_f16 must be 2-byte aligned");
+  if (cloud->capacity > 0 && (reinterpret_cast<uintptr_t>(cloud->positions) % 4 != 0 || cloud->position_stride % 4 != 0))
+    return report_error(CLAY_EINVAL, "clay_splat_bake_static: positions must be 4-byte aligned with a stride of whole floats");
   if (!cloud->positions && cloud->capacity > 0) return report_error(CLAY_EINVAL, "clay_splat_bake_static: no positions");
   if (cloud->position_stride < 12 && cloud->capacity > 1)
     return report_error(CLAY_EINVAL, "clay_splat_bake_static: position stride below 12 bytes");
@@ -110,6 +120,17 @@ extern "C" int clay_splat_bake_static(const clay_cloud_desc* cloud, const clay_s
     return report_error(CLAY_EINVAL, "clay_splat_bake_static: bad live rule");
   // The options of SplatField (splat.ts:148-153) and the SdfVolume mip rule (volume.ts:156-160).
   const int res = (o->set & CLAY_SPLAT_RESOLUTION) ? o->resolution : 64;
+  // Bound the resolution before anything is derived from it: no level of a bake above
+  // kStaticMaxRes fits the scratch, and the cubes below stay far from 64-bit overflow.
+  constexpr int kStaticMaxRes = 128;
+  if (res <= 0 || res > kStaticMaxRes) {
+    char msg[192];
+    std::snprintf(msg, sizeof(msg),
+                  "clay_splat_bake_static: resolution %d is outside 1..%d (the static scratch holds at most %lld voxels)",
+                  res, kStaticMaxRes, kStaticKeys);
+    return report_error(CLAY_EINVAL, msg);
+  }
+  if (!(o->radius >= 0)) return report_error(CLAY_EINVAL, "clay_splat_bake_static: radius must be a non-negative number");
   const int mips = (o->set & CLAY_SPLAT_MIP_LEVELS) ? o->mip_levels
                                                     : std::max(1, static_cast<int>(std::log2(static_cast<double>(res) / 8)));
   const double band = (o->set & CLAY_SPLAT_BAND) ? o->band : 2.0;

@@ -176,3 +176,44 @@ CONFIG5 = dict(
     rate=2000.0, k_lo=1, k_hi=8, pool=1024, n_lo=2048, n_hi=262144, bakes=(32, 64, 128),
     budget_bytes=150 * 10 ** 9,
 )
+
+
+def config3_scene(root, i, n, seed, with_body=True, mode=None):
+    """Scene `i` of the batched configuration: a FluidSim of capacity `n` over its own 64^3
+    collider of 8 seeded brushes, its particles a jittered lattice block resting above the
+    floor; every `body_every`-th scene also carries a clay-body shell (surface-net particles
+    of a sphere, oriented discs) baked into a 32^3 x 2 SplatField that follows the body via
+    setCenter, unioned into the scene's collider. Returns a dict: sim, body (the body's
+    SplatField or None), collider (its SdfVolume), body_center, keep (objects the scene needs
+    alive)."""
+    import torch
+
+    from .core import FluidSim, SdfVolume, SplatField, bodyCloud, unionField, volumeField
+
+    cfg = CONFIG3
+    bcfg = cfg["body"]
+    vol = SdfVolume(root, resolution=cfg["collider"]["resolution"], worldSize=WORLD_SIZE, origin=WORLD_ORIGIN)
+    vol.build(random_brushes(8, seed=seed * 100003 + i, lo=(-10, -3.5, -10), hi=(10, 1.0, 10)))
+    world = volumeField(vol)
+    keep = [vol, world]
+    body = center = None
+    if with_body and i % cfg["body_every"] == 0:
+        center = (2.0, -1.4, 1.0)
+        shell, shell_n = surface_net_sphere(bcfg["radius"], bcfg["cell"])
+        parts, brec = body_records(shell + np.array(center, np.float32), shell_n, center)
+        dp = torch.from_numpy(parts.view(np.uint8)).cuda()
+        db = torch.from_numpy(brec.view(np.uint8)).cuda()
+        box = bcfg["bake_box"]
+        body = SplatField(root, bodyCloud(dp, db, 0), radius=(box / bcfg["bake_res"]) * 1.15,
+                          resolution=bcfg["bake_res"], band=bcfg["band"], worldSize=box)
+        body.setCenter(center)
+        world = unionField(world, body.field)
+        keep += [dp, db, body, world]
+    o = dict(cfg["fluid"])
+    o["capacity"] = int(n)
+    sim = FluidSim(root, world, o)
+    if mode:
+        sim.set_mode(mode)
+    side = math.ceil(n ** (1 / 3)) * 0.1
+    sim.upload(lattice_block(int(n), 0.1, (0.0, -2.3 + side / 2, 0.0), seed * 7919 + i))
+    return {"sim": sim, "body": body, "collider": vol, "body_center": center, "keep": keep, "options": o}

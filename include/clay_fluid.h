@@ -230,6 +230,10 @@ void clay_splat_destroy(clay_splat* s);
 int clay_splat_set_center(clay_splat* s, double x, double y, double z);
 /* SplatField.bake (splat.ts:296-304). */
 int clay_splat_bake(clay_splat* s, void* stream);
+/* Measurement hook, no counterpart in the reference: the (particle, voxel) pairs a bake of
+ * the cloud as it is now lowers (sd < bandWorld, splat.ts:246), over every level.
+ * Allocates a small temporary and synchronises `stream`. */
+int clay_splat_census(clay_splat* s, void* stream, uint64_t* pairs_out);
 /* A SplatField bake that allocates no device memory. No counterpart in the reference: it
  * is for callers that may not allocate once running - a per-frame tick where cudaMalloc or
  * cudaFree would synchronise the device and stall the frame, or a plugin host that gives
@@ -389,6 +393,20 @@ int clay_fluid_download(const clay_fluid* sim, clay_fluid_particle* host, int64_
  * particleCount particles, or 0xffffffff for a particle outside the grid (fluid.ts:319-321).
  * Host output; synchronises `stream`. */
 int clay_fluid_cell_indices(clay_fluid* sim, uint32_t* host_out, void* stream);
+/* Measurement hook, no counterpart in the reference: the algorithmic work of the frame the
+ * last clay_fluid_step did, counted with the reference's own arithmetic. `candidates` are
+ * the neighbours the density pass tests (fluid.ts:346-364) and `accepted` those within the
+ * smoothing length (self included, :357-361), both over the cell order of the LAST substep
+ * (multiply by the substeps for a frame); `splat_pairs` are the (particle, voxel) pairs of
+ * the surface bake with sd < bandWorld (splat.ts:246: the reference's atomicMin count), over
+ * every level. Allocates a small temporary and synchronises `stream`. */
+typedef struct clay_census {
+  uint64_t particles;
+  uint64_t candidates;
+  uint64_t accepted;
+  uint64_t splat_pairs;
+} clay_census;
+int clay_fluid_census(clay_fluid* sim, void* stream, clay_census* out);
 /* FluidSim.surface / .field (fluid.ts:119-120); owned by the sim. */
 clay_splat* clay_fluid_surface(clay_fluid* sim);
 clay_field* clay_fluid_field(clay_fluid* sim);
@@ -600,7 +618,9 @@ typedef struct clay_server_stats {
   int32_t inflight;
 } clay_server_stats;
 int clay_server_get_stats(const clay_server* s, clay_server_stats* out);
-/* The scene's FluidSim while it is resident, else NULL (valid until the next pump). */
+/* The scene's FluidSim while it is resident, else NULL (valid until the next pump). An
+ * eviction keeps the particle records and their count only: a spawn made through this
+ * view that is still pending, and the sim's emission seed, do not survive it. */
 int clay_server_scene_sim(clay_server* s, int32_t scene, clay_fluid** sim_out);
 /* The scene's particle state after all its submitted frames: waits for them, then copies
  * from the device (resident) or the host snapshot (evicted). `n_out`: live particles. */

@@ -1,0 +1,260 @@
+"""Parity at the benchmark's own configurations, in the modes the benchmark runs.
+
+- The tap at scale (capacity 262,144, spawn(4096) every frame, a 192^3 collider of 64 seeded
+  brushes, a 128^3 x 4 band-4 bake): in reference mode bit for bit against the oracle, both
+  while the ring fills from empty and with the ring full and wrapping over a pile resting on
+  the collider (particle state, contact counter, bake keys); in fast mode teacher-forced each
+  frame, every field within the fast-mode tolerance and the bake bit-exact on the GPU's own
+  positions.
+- A sample of the batched scenes (the largest of the 256, the smallest, and one whose collider
+  is unioned with a clay-body shell bake) stepped in fast mode in one Batch whose scenes fall
+  into three thread-block-size groups, teacher-forced each frame: every field within the
+  tolerance, bake bit-exact on the GPU's positions, density within 1e-4 of the f64 twin.
+
+Set PRECISION_REPORT=<path> to write the measured errors as JSON.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle.fluid_frame import OracleFluid
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 8
+# The fast-mode bounds of the small-configuration test: relative to the field's largest
+# magnitude; pressure = stiffness * (rho - rho0) cancels, so it has its own bound.
+FAST_REL_TOL = 2e-5
+FAST_REL_TOL_PRESSURE = 2e-4
+FIELDS = ("pos", "vel", "nvel", "density", "pressure")
+
+
+def report(key, value):
+    path = os.environ.get("PRECISION_REPORT")
+    data = {}
+    if path and os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+    data[key] = value
+    if path:
+        with open(path, "w") as f:
+            json.dump(data, f, indent=1)
+    print(key, value)
+
+
+def assert_bits_equal(g, r, n, what):
+    for name in FIELDS:
+        a = np.ascontiguousarray(g[name][:n]).view(np.uint32)
+        b = np.ascontiguousarray(r[name][:n]).view(np.uint32)
+        bad = np.nonzero((a != b).reshape(n, -1).any(1))[0]
+        assert bad.size == 0, f"{what}{name}: {bad.size} particles differ, first {bad[:4]}"
+
+
+def rel_errors(g, r, n):
+    out = {}
+    for name in FIELDS:
+        a = g[name][:n].astype(np.float64)
+        b = r[name][:n].astype(np.float64)
+        scale = max(float(np.abs(b).max()), 1e-6)
+        out[name] = float(np.abs(a - b).max()) / scale
+    return out
+
+
+def assert_within_fast_tolerance(errs, what):
+    for name, err in errs.items():
+        tol = FAST_REL_TOL_PRESSURE if name == "pressure" else FAST_REL_TOL
+        assert err <= tol, f"{what}{name}: rel err {err:.3g} > {tol:g}"
+
+
+def keys_of(sim):
+    import torch
+
+    keys = torch.zeros(sim.surface.volume.totalVoxels, dtype=torch.int32, device="cuda")
+    sim.surface.capture_keys(keys)
+    return keys
+
+
+def oracle_keys_on(oracle, ref, pos, n):
+    """The oracle's bake of the given positions (the bake is exact in every mode)."""
+    cloud = oracle.CloudData(np.ascontiguousarray(pos), live_mode=1, live_a=n)
+    return oracle.splat_keys(ref.splat, cloud, threads=THREADS)
+
+
+# ---------------------------------------------------------------------------------------
+# The tap at scale
+
+def tap_pair(root, oracle, mode):
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    cfg = scenes.CONFIG2
+    vol = ce.SdfVolume(root, resolution=cfg["collider"]["resolution"], worldSize=24.0, origin=scenes.WORLD_ORIGIN)
+    vol.build(scenes.random_brushes(64, seed=11))
+    d, m = vol.download()
+    ov = oracle.VolumeData(vol.resolution, vol.mipLevels, scenes.WORLD_ORIGIN, 24.0, 4.0, dist=d, mat=m)
+    field = ce.volumeField(vol)
+    sim = ce.FluidSim(root, field, cfg["fluid"])
+    sim.set_mode(mode)
+    ref = OracleFluid(oracle, [ov], threads=THREADS, **cfg["fluid"])
+    return sim, ref, (vol, field)
+
+
+def full_ring_pile():
+    """262,144 - 2,048 particles in a jittered block resting on the collider's floor and
+    brushes, falling at 1.5 m/s: the first spawn of 4,096 wraps the ring."""
+    from clay_engine_b200 import scenes
+
+    p = scenes.lattice_block(262144 - 2048, 0.1, (0.0, -1.0, 0.0), 21)
+    p["vel"] = (0.2, -1.5, 0.1)
+    return p
+
+
+def tap_spawn(sim, ref, rng, cfg):
+    tap = cfg["tap"]
+    vel = (0.0, -float(rng.normal(*tap["speed"])), 0.0)
+    sim.spawn(tap["n"], tap["pos"], vel)
+    ref.spawn(tap["n"], tap["pos"], vel)
+
+
+def test_tap_reference_mode_bit_exact(root, oracle):
+    """Config 2 in reference mode: 3 frames filling the ring from empty, then 2 frames with
+    the ring full and wrapping over a pile on the collider."""
+    import torch
+
+    from clay_engine_b200 import scenes
+
+    cfg = scenes.CONFIG2
+    rng = np.random.default_rng(5)
+    for phase, start in (("fill", None), ("wrap", full_ring_pile())):
+        sim, ref, keep = tap_pair(root, oracle, "reference")
+        if start is not None:
+            sim.upload(start)
+            ref.upload(start)
+        keys = keys_of(sim)
+        contacts = 0
+        for frame in range(3 if phase == "fill" else 2):
+            tap_spawn(sim, ref, rng, cfg)
+            sim.step()
+            ok = ref.step()
+            n = sim.particleCount
+            assert n == ref.live
+            assert_bits_equal(sim.download(), ref.parts, n, f"{phase} frame {frame}: ")
+            gk = keys.cpu().numpy().view(np.uint32)
+            assert np.array_equal(gk, ok), f"{phase} frame {frame}: {(gk != ok).sum()} bake keys differ"
+            pts, count = sim.readContacts()
+            assert count == ref.contacts[0], f"{phase} frame {frame}: contacts {count} vs {ref.contacts[0]}"
+            contacts += count
+        if phase == "wrap":
+            assert sim.particleCount == 262144
+            assert contacts > 0, "vacuous: the pile never touched the collider"
+        torch.cuda.synchronize()
+        sim.destroy()
+
+
+def test_tap_fast_mode_teacher_forced(root, oracle):
+    """Config 2 in fast mode (the benchmark's mode), each frame from the GPU's own state."""
+    from clay_engine_b200 import scenes
+
+    cfg = scenes.CONFIG2
+    rng = np.random.default_rng(6)
+    sim, ref, keep = tap_pair(root, oracle, "fast")
+    p = full_ring_pile()
+    sim.upload(p)
+    ref.upload(p)
+    keys = keys_of(sim)
+    worst = {}
+    for frame in range(3):
+        n0 = sim.particleCount
+        ref.parts[:n0] = sim.download()  # teacher forcing; the emission bookkeeping stays in step
+        tap_spawn(sim, ref, rng, cfg)
+        sim.step()
+        ref.step()
+        n = sim.particleCount
+        assert n == ref.live
+        g = sim.download()
+        errs = rel_errors(g, ref.parts, n)
+        assert_within_fast_tolerance(errs, f"frame {frame}: ")
+        for k, v in errs.items():
+            worst[k] = max(worst.get(k, 0.0), v)
+        gk = keys.cpu().numpy().view(np.uint32)
+        ok = oracle_keys_on(oracle, ref, g["pos"], n)
+        assert np.array_equal(gk, ok), f"frame {frame}: {(gk != ok).sum()} bake keys differ on the GPU's positions"
+    report("tap_262144_fast_vs_f32_oracle", {"frames": 3, "max_rel_err": worst})
+    sim.destroy()
+
+
+# ---------------------------------------------------------------------------------------
+# A sample of the batched scenes, in one Batch with three block-size groups
+
+def test_batched_sample_fast_mode_teacher_forced(root, oracle):
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    cfg = scenes.CONFIG3
+    seed = 3  # the benchmark's seed
+    counts = scenes.log_uniform_counts(cfg["scenes"], cfg["n_lo"], cfg["n_hi"], seed)
+    big = int(np.argmax(counts))
+    small = int(np.argmin(counts))
+    with_body = next(i for i in range(len(counts)) if i % cfg["body_every"] == 0 and 4096 <= counts[i] < 16384)
+    chosen = [big, small, with_body]
+    built = [scenes.config3_scene(root, i, int(counts[i]), seed, mode="fast") for i in chosen]
+    assert built[2]["body"] is not None
+    sims = [b["sim"] for b in built]
+    bodies = [b["body"] for b in built if b["body"] is not None]
+    for b in bodies:
+        b.bake()  # the body is static: its bake is the same every frame
+    batch = ce.Batch(root, sims, extra_splats=bodies)
+    # capacity < 4096 -> 128 threads, < 16384 -> 192, the rest 256: three groups per pass
+    batch.set_bucket_blocks([4096, 16384, 65536], [128, 192, 256])
+    refs = []
+    for b in built:
+        d, m = b["collider"].download()
+        vols = [oracle.VolumeData(64, b["collider"].mipLevels, scenes.WORLD_ORIGIN, 24.0, 4.0, dist=d, mat=m)]
+        if b["body"] is not None:
+            bv = b["body"].volume
+            bd, bm = bv.download()
+            box = cfg["body"]["bake_box"]
+            borigin = tuple(c - box / 2 for c in b["body_center"])
+            vols.append(oracle.VolumeData(bv.resolution, bv.mipLevels, borigin, box, cfg["body"]["band"],
+                                          dist=bd, mat=bm))
+        refs.append(OracleFluid(oracle, vols, threads=THREADS, **b["options"]))
+    keys = [keys_of(s) for s in sims]
+    worst = {}
+    d64_err = 0.0
+    for frame in range(3):
+        states = [s.download() for s in sims]
+        for s, r, st in zip(sims, refs, states):
+            r.upload(st)
+        batch.step()
+        for k, (s, r, st, i) in enumerate(zip(sims, refs, states, chosen)):
+            r.step()
+            n = s.particleCount
+            g = s.download()
+            errs = rel_errors(g, r.parts, n)
+            assert_within_fast_tolerance(errs, f"scene {i} ({n} particles) frame {frame}: ")
+            for f, v in errs.items():
+                worst[f] = max(worst.get(f, 0.0), v)
+            gk = keys[k].cpu().numpy().view(np.uint32)
+            ok = oracle_keys_on(oracle, r, g["pos"], n)
+            assert np.array_equal(gk, ok), f"scene {i} frame {frame}: {(gk != ok).sum()} bake keys differ"
+            if frame == 0:
+                # density of the first substep against the f64 twin, from the same input state: a
+                # one-substep step of a twin sim in fast mode
+                prm = oracle.params_from(dict(r.frozen, count=n, emit_base=0, emit_count=0))
+                d64 = oracle.fluid_density_f64(r.cfg, prm, st, threads=THREADS)[:, 0]
+                one = ce.FluidSim(root, None, dict(built[k]["options"], substeps=1))
+                one.set_mode("fast")
+                one.upload(st)
+                one.step()
+                rel = np.abs(one.download()["density"].astype(np.float64) - d64) / np.abs(d64)
+                d64_err = max(d64_err, float(rel.max()))
+                one.destroy()
+    assert d64_err <= 1e-4, f"density vs f64: {d64_err:.3g}"
+    report("batched_sample_fast_vs_f32_oracle", {"scenes": [int(counts[i]) for i in chosen], "frames": 3,
+                                                 "block_groups": [128, 192, 256], "max_rel_err": worst,
+                                                 "density_vs_f64_max_rel": d64_err})
+    batch.destroy()
+    for b in built:
+        b["sim"].destroy()

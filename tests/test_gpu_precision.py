@@ -123,3 +123,41 @@ def test_position_drift_over_240_frames(root, oracle):
     sim.destroy()
     field.destroy()
     vol.destroy()
+
+
+def test_position_drift_million_particles(root, oracle):
+    """Config 4's own size: 1,048,576 particles over the 288^3 collider, 2 substeps, against
+    the f64 twin stepped on the host cores for 10 frames (about 2-4 s per frame on 16 cores;
+    the 240 frames of the configuration would take over 10 minutes there, so the 240-frame
+    drift is measured on 16k particles above). Reported, not gated beyond the first frame."""
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    n = 1 << 20
+    vol, field, ov = collider(root, oracle, 288)
+    opts = dict(capacity=n, spacing=0.1, radius=0.05, substeps=2, gravity=(0, -9.8, 0), bakeResolution=128,
+                bakeMipLevels=4, bakeBand=4.0, worldSize=24.0, origin=ORIGIN)
+    sim = ce.FluidSim(root, field, opts)
+    p = scenes.lattice_block(n, 0.1, (0.0, 1.0, 0.0), 4)
+    p["vel"] = (0.2, -1.0, 0.1)
+    sim.upload(p)
+    from oracle.fluid_frame import OracleFluid
+
+    ref = OracleFluid(oracle, [ov], threads=THREADS, **opts)
+    parts64 = oracle.to_f64(p)
+    drift = []
+    for frame in range(10):
+        sim.step()
+        prm = oracle.params_from(dict(ref.frozen, count=n, emit_base=0, emit_count=0))
+        for _ in range(opts["substeps"]):
+            oracle.fluid_substep_f64(ref.cfg, prm, ref.field, parts64, threads=THREADS)
+        if frame in (0, 1, 4, 9):
+            g = sim.download()
+            dp = np.linalg.norm(g["pos"].astype(np.float64) - parts64["pos"], axis=1)
+            drift.append({"frame": frame + 1, "max": float(dp.max()), "mean": float(dp.mean()),
+                          "p99": float(np.percentile(dp, 99))})
+    report("position_drift_1m_vs_f64", drift)
+    assert drift[0]["max"] < 1e-4
+    sim.destroy()
+    field.destroy()
+    vol.destroy()

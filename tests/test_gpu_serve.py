@@ -101,13 +101,18 @@ def test_budget_admission_and_eviction_keep_state(root, colliders):
     est = [serve.scene_bytes_estimate(options(i)) for i in range(len(COUNTS))]
     budget = est[1] + est[3] + 1024  # two of the larger scenes at a time
     srv = server(root, colliders, budget, stream)
-    s = srv.serve([(0.0, 0, 2), (0.0, 1, 2), (0.0, 2, 1), (0.0, 3, 2), (0.001, 4, 1), (0.002, 0, 2)])
+    # scene 0 steps twice and goes idle; scenes 1 and 3 then need more room than is left beside
+    # it, so scene 0 (the least recently used idle scene) must be evicted to admit them
+    srv.serve([(0.0, 0, 2)])
+    srv.serve([(0.0, 1, 2), (0.0, 3, 2)])
+    assert srv.sim(0) is None, "scene 0 should have been evicted"
+    assert srv.stats()["evictions"] >= 1
+    # scene 0 comes back with its state and steps twice more, in a mix with other scenes
+    s = srv.serve([(0.0, 0, 2), (0.0, 2, 1), (0.001, 4, 1)])
     st = srv.stats()
-    assert s["completed"] == 6 and st["completed"] == 6
-    assert st["evictions"] > 0
+    assert s["completed"] == 3 and st["completed"] == 6
     assert st["resident_bytes"] <= budget
-    # scene 0 made 4 frames in two requests, possibly evicted and restored in between
-    for i, frames in ((0, 4), (1, 2), (2, 1)):
+    for i, frames in ((0, 4), (1, 2), (2, 1), (3, 2), (4, 1)):
         ref = plain(root, colliders, i, frames, stream)
         assert same_particles(srv.download(i), ref.download()), i
         ref.destroy()

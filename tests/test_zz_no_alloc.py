@@ -22,14 +22,15 @@ def _cloud(n, seed, center):
     return p.astype(np.float32)
 
 
-def _bake_both(root, host_pos, res, mips, band, radius, origin):
+def _bake_both(root, host_pos, res, mips, band, radius, origin, cloud=None):
     import torch
 
     import clay_engine_b200 as ce
     from clay_engine_b200 import _native as N
 
-    dpos = torch.from_numpy(host_pos).cuda()
-    cloud = ce.ParticleCloud(len(host_pos), dpos, stride=12)
+    if cloud is None:
+        dpos = torch.from_numpy(host_pos).cuda()
+        cloud = ce.ParticleCloud(len(host_pos), dpos, stride=12)
     # the allocating entry point
     s = ce.SplatField(root, cloud, radius=radius, resolution=res, mipLevels=mips, band=band, worldSize=24.0,
                       origin=origin, material=2.0)
@@ -59,6 +60,34 @@ def test_static_bake_matches_the_allocating_bake_twice(root):
         assert np.array_equal(d, ref_d), f"call {call}: {(d != ref_d).sum()} voxels differ"
         assert np.array_equal(m, ref_m), f"call {call}: material differs"
         assert (ref_d != 0x3C00).sum() > 1000, "vacuous: nothing was baked"
+
+
+def test_static_bake_matches_for_discs_and_a_live_count(root):
+    """The other branches of the splat: an oriented-disc cloud (normals rotated by a body
+    quaternion, as bodyCloud bakes a clay body) and a cloud whose live count, read on the
+    device, is below its capacity. Each twice in a row, bit for bit against clay_splat_bake."""
+    import torch
+
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    origin = (-12.0, -4.0, -12.0)
+    pos, nrm = scenes.surface_net_sphere(0.95, 0.076, center=(1.0, 0.5, -0.5))
+    rec = np.zeros((len(pos), 8), np.float32)  # 32-byte records: position, pad, normal, pad
+    rec[:, 0:3], rec[:, 4:7] = pos, nrm
+    drec = torch.from_numpy(rec).cuda()
+    quat = torch.tensor([0.0, 0.3826834, 0.0, 0.9238795], dtype=torch.float32, device="cuda")
+    discs = ce.ParticleCloud(len(pos), drec, stride=32, normals=drec[:, 4:], normal_stride=32, rotation=quat)
+    dense = _cloud(30000, 5, (0.5, 1.0, 0.0))
+    dpos = torch.from_numpy(dense).cuda()
+    live = torch.tensor([21000], dtype=torch.int32, device="cuda")
+    counted = ce.ParticleCloud(len(dense), dpos, stride=12, live=("count", live))
+    for call in range(2):
+        for name, cloud, radius in (("discs", discs, 0.083 * 1.15), ("live count", counted, 0.11)):
+            ref_d, ref_m, d, m = _bake_both(root, None, 64, 3, 4.0, radius, origin, cloud=cloud)
+            assert np.array_equal(d, ref_d), f"{name}, call {call}: {(d != ref_d).sum()} voxels differ"
+            assert np.array_equal(m, ref_m), f"{name}, call {call}: material differs"
+            assert (ref_d != 0x3C00).sum() > 1000, f"{name}: vacuous, nothing was baked"
 
 
 def test_static_bake_refuses_beyond_its_maximum(root):
