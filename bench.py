@@ -711,13 +711,14 @@ def main():
     sims, bodies, keep = build_scenes(root, n_scenes, seed)
     particles = sum(s.particleCount for s in sims)
     stream = torch.cuda.Stream()
-    # autotune (untimed): block size of the particle passes per scene-size bucket
+    # autotune (untimed): per scene-size bucket, the particle passes' block size, the density
+    # variant and the splat's strategy thresholds
     from clay_engine_b200 import autotune
 
     t_tune = time.perf_counter()
-    tuned, tune_report = autotune.tune(root, sims, bodies, stream, frames=8, use_cache=False)
+    tuned, tune_report = autotune.tune(root, sims, bodies, stream, frames=10, use_cache=False)
     t_tune = time.perf_counter() - t_tune
-    batch = ce.Batch(root, sims, extra_splats=bodies, use_graph=True, sph_block=tuned["default"])
+    batch = ce.Batch(root, sims, extra_splats=bodies, use_graph=True, sph_block=tuned["tunings"][-1]["sph_block"])
     autotune.apply(batch, tuned)
     torch.cuda.synchronize()
     clocks = ClockSampler(local).__enter__()
@@ -937,7 +938,8 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "roofline": roof,
-            "autotune": {"blocks": tuned["blocks"], "default": tuned["default"]},
+            "autotune": {"changed": tuned["changed"], "gain": r3(tuned["gain"]),
+                         "trials": len(tune_report.get("trials", []))},
             "configs": cfgs,
             "plain": {"value": plain_value, "ratio_batched_over_plain": (value / plain_value) if plain_value else None},
             "served": srv,

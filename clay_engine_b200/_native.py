@@ -66,6 +66,11 @@ class CloudDesc(C.Structure):
                 ("rotation", C.c_void_p)]
 
 
+class BucketTuning(C.Structure):
+    _fields_ = [("sph_block", C.c_int32), ("density_two_phase", C.c_int32), ("splat_tile_ratio", C.c_int32),
+                ("splat_walk_weight", C.c_int32)]
+
+
 class Census(C.Structure):
     _fields_ = [("particles", C.c_uint64), ("candidates", C.c_uint64), ("accepted", C.c_uint64),
                 ("splat_pairs", C.c_uint64)]
@@ -205,6 +210,7 @@ SIGNATURES = {
     "clay_batch_set_tuning": (I, [P, C.POINTER(BatchTuning)]),
     "clay_batch_get_tuning": (I, [P, C.POINTER(BatchTuning)]),
     "clay_batch_set_bucket_blocks": (I, [P, P, P, I]),
+    "clay_batch_set_bucket_tuning": (I, [P, P, P, I]),
     "clay_batch_step": (I, [P, P]),
     "clay_batch_step_subset": (I, [P, P, I, P]),
     "clay_batch_read_contacts_async": (I, [P, P, P]),

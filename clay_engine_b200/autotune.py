@@ -1,12 +1,18 @@
-"""Autotuner: picks the thread-block size of the particle passes per scene-size bucket.
+"""Autotuner: picks, per scene-size bucket, the launch shapes and strategies of the frame.
 
-Scenes are grouped by capacity into buckets. For each bucket in turn (coordinate descent,
-the other buckets held at their current choice), every candidate block size is timed over a
-few real batched frames (CUDA graph replays, CUDA events on the launching stream) and the
-fastest kept. The scenes' particle state is saved before tuning, restored before every
-candidate (so all are timed from the same state) and after tuning, so tuning does not advance
-the simulation. Results are cached per bucket signature in a JSON
-file next to the library.
+Scenes are grouped by capacity into buckets. The knobs of a bucket are the thread-block size of
+the particle passes, the density pass's variant (one loop, or distance tests then the accepted
+neighbours) and the splat's strategy thresholds (how much larger than the particles' own voxel
+boxes a block's union box may be and still take the register-blocked tile walk, or the block
+walk). Every setting gives the same results (reference mode bit for bit); they only move time
+between code paths, so the choice is a pure timing decision.
+
+Search: coordinate descent, bucket after bucket and knob after knob (the others held at their
+current choice). Every value of a knob is timed over real batched frames (CUDA graph replays,
+CUDA events on the launching stream) from the same saved particle state, and a value replaces
+the current one only when it is faster by more than `min_gain` of the frame. The scenes' state
+is restored after tuning, so tuning does not advance the simulation. Results are cached per
+bucket signature in a JSON file next to the library.
 """
 from __future__ import annotations
 
@@ -18,7 +24,13 @@ import numpy as np
 from .core import Batch
 
 BUCKETS = (4096, 16384, 65536)       # capacity < 4k, < 16k, < 64k, and the rest
-CANDIDATES = (64, 128, 192, 256)
+KNOBS = {
+    "sph_block": (64, 128, 192, 256),
+    "density_two_phase": (0, 1),
+    "splat_tile_ratio": (3, 6, 12),
+    "splat_walk_weight": (2, 3, 6),
+}
+DEFAULT = {"sph_block": 256, "density_two_phase": 1, "splat_tile_ratio": 6, "splat_walk_weight": 3}
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "autotune.json")
 
 
@@ -32,7 +44,7 @@ def bucket_index(capacity: int) -> int:
 def signature(sims) -> str:
     counts = np.bincount([bucket_index(s.capacity) for s in sims], minlength=len(BUCKETS) + 1)
     # scenes per bucket rounded to a power of two: similar batches share a tuning
-    return "b" + "-".join(str(1 << int(np.ceil(np.log2(c)))) if c else "0" for c in counts)
+    return "t" + "-".join(str(1 << int(np.ceil(np.log2(c)))) if c else "0" for c in counts)
 
 
 def _time(batch, stream, frames):
@@ -49,8 +61,20 @@ def _time(batch, stream, frames):
     return a.elapsed_time(z) / frames
 
 
-def tune(root, sims, extra=(), stream=None, frames=8, use_cache=True, default=256, min_gain=0.02):
-    """Returns ({"uppers": [...], "blocks": [...]}, report) for this set of scenes."""
+def _trial(root, sims, extra, snaps, choice, stream, frames):
+    # every trial from the same state: stepping moves the fluid, and a later, more spread-out
+    # state would cost more whatever the setting
+    for s, snap in zip(sims, snaps):
+        s.upload(snap)
+    batch = Batch(root, sims, extra_splats=extra, sph_block=choice[len(BUCKETS)]["sph_block"], use_graph=True)
+    apply(batch, {"uppers": list(BUCKETS), "tunings": [choice[i] for i in range(len(BUCKETS) + 1)]})
+    ms = _time(batch, stream, frames)
+    batch.destroy()
+    return ms
+
+
+def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=0.005):
+    """Returns ({"uppers": [...], "tunings": [per bucket dict], "gain": ...}, report)."""
     import torch
 
     stream = stream or torch.cuda.current_stream()
@@ -65,35 +89,38 @@ def tune(root, sims, extra=(), stream=None, frames=8, use_cache=True, default=25
     if use_cache and sig in cache:
         return cache[sig], {"cached": True, "signature": sig}
     present = sorted({bucket_index(s.capacity) for s in sims})
-    choice = {i: default for i in range(len(BUCKETS) + 1)}
+    choice = {i: dict(DEFAULT) for i in range(len(BUCKETS) + 1)}
     snaps = [s.download() for s in sims]
     report = {"signature": sig, "trials": []}
     try:
+        base_ms = _trial(root, sims, extra, snaps, choice, stream, frames)
+        best_ms = base_ms
         for bi in present:
-            times = {}
-            for cand in CANDIDATES:
-                choice[bi] = cand
-                # every candidate is timed from the same state (stepping moves the fluid, and a
-                # later, more spread-out state would cost more whatever the block size)
-                for s, snap in zip(sims, snaps):
-                    s.upload(snap)
-                batch = Batch(root, sims, extra_splats=extra, sph_block=choice[len(BUCKETS)], use_graph=True)
-                batch.set_bucket_blocks(list(BUCKETS), [choice[i] for i in range(len(BUCKETS))])
-                ms = _time(batch, stream, frames)
-                batch.destroy()
-                times[cand] = ms
-                report["trials"].append({"bucket": bi, "block": cand, "ms": ms})
-            # keep the default unless a candidate beats it by more than the timing noise
-            best_b = min(times, key=times.get)
-            if times[best_b] > times[default] * (1.0 - min_gain):
-                best_b = default
-            choice[bi] = best_b
+            for knob, values in KNOBS.items():
+                times = {choice[bi][knob]: best_ms}
+                for v in values:
+                    if v in times:
+                        continue
+                    cand = {i: dict(c) for i, c in choice.items()}
+                    cand[bi][knob] = v
+                    times[v] = _trial(root, sims, extra, snaps, cand, stream, frames)
+                    report["trials"].append({"bucket": bi, knob: v, "ms": round(times[v], 4)})
+                best_v = min(times, key=times.get)
+                if times[best_v] < best_ms * (1.0 - min_gain):
+                    choice[bi][knob] = best_v
+                    best_ms = times[best_v]
+        # the chosen settings against the defaults, timed again side by side
+        default = {i: dict(DEFAULT) for i in range(len(BUCKETS) + 1)}
+        t_default = _trial(root, sims, extra, snaps, default, stream, frames)
+        t_tuned = _trial(root, sims, extra, snaps, choice, stream, frames)
     finally:
         torch.cuda.synchronize()
         for s, snap in zip(sims, snaps):
             s.upload(snap)
-    result = {"uppers": list(BUCKETS), "blocks": [choice[i] for i in range(len(BUCKETS))],
-              "default": choice[len(BUCKETS)]}
+    result = {"uppers": list(BUCKETS), "tunings": [choice[i] for i in range(len(BUCKETS) + 1)],
+              "default_ms": t_default, "tuned_ms": t_tuned, "gain": t_default / t_tuned - 1.0,
+              "changed": [{"bucket": i, **{k: v for k, v in choice[i].items() if v != DEFAULT[k]}}
+                          for i in present if choice[i] != DEFAULT]}
     if use_cache:
         cache[sig] = result
         os.makedirs(os.path.dirname(CACHE), exist_ok=True)
@@ -103,4 +130,4 @@ def tune(root, sims, extra=(), stream=None, frames=8, use_cache=True, default=25
 
 
 def apply(batch, result):
-    batch.set_bucket_blocks(result["uppers"], result["blocks"])
+    batch.set_bucket_tuning(result["uppers"], result["tunings"])

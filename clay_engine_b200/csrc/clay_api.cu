@@ -508,6 +508,8 @@ int make_splat(clay_ctx* ctx, const clay_cloud_desc* cloud, const clay_splat_opt
       h.inv_voxel[m] = static_cast<float>(1 / voxel);
     }
     h.total = vol->total;
+    h.tile_ratio = kSplatTileRatio;
+    h.walk_weight = kSplatWalkWeight;
     s->desc_dirty = true;
     cudaStream_t st = nullptr;
     rc = s->flush(st);
@@ -1358,16 +1360,34 @@ struct clay_batch {
   // distinct block size per pass.
   std::vector<int64_t> bucket_upper;
   std::vector<int> bucket_block;
+  // Per bucket (bucket_upper.size() + 1 entries once set, the last for the larger scenes):
+  // the density variant and the splat's strategy thresholds of the scenes in it.
+  std::vector<clay_bucket_tuning> bucket_tune;
   struct PartGroup {
     Work* w;
     int n;
     int T;
+    bool two_phase;
   };
   std::vector<PartGroup> groups;
-  int block_of(int64_t capacity) const {
+  int bucket_of(int64_t capacity) const {
     for (size_t i = 0; i < bucket_upper.size(); i++)
-      if (capacity < bucket_upper[i]) return bucket_block[i];
-    return tune.sph_block;
+      if (capacity < bucket_upper[i]) return static_cast<int>(i);
+    return static_cast<int>(bucket_upper.size());
+  }
+  int block_of(int64_t capacity) const {
+    const size_t i = static_cast<size_t>(bucket_of(capacity));
+    return i < bucket_block.size() ? bucket_block[i] : tune.sph_block;
+  }
+  clay_bucket_tuning tuning_of(int64_t capacity) const {
+    const size_t i = static_cast<size_t>(bucket_of(capacity));
+    if (i < bucket_tune.size()) return bucket_tune[i];
+    clay_bucket_tuning t{};
+    t.sph_block = block_of(capacity);
+    t.density_two_phase = kDensityTwoPhase ? 1 : 0;
+    t.splat_tile_ratio = static_cast<int32_t>(kSplatTileRatio);
+    t.splat_walk_weight = static_cast<int32_t>(kSplatWalkWeight);
+    return t;
   }
   int64_t launches_per_step = 0;
   // The scenes' FluidParams, contiguous, written from pinned memory in one copy per frame
@@ -1445,17 +1465,20 @@ int batch_build(clay_batch* b) {
   std::vector<SceneDev> scenes;
   std::vector<Work> wp, we, wsc;
   b->max_substeps = 0;
-  std::vector<int> blocks;
+  // one group of particle-pass launches per distinct (block size, density variant)
+  std::vector<std::pair<int, bool>> blocks;
   std::vector<std::vector<Work>> by_block;
   for (size_t i = 0; i < b->sims.size(); i++) {
     clay_fluid* f = b->sims[i];
     scenes.push_back(f->hs);
     b->max_substeps = std::max(b->max_substeps, f->substeps);
     uint32_t obj = static_cast<uint32_t>(i);
-    const int Ts = b->block_of(f->capacity);
-    size_t gi = std::find(blocks.begin(), blocks.end(), Ts) - blocks.begin();
+    const clay_bucket_tuning bt = b->tuning_of(f->capacity);
+    const int Ts = bt.sph_block;
+    const std::pair<int, bool> key(Ts, bt.density_two_phase != 0);
+    size_t gi = std::find(blocks.begin(), blocks.end(), key) - blocks.begin();
     if (gi == blocks.size()) {
-      blocks.push_back(Ts);
+      blocks.push_back(key);
       by_block.emplace_back();
     }
     for (int64_t x = 0; x < f->capacity; x += Ts) {
@@ -1478,6 +1501,9 @@ int batch_build(clay_batch* b) {
     clay_splat* s = b->sims[i]->surface;
     SplatDev d = s->h;
     d.order = s->order;
+    const clay_bucket_tuning bt = b->tuning_of(b->sims[i]->capacity);
+    d.tile_ratio = static_cast<uint32_t>(bt.splat_tile_ratio);
+    d.walk_weight = static_cast<uint32_t>(bt.splat_walk_weight);
     ss.push_back(d);
     add_splat_work(wss, wsr, static_cast<uint32_t>(i), s, b->sims[i]->capacity, kSplatThreads);
   }
@@ -1508,7 +1534,7 @@ int batch_build(clay_batch* b) {
   for (size_t g = 0; g < blocks.size(); g++) {
     Work* w = nullptr;
     if ((rc = b->upload_table(&w, by_block[g]))) return rc;
-    b->groups.push_back({w, static_cast<int>(by_block[g].size()), blocks[g]});
+    b->groups.push_back({w, static_cast<int>(by_block[g].size()), blocks[g].first, blocks[g].second});
   }
   b->n_emit = static_cast<int>(we.size());
   b->n_scan = static_cast<int>(wsc.size());
@@ -1537,8 +1563,8 @@ int batch_enqueue(clay_batch* b, cudaStream_t s) {
       for (auto& g : b->groups) CK(L_cell_scatter(d, g.w, g.n, g.T, sub, s));
       for (auto& g : b->groups) CK(L_cell_order(d, g.w, g.n, g.T, sub, s));
       for (auto& g : b->groups) {
-        if (b->mode == CLAY_MODE_REFERENCE) CK(L_density_ref(d, g.w, g.n, g.T, sub, s));
-        else CK(L_density_fast(d, g.w, g.n, g.T, sub, s));
+        if (b->mode == CLAY_MODE_REFERENCE) CK(L_density_ref(d, g.w, g.n, g.T, sub, s, g.two_phase));
+        else CK(L_density_fast(d, g.w, g.n, g.T, sub, s, g.two_phase));
       }
       for (auto& g : b->groups) {
         if (b->mode == CLAY_MODE_REFERENCE) CK(L_forces_ref(d, g.w, g.n, g.T, sub, s));
@@ -1606,6 +1632,24 @@ int clay_batch_set_bucket_blocks(clay_batch* b, const int64_t* upper, const int3
   }
   b->bucket_upper.assign(upper, upper + n);
   b->bucket_block.assign(blocks, blocks + n);
+  b->bucket_tune.clear();
+  b->release();
+  return CLAY_OK;
+}
+
+int clay_batch_set_bucket_tuning(clay_batch* b, const int64_t* upper, const clay_bucket_tuning* t, int n) {
+  if (!b || n < 0 || !t || (n > 0 && !upper)) return fail(CLAY_EINVAL, "clay_batch_set_bucket_tuning: bad argument");
+  for (int i = 0; i <= n; i++) {
+    if (t[i].sph_block < 64 || t[i].sph_block > 256 || (t[i].sph_block & 31))
+      return fail(CLAY_EINVAL, "bucket block %d must be a multiple of 32 in 64..256", t[i].sph_block);
+    if (t[i].splat_tile_ratio < 1 || t[i].splat_tile_ratio > 64 || t[i].splat_walk_weight < 1 || t[i].splat_walk_weight > 64)
+      return fail(CLAY_EINVAL, "bucket splat thresholds must be in 1..64");
+    if (i > 0 && i < n && upper[i] <= upper[i - 1]) return fail(CLAY_EINVAL, "bucket bounds must increase");
+  }
+  b->bucket_upper.assign(upper, upper + n);
+  b->bucket_block.clear();
+  for (int i = 0; i < n; i++) b->bucket_block.push_back(t[i].sph_block);
+  b->bucket_tune.assign(t, t + n + 1);
   b->release();
   return CLAY_OK;
 }
@@ -1732,7 +1776,8 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
         if ((rc = timed("cell_order", [&] { return L_cell_order(d, g.w, g.n, g.T, sub, s); }))) return rc;
       for (auto& g : b->groups)
         if ((rc = timed("density", [&] {
-               return ref ? L_density_ref(d, g.w, g.n, g.T, sub, s) : L_density_fast(d, g.w, g.n, g.T, sub, s);
+               return ref ? L_density_ref(d, g.w, g.n, g.T, sub, s, g.two_phase)
+                          : L_density_fast(d, g.w, g.n, g.T, sub, s, g.two_phase);
              })))
           return rc;
       for (auto& g : b->groups)

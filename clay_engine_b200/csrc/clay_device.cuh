@@ -168,7 +168,13 @@ struct __align__(16) SplatDev {
   long long off[kMaxMips];
   float voxel[kMaxMips], bw[kMaxMips], reach[kMaxMips], inv_voxel[kMaxMips];
   long long total;
+  // Strategy thresholds of the splat (every strategy gives the same keys): a sphere block takes
+  // the register-blocked tile walk while its union box holds at most tile_ratio times the pairs
+  // of the particles' own boxes; the block walk is taken while its pairs (x2 for discs) are at
+  // most walk_weight times those of the own boxes.
+  uint32_t tile_ratio, walk_weight;
 };
+constexpr uint32_t kSplatTileRatio = 6, kSplatWalkWeight = 3;
 
 // A unit of work of one launch: object index (scene or splat), sub-index (mip level or
 // scan part), first element, element count.
@@ -829,8 +835,52 @@ __device__ __forceinline__ void for_neighbours(const SceneDev& S, const BoxInfo&
   }
 }
 
-// density (fluid.ts:333-368). kFast accumulates with Kahan-Neumaier compensation.
-template <bool kFast>
+// The same 27 cells as contiguous ranges of the cell order, in the reference's visiting
+// order: f(s, e) once per (dz, dy) row of cells (or per cell, capped at `bucket`, when some
+// cell of the scene overflowed).
+template <class F>
+__device__ __forceinline__ void for_neighbour_ranges(const SceneDev& S, const BoxInfo& b, bool overflow, int cx, int cy,
+                                                     int cz, F&& f) {
+  const int G = S.G;
+  cx = min(max(cx, -2), G + 1);
+  cy = min(max(cy, -2), G + 1);
+  cz = min(max(cz, -2), G + 1);
+  const int x1b = b.x0 + static_cast<int>(b.bx) - 1;
+  const int y1b = b.y0 + static_cast<int>(b.by) - 1;
+  const int z1b = b.z0 + static_cast<int>(b.bz) - 1;
+  if (b.L == 0) return;
+  int xl = max(cx - 1, b.x0), xh = min(cx + 1, x1b);
+  if (xl > xh) return;
+  for (int dz = -1; dz <= 1; dz++) {
+    int z = cz + dz;
+    if (z < b.z0 || z > z1b) continue;
+    for (int dy = -1; dy <= 1; dy++) {
+      int y = cy + dy;
+      if (y < b.y0 || y > y1b) continue;
+      uint32_t row = b.bx * (static_cast<uint32_t>(y - b.y0) + b.by * static_cast<uint32_t>(z - b.z0));
+      uint32_t l0 = row + static_cast<uint32_t>(xl - b.x0);
+      uint32_t l1 = row + static_cast<uint32_t>(xh - b.x0);
+      if (!overflow) {
+        f(__ldg(S.cell_start + l0), __ldg(S.cell_start + l1 + 1));
+      } else {
+        for (uint32_t l = l0; l <= l1; l++) {
+          uint32_t s = __ldg(S.cell_start + l), e = __ldg(S.cell_start + l + 1);
+          f(s, s + min(e - s, S.bucket));
+        }
+      }
+    }
+  }
+}
+
+// density (fluid.ts:333-368). kFast accumulates with Kahan compensation.
+//
+// kTwoPhase takes the candidates of a range 32 at a time in two phases: the distance test of
+// every candidate, which leaves a bit mask of the accepted ones, then the accepted ones alone,
+// in ascending order (the reference's visiting order), each re-read from cache. A warp's lanes
+// accept at different candidates, so running the accept work inside the test loop (the other
+// variant) keeps most lanes idle through it; in the second phase every lane with a pending
+// neighbour works. Both variants visit, sum and list the neighbours in the same order.
+template <bool kFast, bool kTwoPhase>
 __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
@@ -852,27 +902,52 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   uint32_t* __restrict__ nl = reinterpret_cast<uint32_t*>(S.nbr + k);
   const uint32_t stride = 4u * S.capacity;
   uint32_t cnt = 0;
-  for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
-    float4 o = __ldg(spos + q);
-    float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
-    float r2 = (dx * dx + dy * dy) + dz * dz;
-    if (r2 < h2) {
-      if (cnt < kMaxNbr) nl[(cnt >> 2) * stride + (cnt & 3u)] = q;
-      cnt++;
-      float wv = h2 - r2;
-      float term = mp6 * ((wv * wv) * wv);
-      if (kFast) {
-        // Neumaier: explicit round-to-nearest adds so nothing is contracted into an FMA.
-        float t = __fadd_rn(rho, term);
-        if (fabsf(rho) >= fabsf(term)) comp = __fadd_rn(comp, __fadd_rn(__fsub_rn(rho, t), term));
-        else comp = __fadd_rn(comp, __fadd_rn(__fsub_rn(term, t), rho));
-        rho = t;
-      } else {
-        rho = rho + term;
+  // one accepted neighbour q at squared length r2, in visiting order
+  auto accept = [&](uint32_t q, float r2) {
+    if (cnt < kMaxNbr) nl[(cnt >> 2) * stride + (cnt & 3u)] = q;
+    cnt++;
+    // fast mode may contract a recomputed length differently from the test: a pair at the
+    // boundary then adds a term of order (h^2 * 1e-7)^3, not a missing neighbour
+    const float wv = fmaxf(h2 - r2, 0.0f);
+    const float term = mp6 * ((wv * wv) * wv);
+    if (kFast) {
+      // Kahan: explicit round-to-nearest operations so nothing is contracted into an FMA
+      // (every term is positive, so the running sum bounds each term after the first)
+      const float y = __fsub_rn(term, comp);
+      const float t = __fadd_rn(rho, y);
+      comp = __fsub_rn(__fsub_rn(t, rho), y);
+      rho = t;
+    } else {
+      rho = rho + term;
+    }
+  };
+  if (!kTwoPhase) {
+    for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
+      const float4 o = __ldg(spos + q);
+      const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+      const float r2 = (dx * dx + dy * dy) + dz * dz;
+      if (r2 < h2) accept(q, r2);
+    });
+  } else for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e) {
+    for (uint32_t base = s; base < e; base += 32u) {
+      const uint32_t n = min(32u, e - base);
+      uint32_t m = 0;
+      for (uint32_t i = 0; i < n; i++) {
+        const float4 o = __ldg(spos + base + i);
+        const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+        const float r2 = (dx * dx + dy * dy) + dz * dz;
+        m |= (r2 < h2 ? 1u : 0u) << i;
+      }
+      while (m) {
+        const uint32_t q = base + static_cast<uint32_t>(__ffs(m) - 1);
+        m &= m - 1u;
+        const float4 o = __ldg(spos + q);
+        const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+        accept(q, (dx * dx + dy * dy) + dz * dz);
       }
     }
   });
-  if (kFast) rho = __fadd_rn(rho, comp);
+  if (kFast) rho = __fsub_rn(rho, comp);
   const float stiff = S.prm->stiffness;
   const float dens = fmaxf(rho, S.rest_floor);
   const float pres = fmaxf(stiff * (rho - S.rest), 0.0f), inv = __frcp_rn(dens);
@@ -1252,13 +1327,13 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     // pair evaluations of the block walk against those of each particle's own box, weighted by
     // their relative cost (the block walk's pair is ~3x cheaper for spheres, ~1.5x for discs)
     const uint64_t lhs = bnu * nlive * (has_n ? 2ull : 1ull);
-    const uint64_t rhs = s_cost * 3ull;
+    const uint64_t rhs = s_cost * D.walk_weight;
     // Spheres, union box within the shared tile: register-blocked block walk. A work item is
     // a brick of 4 x 2 x 2 voxels against a slice of the block's particles; the squared
     // lengths share dx*dx, dy*dy, dz*dz and dx*dx + dy*dy across the brick (the reference's
     // rounding order is kept), minima go to the shared tile as float bits (non-negative
     // floats order like their bit patterns), and the tile is turned into keys at the end.
-    if (!has_n && bnu <= acc_cap && bnu * nlive <= s_cost * 6ull) {
+    if (!has_n && bnu <= acc_cap && bnu * nlive <= s_cost * D.tile_ratio) {
       extern __shared__ uint32_t s_tile[];
       const uint32_t nbu = static_cast<uint32_t>(bnu);
       for (uint32_t v = threadIdx.x; v < nbu; v += blockDim.x) s_tile[v] = 0x7f800000u;

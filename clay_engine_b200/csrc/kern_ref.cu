@@ -44,8 +44,12 @@ cudaError_t L_cell_scatter(const SceneDev* s, const Work* w, int blocks, int thr
 cudaError_t L_cell_order(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
   CLAY_LAUNCH(k_cell_order, blocks, threads, st, s, w, sub);
 }
-cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
-  CLAY_LAUNCH(k_density<false>, blocks, threads, st, s, w, sub);
+cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
+                          bool two_phase) {
+  if (two_phase) k_density<false, true><<<blocks, threads, 0, st>>>(s, w, sub);
+  else k_density<false, false><<<blocks, threads, 0, st>>>(s, w, sub);
+  count_launch();
+  return cudaPeekAtLastError();
 }
 cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
   CLAY_LAUNCH(k_forces_integrate<false>, blocks, threads, st, s, w, sub);

@@ -187,6 +187,8 @@ extern "C" int clay_splat_bake_static(const clay_cloud_desc* cloud, const clay_s
     off += static_cast<long long>(h.r[m]) * h.r[m] * h.r[m];
   }
   h.total = total;
+  h.tile_ratio = kSplatTileRatio;
+  h.walk_weight = kSplatWalkWeight;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   // The array keeps the last call's values: start from the clear value kNoHit.
   k_static_clear<<<static_cast<unsigned>((total + 255) / 256), 256, 0, s>>>(keys, total);

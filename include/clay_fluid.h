@@ -448,6 +448,17 @@ int clay_batch_get_tuning(const clay_batch* b, clay_batch_tuning* t);
  * whose capacity is below upper[i] uses blocks[i] threads per block; larger scenes use the
  * batch's sph_block. upper[] increasing; blocks[] multiples of 32 in 64..256. */
 int clay_batch_set_bucket_blocks(clay_batch* b, const int64_t* upper, const int32_t* blocks, int n);
+/* The autotuner's full output, per scene-size bucket: bucket i < n holds the scenes whose
+ * capacity is below upper[i] (and not below upper[i-1]); bucket n the rest, so `t` has n + 1
+ * entries. Every choice gives the same results (reference mode bit for bit): they only move
+ * time between the passes' strategies. */
+typedef struct clay_bucket_tuning {
+  int32_t sph_block;          /* threads per block of the particle passes, 64..256, multiple of 32 */
+  int32_t density_two_phase;  /* 1: distance tests, then the accepted neighbours; 0: one loop */
+  int32_t splat_tile_ratio;   /* sphere blocks take the tile walk up to this many times their pairs (6) */
+  int32_t splat_walk_weight;  /* blocks take the block walk up to this many times their pairs (3) */
+} clay_bucket_tuning;
+int clay_batch_set_bucket_tuning(clay_batch* b, const int64_t* upper, const clay_bucket_tuning* t, int n);
 /* One frame for every scene: host bookkeeping of each sim (as clay_fluid_step), then the
  * batched passes (or the captured graph) on `stream`. */
 int clay_batch_step(clay_batch* b, void* stream);

@@ -1,5 +1,6 @@
-"""The autotuner picks a block size per scene-size bucket from real timed frames, leaves the
-scenes' state as it found it, and the tuned batch computes exactly what the untuned one does."""
+"""The autotuner picks its knobs per scene-size bucket from real timed frames, leaves the scenes'
+state as it found it, and the tuned batch computes exactly what the untuned one does; and every
+value of every knob gives the same frame as the defaults, in reference mode bit for bit."""
 import numpy as np
 import pytest
 
@@ -35,13 +36,16 @@ def test_tuning_restores_state_and_keeps_results(root):
     before = [s.download() for s in a]
     stream = torch.cuda.Stream()
     result, report = autotune.tune(root, a, stream=stream, frames=1, use_cache=False)
-    assert len(result["blocks"]) == len(autotune.BUCKETS)
-    assert all(x in autotune.CANDIDATES for x in result["blocks"])
-    assert len(report["trials"]) == len(autotune.CANDIDATES) * len({autotune.bucket_index(c) for c in counts})
+    assert len(result["tunings"]) == len(autotune.BUCKETS) + 1
+    for t in result["tunings"]:
+        assert all(t[k] in v for k, v in autotune.KNOBS.items())
+    n_buckets = len({autotune.bucket_index(c) for c in counts})
+    assert len(report["trials"]) == n_buckets * sum(len(v) - 1 for v in autotune.KNOBS.values())
+    assert result["default_ms"] > 0 and result["tuned_ms"] > 0
     for s, snap in zip(a, before):
         now = s.download()
         assert np.array_equal(now["pos"].view(np.uint32), snap["pos"].view(np.uint32))
-    tuned = ce.Batch(root, a, sph_block=result["default"])
+    tuned = ce.Batch(root, a, sph_block=result["tunings"][-1]["sph_block"])
     autotune.apply(tuned, result)
     plain = ce.Batch(root, b, sph_block=256)
     for _ in range(2):
@@ -55,3 +59,53 @@ def test_tuning_restores_state_and_keeps_results(root):
                                   np.ascontiguousarray(gy[name]).view(np.uint32)), name
     for o in [tuned, plain] + a + b:
         o.destroy()
+
+
+@pytest.mark.parametrize("knob", sorted(__import__("clay_engine_b200.autotune", fromlist=["KNOBS"]).KNOBS))
+def test_every_setting_is_bit_exact_in_reference_mode(root, knob):
+    """Each value of each knob, applied to every bucket, against the defaults: same particle
+    state and bake after two frames (a batch with spheres and a clay-body shell of discs)."""
+    import torch
+
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import autotune, scenes
+
+    counts = [1200, 5000, 20000, 70000]
+    stream = torch.cuda.Stream()
+
+    def run(setting):
+        sims = make(root, counts, 9)
+        for s in sims:
+            s.set_mode("reference")
+        pos, nrm = scenes.surface_net_sphere(0.95, 0.076, center=(1.0, 0.0, 0.0))
+        parts, body = scenes.body_records(pos, nrm, (1.0, 0.0, 0.0), capacity=4096)
+        dp = torch.from_numpy(parts.view(np.uint8)).cuda()
+        db = torch.from_numpy(body.view(np.uint8)).cuda()
+        shell = ce.SplatField(root, ce.bodyCloud(dp, db, 0), radius=0.095, resolution=32, band=4.0,
+                              worldSize=32 * 0.083)
+        shell.setCenter((1.0, 0.0, 0.0))
+        b = ce.Batch(root, sims, extra_splats=[shell])
+        tun = [dict(autotune.DEFAULT, **setting) for _ in range(len(autotune.BUCKETS) + 1)]
+        autotune.apply(b, {"uppers": list(autotune.BUCKETS), "tunings": tun})
+        for _ in range(2):
+            b.step(stream)
+        torch.cuda.synchronize()
+        out = [(s.download(), s.surface.volume.download()[0]) for s in sims] + [(None, shell.volume.download()[0])]
+        b.destroy()
+        for s in sims:
+            s.destroy()
+        shell.destroy()
+        return out
+
+    ref = run({})
+    for v in autotune.KNOBS[knob]:
+        if v == autotune.DEFAULT[knob]:
+            continue
+        got = run({knob: v})
+        for (ga, gd), (ra, rd) in zip(got, ref):
+            assert np.array_equal(gd, rd), f"{knob}={v}: bake differs"
+            if ga is None:
+                continue
+            for name in ("pos", "vel", "density", "pressure", "nvel"):
+                assert np.array_equal(np.ascontiguousarray(ga[name]).view(np.uint32),
+                                      np.ascontiguousarray(ra[name]).view(np.uint32)), f"{knob}={v}: {name}"

@@ -28,7 +28,9 @@ def test_autotune_buckets():
             self.capacity = c
 
     # scenes per bucket rounded up to a power of two
-    assert autotune.signature([S(1000)] * 3 + [S(5000)] * 5 + [S(70000)]) == "b4-8-0-1"
+    assert autotune.signature([S(1000)] * 3 + [S(5000)] * 5 + [S(70000)]) == "t4-8-0-1"
+    # every knob's default is one of its candidates
+    assert all(autotune.DEFAULT[k] in v for k, v in autotune.KNOBS.items())
 
 
 def test_estimate_counts_384_bytes_per_particle():
