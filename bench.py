@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--serve-pool", type=int, default=1024, help="resident scenes of the serving pool")
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-next", action="store_true", help="skip the measurements of the rows after the frame")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (every bucket at the defaults)")
     ap.add_argument("--workload", default="batched", choices=["batched", "tap"],
                     help="batched: the 256-scene batch (+plain, served); tap: one 262,144-particle scene fed by a tap")
     return ap.parse_args()
@@ -716,7 +717,13 @@ def main():
     from clay_engine_b200 import autotune
 
     t_tune = time.perf_counter()
-    tuned, tune_report = autotune.tune(root, sims, bodies, stream, frames=10, use_cache=False)
+    if args.no_tune:
+        n_b = len(autotune.BUCKETS) + 1
+        tuned = {"uppers": list(autotune.BUCKETS), "tunings": [dict(autotune.DEFAULT) for _ in range(n_b)],
+                 "changed": [], "gain": 0.0}
+        tune_report = {"trials": []}
+    else:
+        tuned, tune_report = autotune.tune(root, sims, bodies, stream, frames=10, use_cache=False)
     t_tune = time.perf_counter() - t_tune
     batch = ce.Batch(root, sims, extra_splats=bodies, use_graph=True, sph_block=tuned["tunings"][-1]["sph_block"])
     autotune.apply(batch, tuned)
