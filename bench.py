@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-next", action="store_true", help="skip the measurements of the rows after the frame")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (every bucket at the defaults)")
+    ap.add_argument("--set", action="append", default=[], metavar="KNOB=VALUE",
+                    help="with --no-tune: run every bucket at this setting of an autotuner knob instead of its default")
     ap.add_argument("--workload", default="batched", choices=["batched", "tap"],
                     help="batched: the 256-scene batch (+plain, served); tap: one 262,144-particle scene fed by a tap")
     return ap.parse_args()
@@ -719,8 +721,15 @@ def main():
     t_tune = time.perf_counter()
     if args.no_tune:
         n_b = len(autotune.BUCKETS) + 1
-        tuned = {"uppers": list(autotune.BUCKETS), "tunings": [dict(autotune.DEFAULT) for _ in range(n_b)],
-                 "changed": [], "gain": 0.0}
+        fixed = dict(autotune.DEFAULT)
+        for kv in args.set:
+            k, v = kv.split("=")
+            if k not in autotune.KNOBS:
+                raise SystemExit(f"--set: unknown knob {k}")
+            fixed[k] = int(v)
+        tuned = {"uppers": list(autotune.BUCKETS), "tunings": [dict(fixed) for _ in range(n_b)],
+                 "changed": [{k: v for k, v in fixed.items() if v != autotune.DEFAULT[k]}] if fixed != autotune.DEFAULT
+                 else [], "gain": 0.0}
         tune_report = {"trials": []}
     else:
         tuned, tune_report = autotune.tune(root, sims, bodies, stream, frames=10, use_cache=False)
@@ -782,6 +791,9 @@ def main():
     e2e_ms = D.reduce_max(e0.elapsed_time(e1))
     e2e_value = total_particles * e2e_steps / (e2e_ms / 1000)
 
+    # the clock sampler's window closed with the timed frames; stop its thread before the
+    # per-launch profile, whose event pairs would otherwise also time its NVML queries' stalls
+    clocks.__exit__(None, None, None)
     prof = batch.profile(stream)
     frame_ms = sum(v[0] for v in prof.values())
 
@@ -803,7 +815,6 @@ def main():
         plain_ms = D.reduce_max(p0.elapsed_time(p1))
         plain_value = total_particles * args.plain_steps / (plain_ms / 1000)
 
-    clocks.__exit__(None, None, None)
     clk = clocks.summary()
     # ---- census of the frame's algorithmic work (untimed): neighbour candidates and accepted
     # pairs of the last substep, the bake's in-band (particle, voxel) pairs, per scene

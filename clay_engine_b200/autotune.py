@@ -7,11 +7,14 @@ boxes a block's union box may be and still take the register-blocked tile walk, 
 walk). Every setting gives the same results (reference mode bit for bit); they only move time
 between code paths, so the choice is a pure timing decision.
 
-Search: coordinate descent, bucket after bucket and knob after knob (the others held at their
-current choice). Every value of a knob is timed over real batched frames (CUDA graph replays,
-CUDA events on the launching stream) from the same saved particle state, and a value replaces
-the current one only when it is faster by more than `min_gain` of the frame. The scenes' state
-is restored after tuning, so tuning does not advance the simulation. Results are cached per
+Search: coordinate descent, knob after knob, first for every bucket at once (a setting that
+differs between buckets splits a pass into one launch per distinct setting, which costs a
+little by itself, so a knob is first judged without that cost), then bucket after bucket. A
+candidate is timed over real batched frames (CUDA graph replays, CUDA events on the launching
+stream) from the same saved particle state, between two timings of the current choice, and
+replaces it only when it is faster than their mean by more than `min_gain` of the frame, so a
+slow drift of the GPU's speed over the search cannot pass for a gain. The scenes' state is
+restored after tuning, so tuning does not advance the simulation. Results are cached per
 bucket signature in a JSON file next to the library.
 """
 from __future__ import annotations
@@ -73,7 +76,7 @@ def _trial(root, sims, extra, snaps, choice, stream, frames):
     return ms
 
 
-def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=0.005):
+def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=0.004):
     """Returns ({"uppers": [...], "tunings": [per bucket dict], "gain": ...}, report)."""
     import torch
 
@@ -92,27 +95,38 @@ def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=
     choice = {i: dict(DEFAULT) for i in range(len(BUCKETS) + 1)}
     snaps = [s.download() for s in sims]
     report = {"signature": sig, "trials": []}
+
+    def timed(ch):
+        return _trial(root, sims, extra, snaps, ch, stream, frames)
+
+    def consider(buckets, knob, label):
+        nonlocal choice
+        for v in KNOBS[knob]:
+            if all(choice[b][knob] == v for b in buckets):
+                continue
+            cand = {i: dict(c) for i, c in choice.items()}
+            for b in buckets:
+                cand[b][knob] = v
+            before = timed(choice)
+            ms = timed(cand)
+            after = timed(choice)
+            cur = 0.5 * (before + after)
+            report["trials"].append({"bucket": label, knob: v, "ms": round(ms, 4), "current_ms": round(cur, 4)})
+            if ms < cur * (1.0 - min_gain):
+                choice = cand
+
     try:
-        base_ms = _trial(root, sims, extra, snaps, choice, stream, frames)
-        best_ms = base_ms
-        for bi in present:
-            for knob, values in KNOBS.items():
-                times = {choice[bi][knob]: best_ms}
-                for v in values:
-                    if v in times:
-                        continue
-                    cand = {i: dict(c) for i, c in choice.items()}
-                    cand[bi][knob] = v
-                    times[v] = _trial(root, sims, extra, snaps, cand, stream, frames)
-                    report["trials"].append({"bucket": bi, knob: v, "ms": round(times[v], 4)})
-                best_v = min(times, key=times.get)
-                if times[best_v] < best_ms * (1.0 - min_gain):
-                    choice[bi][knob] = best_v
-                    best_ms = times[best_v]
+        everyone = list(range(len(BUCKETS) + 1))
+        for knob in KNOBS:
+            consider(everyone, knob, "all")
+        if len(present) > 1:
+            for bi in present:
+                for knob in KNOBS:
+                    consider([bi], knob, bi)
         # the chosen settings against the defaults, timed again side by side
         default = {i: dict(DEFAULT) for i in range(len(BUCKETS) + 1)}
-        t_default = _trial(root, sims, extra, snaps, default, stream, frames)
-        t_tuned = _trial(root, sims, extra, snaps, choice, stream, frames)
+        t_default = timed(default)
+        t_tuned = timed(choice)
     finally:
         torch.cuda.synchronize()
         for s, snap in zip(sims, snaps):
@@ -120,7 +134,8 @@ def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=
     result = {"uppers": list(BUCKETS), "tunings": [choice[i] for i in range(len(BUCKETS) + 1)],
               "default_ms": t_default, "tuned_ms": t_tuned, "gain": t_default / t_tuned - 1.0,
               "changed": [{"bucket": i, **{k: v for k, v in choice[i].items() if v != DEFAULT[k]}}
-                          for i in present if choice[i] != DEFAULT]}
+                          for i in present if choice[i] != DEFAULT],
+              "buckets_present": present}
     if use_cache:
         cache[sig] = result
         os.makedirs(os.path.dirname(CACHE), exist_ok=True)

@@ -24,10 +24,14 @@ from oracle.fluid_frame import OracleFluid
 pytestmark = pytest.mark.gpu
 
 THREADS = os.cpu_count() or 8
-# The fast-mode bounds of the small-configuration test: relative to the field's largest
-# magnitude; pressure = stiffness * (rho - rho0) cancels, so it has its own bound.
+# Fast-mode bounds, relative to the field's largest magnitude: positions and densities 2e-5
+# (the small-configuration test's bound); pressure = stiffness * (rho - rho0) cancels, so it
+# has its own bound, 2e-4; velocities 1e-4, between the two: in a pile at rest under gravity
+# a substep's velocity change is mostly the pressure force, which carries the pressure's
+# relative error, while the velocity itself is small.
 FAST_REL_TOL = 2e-5
 FAST_REL_TOL_PRESSURE = 2e-4
+FAST_REL_TOL_VELOCITY = 1e-4
 FIELDS = ("pos", "vel", "nvel", "density", "pressure")
 
 
@@ -64,7 +68,8 @@ def rel_errors(g, r, n):
 
 def assert_within_fast_tolerance(errs, what):
     for name, err in errs.items():
-        tol = FAST_REL_TOL_PRESSURE if name == "pressure" else FAST_REL_TOL
+        tol = {"pressure": FAST_REL_TOL_PRESSURE, "vel": FAST_REL_TOL_VELOCITY,
+               "nvel": FAST_REL_TOL_VELOCITY}.get(name, FAST_REL_TOL)
         assert err <= tol, f"{what}{name}: rel err {err:.3g} > {tol:g}"
 
 
