@@ -33,7 +33,7 @@ KNOBS = {
     "splat_tile_ratio": (3, 6, 12),
     "splat_walk_weight": (2, 3, 6),
 }
-DEFAULT = {"sph_block": 256, "density_two_phase": 1, "splat_tile_ratio": 6, "splat_walk_weight": 3}
+DEFAULT = {"sph_block": 256, "density_two_phase": 0, "splat_tile_ratio": 6, "splat_walk_weight": 3}
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "autotune.json")
 
 

@@ -1732,10 +1732,22 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
     cudaEvent_t a, z;
   };
   std::vector<Rec> recs;
+  // every event is created before the frame: creating them between launches would leave the
+  // device idle between an event and its kernel, and the idle time would count as the kernel's
+  struct EventPool {
+    std::vector<cudaEvent_t> ev;
+    ~EventPool() {
+      for (cudaEvent_t e : ev)
+        if (e) cudaEventDestroy(e);
+    }
+  } pool;
+  pool.ev.assign(2 * 64 * static_cast<size_t>(std::max(1, b->max_substeps) + 1), nullptr);
+  size_t next_ev = 0;
+  for (auto& e : pool.ev) CK(cudaEventCreate(&e));
   auto timed = [&](const char* name, auto&& launch) -> int {
-    Rec r{name, nullptr, nullptr};
-    CK(cudaEventCreate(&r.a));
-    CK(cudaEventCreate(&r.z));
+    if (next_ev + 2 > pool.ev.size()) return fail(CLAY_ESTATE, "clay_batch_profile: too many launches");
+    Rec r{name, pool.ev[next_ev], pool.ev[next_ev + 1]};
+    next_ev += 2;
     CK(cudaEventRecord(r.a, s));
     CK(launch());
     CK(cudaEventRecord(r.z, s));
@@ -1794,8 +1806,6 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
   for (auto& r : recs) {
     float ms = 0;
     cudaEventElapsedTime(&ms, r.a, r.z);
-    cudaEventDestroy(r.a);
-    cudaEventDestroy(r.z);
     bool found = false;
     for (auto& a : agg)
       if (std::strcmp(a.name, r.name) == 0) {

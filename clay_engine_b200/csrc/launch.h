@@ -21,7 +21,7 @@ void count_launches(uint64_t n);  // kernels replayed by a graph launch
 // Threads per block of the particle passes when no tuning overrides it.
 constexpr int kBlock = 256;
 // The density variant used when no tuning overrides it.
-constexpr bool kDensityTwoPhase = true;
+constexpr bool kDensityTwoPhase = false;
 
 cudaError_t L_emit(const SceneDev* s, const Work* w, int blocks, int threads, cudaStream_t st);
 cudaError_t L_cell_key(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
