@@ -1127,6 +1127,18 @@ __device__ __forceinline__ uint32_t enc_key(float sd, float bw) {
   return static_cast<uint32_t>((v + 1.0f) * 32767.5f);
 }
 
+// A disc's distance max(plane, sqrt(len2) - radius) (splat.ts:177-184) with the square root
+// taken only where it can decide the maximum. With u = plane + radius > 0 and len2 below
+// u * u * 0.99999f (all rounded), sqrt(len2) is below u * (1 - 4.8e-6) even after its own
+// rounding, and u exceeds plane + radius by at most one rounding, so sqrt(len2) - radius is
+// below plane before and after rounding: the maximum is the plane term, exactly what the
+// full expression gives.
+__device__ __forceinline__ float disc_sd(float pl, float len2, float radius) {
+  const float u = pl + radius;
+  if (u > 0.0f && len2 < (u * u) * 0.99999f) return pl;
+  return fmaxf(pl, __fsqrt_rn(len2) - radius);
+}
+
 __device__ __forceinline__ bool cloud_live(const SplatDev& D, uint32_t idx, uint32_t& i) {
   if (D.order) {
     uint32_t n = min(*D.live_count, D.capacity);
@@ -1595,7 +1607,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
                 t = t + dy2;
                 t = t + dz2;
                 const float thr = b[k] + radius;
-                if (thr > 0.0f && t < thr * thr * 1.00001f) b[k] = fminf(b[k], fmaxf(pl, __fsqrt_rn(t) - radius));
+                if (thr > 0.0f && t < thr * thr * 1.00001f) b[k] = fminf(b[k], disc_sd(pl, t, radius));
               }
             }
           }
@@ -1724,7 +1736,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
             if (pl < best) {
               float t = (dx * dx + dy * dy) + dz * dz;
               const float thr = best + radius;
-              if (thr > 0.0f && t < thr * thr * 1.00001f) best = fminf(best, fmaxf(pl, __fsqrt_rn(t) - radius));
+              if (thr > 0.0f && t < thr * thr * 1.00001f) best = fminf(best, disc_sd(pl, t, radius));
             }
           }
         }
@@ -1748,7 +1760,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
           if (pl >= bw) return;
           float t = (dx * dx + dy * dy) + dz * dz;
           if (t >= reach2_hi) return;
-          float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
+          float sd = has_n ? disc_sd(pl, t, radius) : __fsqrt_rn(t) - radius;
           if (sd < bw) emit(x, y, z, sd);
         };
         if (use_st) {
@@ -1782,19 +1794,32 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
           const uint32_t vz = __ballot_sync(0xffffffffu, in_box);
           __syncwarp();
           const uint32_t ns = s_nst;
+          // A stencil wholly inside the volume needs no box test: a voxel outside the
+          // particle's box is at least half a voxel beyond its reach, which the length test
+          // below rejects. Only where the volume clips the box does the box decide.
+          const bool inside = cxv - sn >= 0 && cxv + sn <= last && cyv - sn >= 0 && cyv + sn <= last &&
+                              czv - sn >= 0 && czv + sn <= last;
+          // the voxel of stencil field (ex, ey, ez) as a linear index: in the shared minimum
+          // tile when the block's union box fits it, else in the level's key grid
+          const int asy = sy * static_cast<int>(anx), asz = sz * static_cast<int>(anx * any);
+          const int abase = (cxv - ax0) + static_cast<int>(anx) * ((cyv - ay0) + static_cast<int>(any) * (czv - az0));
+          const int gsy = sy * R, gsz = sz * R * R;
+          const long long gbase = static_cast<long long>(cxv) + static_cast<long long>(R) * (cyv + static_cast<long long>(R) * czv);
           for (uint32_t v = lane; v < ns; v += 32) {
             const uint32_t e = s_st[v];
             const uint32_t ex = e & 15u, ey = (e >> 4) & 15u, ez = (e >> 8) & 15u;
-            if (!((vxy >> ex) & (vxy >> (16u + ey)) & (vz >> ez) & 1u)) continue;
+            if (!inside && !((vxy >> ex) & (vxy >> (16u + ey)) & (vz >> ez) & 1u)) continue;
             const float2 tx = s_dt[wid][0][ex], ty = s_dt[wid][1][ey], tz = s_dt[wid][2][ez];
             const float pl = has_n ? (tx.x + ty.x) + tz.x : -__int_as_float(0x7f800000);
             if (pl >= bw) continue;
             const float t = (tx.y + ty.y) + tz.y;
             if (t >= reach2_hi) continue;
-            const float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
-            if (sd < bw)
-              emit(cxv + sx * (static_cast<int>(ex) - 8), cyv + sy * (static_cast<int>(ey) - 8),
-                   czv + sz * (static_cast<int>(ez) - 8), sd);
+            const float sd = has_n ? disc_sd(pl, t, radius) : __fsqrt_rn(t) - radius;
+            if (sd < bw) {
+              const int rx = static_cast<int>(ex) - 8, ry = static_cast<int>(ey) - 8, rz = static_cast<int>(ez) - 8;
+              if (use_acc) atomicMin(&s_acc[abase + sx * rx + asy * ry + asz * rz], sd_bits(sd));
+              else atomicMin(keys + (gbase + (sx * rx + gsy * ry + gsz * rz)), sd_bits(sd));
+            }
           }
           __syncwarp();  // the tables are rewritten for the next particle
           continue;
