@@ -67,7 +67,7 @@ class CloudDesc(C.Structure):
 
 
 class BucketTuning(C.Structure):
-    _fields_ = [("sph_block", C.c_int32), ("density_two_phase", C.c_int32), ("splat_tile_ratio", C.c_int32),
+    _fields_ = [("sph_block", C.c_int32), ("density_variant", C.c_int32), ("splat_tile_ratio", C.c_int32),
                 ("splat_walk_weight", C.c_int32)]
 
 

@@ -29,11 +29,11 @@ from .core import Batch
 BUCKETS = (4096, 16384, 65536)       # capacity < 4k, < 16k, < 64k, and the rest
 KNOBS = {
     "sph_block": (64, 128, 192, 256),
-    "density_two_phase": (0, 1),
+    "density_variant": (0, 1, 2),
     "splat_tile_ratio": (3, 6, 12),
     "splat_walk_weight": (2, 3, 6),
 }
-DEFAULT = {"sph_block": 256, "density_two_phase": 0, "splat_tile_ratio": 6, "splat_walk_weight": 3}
+DEFAULT = {"sph_block": 256, "density_variant": 0, "splat_tile_ratio": 6, "splat_walk_weight": 3}
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "autotune.json")
 
 

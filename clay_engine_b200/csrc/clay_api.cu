@@ -1367,7 +1367,7 @@ struct clay_batch {
     Work* w;
     int n;
     int T;
-    bool two_phase;
+    int density_variant;
   };
   std::vector<PartGroup> groups;
   int bucket_of(int64_t capacity) const {
@@ -1384,7 +1384,7 @@ struct clay_batch {
     if (i < bucket_tune.size()) return bucket_tune[i];
     clay_bucket_tuning t{};
     t.sph_block = block_of(capacity);
-    t.density_two_phase = kDensityTwoPhase ? 1 : 0;
+    t.density_variant = kDensityVariant;
     t.splat_tile_ratio = static_cast<int32_t>(kSplatTileRatio);
     t.splat_walk_weight = static_cast<int32_t>(kSplatWalkWeight);
     return t;
@@ -1409,8 +1409,16 @@ struct clay_batch {
   Work* d_sub = nullptr;
   size_t d_sub_cap = 0;
 
+  // A second stream for the extra clouds' bake, forked from the frame's stream and joined
+  // before the first forces pass (the first reader of the bodies' volumes): the bodies bake
+  // while the fluids build their cells and densities.
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   ~clay_batch() {
     release();
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
     for (int k = 0; k < 2; k++) {
       if (h_params[k]) cudaFreeHost(h_params[k]);
       if (params_ev[k]) cudaEventDestroy(params_ev[k]);
@@ -1466,7 +1474,7 @@ int batch_build(clay_batch* b) {
   std::vector<Work> wp, we, wsc;
   b->max_substeps = 0;
   // one group of particle-pass launches per distinct (block size, density variant)
-  std::vector<std::pair<int, bool>> blocks;
+  std::vector<std::pair<int, int>> blocks;
   std::vector<std::vector<Work>> by_block;
   for (size_t i = 0; i < b->sims.size(); i++) {
     clay_fluid* f = b->sims[i];
@@ -1475,7 +1483,7 @@ int batch_build(clay_batch* b) {
     uint32_t obj = static_cast<uint32_t>(i);
     const clay_bucket_tuning bt = b->tuning_of(f->capacity);
     const int Ts = bt.sph_block;
-    const std::pair<int, bool> key(Ts, bt.density_two_phase != 0);
+    const std::pair<int, int> key(Ts, bt.density_variant);
     size_t gi = std::find(blocks.begin(), blocks.end(), key) - blocks.begin();
     if (gi == blocks.size()) {
       blocks.push_back(key);
@@ -1542,6 +1550,9 @@ int batch_build(clay_batch* b) {
   b->n_xres = static_cast<int>(wxr.size());
   b->n_ssplat = static_cast<int>(wss.size());
   b->n_sres = static_cast<int>(wsr.size());
+  if (!b->side) CK(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+  if (!b->ev_fork) CK(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+  if (!b->ev_join) CK(cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
   b->built = true;
   return CLAY_OK;
 }
@@ -1551,8 +1562,19 @@ int batch_build(clay_batch* b) {
 int batch_enqueue(clay_batch* b, cudaStream_t s) {
   const int T = b->tune.sph_block;
   const SceneDev* d = b->d_scenes;
-  if (b->n_xsplat) CK(L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, kSplatAccVoxelsDiscs, s));
-  if (b->n_xres) CK(L_resolve(b->d_extra, b->w_xres, b->n_xres, s));
+  // the extra clouds' bake: on the side stream when there are fluids to overlap it with
+  const bool fork = b->n_xsplat && b->n_part && b->max_substeps > 0;
+  bool joined = !fork;
+  if (fork) {  // the stream and events exist from batch_build on (never created inside a capture)
+    CK(cudaEventRecord(b->ev_fork, s));
+    CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+    CK(L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, kSplatAccVoxelsDiscs, b->side));
+    if (b->n_xres) CK(L_resolve(b->d_extra, b->w_xres, b->n_xres, b->side));
+    CK(cudaEventRecord(b->ev_join, b->side));
+  } else {
+    if (b->n_xsplat) CK(L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, kSplatAccVoxelsDiscs, s));
+    if (b->n_xres) CK(L_resolve(b->d_extra, b->w_xres, b->n_xres, s));
+  }
   if (b->n_part) {
     CK(L_emit(d, b->w_emit, b->n_emit, T, s));
     for (int sub = 0; sub < b->max_substeps; sub++) {
@@ -1563,8 +1585,12 @@ int batch_enqueue(clay_batch* b, cudaStream_t s) {
       for (auto& g : b->groups) CK(L_cell_scatter(d, g.w, g.n, g.T, sub, s));
       for (auto& g : b->groups) CK(L_cell_order(d, g.w, g.n, g.T, sub, s));
       for (auto& g : b->groups) {
-        if (b->mode == CLAY_MODE_REFERENCE) CK(L_density_ref(d, g.w, g.n, g.T, sub, s, g.two_phase));
-        else CK(L_density_fast(d, g.w, g.n, g.T, sub, s, g.two_phase));
+        if (b->mode == CLAY_MODE_REFERENCE) CK(L_density_ref(d, g.w, g.n, g.T, sub, s, g.density_variant));
+        else CK(L_density_fast(d, g.w, g.n, g.T, sub, s, g.density_variant));
+      }
+      if (!joined) {  // the fluids collide with the bodies' volumes from here on
+        CK(cudaStreamWaitEvent(s, b->ev_join, 0));
+        joined = true;
       }
       for (auto& g : b->groups) {
         if (b->mode == CLAY_MODE_REFERENCE) CK(L_forces_ref(d, g.w, g.n, g.T, sub, s));
@@ -1572,6 +1598,7 @@ int batch_enqueue(clay_batch* b, cudaStream_t s) {
       }
     }
   }
+  if (!joined) CK(cudaStreamWaitEvent(s, b->ev_join, 0));
   if (b->n_ssplat) CK(L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, kSplatAccVoxels, s));
   if (b->n_sres) CK(L_resolve(b->d_surf, b->w_sres, b->n_sres, s));
   return CLAY_OK;
@@ -1642,6 +1669,8 @@ int clay_batch_set_bucket_tuning(clay_batch* b, const int64_t* upper, const clay
   for (int i = 0; i <= n; i++) {
     if (t[i].sph_block < 64 || t[i].sph_block > 256 || (t[i].sph_block & 31))
       return fail(CLAY_EINVAL, "bucket block %d must be a multiple of 32 in 64..256", t[i].sph_block);
+    if (t[i].density_variant < 0 || t[i].density_variant > 2)
+      return fail(CLAY_EINVAL, "bucket density variant %d is not 0, 1 or 2", t[i].density_variant);
     if (t[i].splat_tile_ratio < 1 || t[i].splat_tile_ratio > 64 || t[i].splat_walk_weight < 1 || t[i].splat_walk_weight > 64)
       return fail(CLAY_EINVAL, "bucket splat thresholds must be in 1..64");
     if (i > 0 && i < n && upper[i] <= upper[i - 1]) return fail(CLAY_EINVAL, "bucket bounds must increase");
@@ -1788,8 +1817,8 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
         if ((rc = timed("cell_order", [&] { return L_cell_order(d, g.w, g.n, g.T, sub, s); }))) return rc;
       for (auto& g : b->groups)
         if ((rc = timed("density", [&] {
-               return ref ? L_density_ref(d, g.w, g.n, g.T, sub, s, g.two_phase)
-                          : L_density_fast(d, g.w, g.n, g.T, sub, s, g.two_phase);
+               return ref ? L_density_ref(d, g.w, g.n, g.T, sub, s, g.density_variant)
+                          : L_density_fast(d, g.w, g.n, g.T, sub, s, g.density_variant);
              })))
           return rc;
       for (auto& g : b->groups)

@@ -860,36 +860,112 @@ __device__ __forceinline__ void for_neighbour_ranges(const SceneDev& S, const Bo
       uint32_t row = b.bx * (static_cast<uint32_t>(y - b.y0) + b.by * static_cast<uint32_t>(z - b.z0));
       uint32_t l0 = row + static_cast<uint32_t>(xl - b.x0);
       uint32_t l1 = row + static_cast<uint32_t>(xh - b.x0);
+      const int r = (dz + 1) * 3 + (dy + 1);
       if (!overflow) {
-        f(__ldg(S.cell_start + l0), __ldg(S.cell_start + l1 + 1));
+        f(__ldg(S.cell_start + l0), __ldg(S.cell_start + l1 + 1), r);
       } else {
         for (uint32_t l = l0; l <= l1; l++) {
           uint32_t s = __ldg(S.cell_start + l), e = __ldg(S.cell_start + l + 1);
-          f(s, s + min(e - s, S.bucket));
+          f(s, s + min(e - s, S.bucket), r);
         }
       }
     }
   }
 }
 
+// The local cell index (the cell build's order key) of a position: L, the out-of-grid bucket,
+// outside the grid (fluid.ts:318-322), else its place in the box of occupied cells.
+__device__ __forceinline__ uint32_t local_cell(const SceneDev& S, const BoxInfo& b, float4 p) {
+  int cx, cy, cz;
+  cell_of(S, p.x, p.y, p.z, cx, cy, cz);
+  if (cx < 0 || cy < 0 || cz < 0 || cx >= S.G || cy >= S.G || cz >= S.G) return b.L;
+  return static_cast<uint32_t>(cx - b.x0) + b.bx * (static_cast<uint32_t>(cy - b.y0) + b.by * static_cast<uint32_t>(cz - b.z0));
+}
+
+constexpr int kDensityStage = 3040;  // staged neighbour positions per block (47.5 KB, under the 48 KB static limit)
+
 // density (fluid.ts:333-368). kFast accumulates with Kahan compensation.
 //
-// kTwoPhase takes the candidates of a range 32 at a time in two phases: the distance test of
-// every candidate, which leaves a bit mask of the accepted ones, then the accepted ones alone,
-// in ascending order (the reference's visiting order), each re-read from cache. A warp's lanes
-// accept at different candidates, so running the accept work inside the test loop (the other
-// variant) keeps most lanes idle through it; in the second phase every lane with a pending
-// neighbour works. Both variants visit, sum and list the neighbours in the same order.
-template <bool kFast, bool kTwoPhase>
+// Three variants, which visit, sum and list the neighbours in the same order:
+//  - kVariant 0: one loop, the accept work inside the distance-test loop;
+//  - kVariant 1: the candidates of a range 32 at a time in two phases: the distance test of
+//    every candidate, which leaves a bit mask of the accepted ones, then the accepted ones
+//    alone, in ascending order (the reference's visiting order), each re-read from cache. A
+//    warp's lanes accept at different candidates, so running the accept work inside the test
+//    loop keeps most lanes idle through it; in the second phase every lane with a pending
+//    neighbour works;
+//  - kVariant 2: variant 0 reading the candidates from shared memory. The block's particles
+//    are consecutive in the cell order, so their cells span a run [l0, l1] of local cell
+//    indices, and the neighbour row (dz, dy) of any of them lies in the cells
+//    [l0 + off - 1, l1 + off + 1], off = bx * (dy + by * dz): nine ranges of the cell-ordered
+//    positions, copied into shared memory once per block when they fit (else the block reads
+//    through the cache as variant 0 does).
+template <bool kFast, int kVariant>
 __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
   if (substep >= S.substeps) return;
   uint32_t count = work_count(S);
   uint32_t k = w.first + threadIdx.x;
-  if (k >= count || threadIdx.x >= w.n) return;
   const BoxInfo b = box_from_state(S.gs);
   const bool overflow = S.gs->overflow != 0u;
+  [[maybe_unused]] float4* s_pos = nullptr;
+  [[maybe_unused]] uint32_t* s_q0 = nullptr;  // first staged particle of each row range
+  [[maybe_unused]] uint32_t* s_sb = nullptr;  // its place in s_pos
+  [[maybe_unused]] bool staged = false;
+  if constexpr (kVariant == 2) {
+    __shared__ float4 st_pos[kDensityStage];
+    __shared__ uint32_t st_q0[9], st_sb[9], st_n[9];
+    __shared__ int st_ok;
+    s_pos = st_pos;
+    s_q0 = st_q0;
+    s_sb = st_sb;
+    const uint32_t last = min(count, w.first + w.n);  // one past the block's last particle
+    if (w.first >= last) return;  // the whole block is past the live count
+    if (threadIdx.x < 32) {
+      const uint32_t lane = threadIdx.x;
+      uint32_t n = 0, q0 = 0;
+      // a particle outside the grid (sorted last, local cell L) still reads the grid's edge
+      // rows around its clamped cell, which the ranges below do not cover: such a block reads
+      // through the cache
+      const uint32_t l1u = b.L > 0 ? local_cell(S, b, S.spos[last - 1]) : 0u;
+      const bool fits = b.L > 0 && l1u < b.L;
+      if (lane < 9 && fits) {
+        const int l0 = static_cast<int>(local_cell(S, b, S.spos[w.first]));
+        const int l1 = static_cast<int>(l1u);
+        const int dz = static_cast<int>(lane) / 3 - 1, dy = static_cast<int>(lane) % 3 - 1;
+        const int off = static_cast<int>(b.bx) * (dy + static_cast<int>(b.by) * dz);
+        const int lo = max(l0 + off - 1, 0), hi = min(l1 + off + 1, static_cast<int>(b.L) - 1);
+        if (lo <= hi) {
+          q0 = S.cell_start[lo];
+          n = S.cell_start[hi + 1] - q0;
+        }
+      }
+      uint32_t incl = n;
+#pragma unroll
+      for (int o = 1; o < 16; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= static_cast<uint32_t>(o)) incl += y;
+      }
+      if (lane < 9) {
+        st_q0[lane] = q0;
+        st_sb[lane] = incl - n;
+        st_n[lane] = n;
+      }
+      const uint32_t total = __shfl_sync(0xffffffffu, incl, 8);
+      if (lane == 0) st_ok = fits && total <= static_cast<uint32_t>(kDensityStage);
+    }
+    __syncthreads();
+    staged = st_ok != 0;
+    if (staged) {
+      for (int r = 0; r < 9; r++) {
+        const uint32_t n = st_n[r], q0 = st_q0[r], sb = st_sb[r];
+        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) st_pos[sb + i] = __ldg(S.spos + q0 + i);
+      }
+      __syncthreads();
+    }
+  }
+  if (k >= count || threadIdx.x >= w.n) return;
   const float4 me = S.spos[k];
   int cx, cy, cz;
   cell_of(S, me.x, me.y, me.z, cx, cy, cz);
@@ -921,14 +997,26 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
       rho = rho + term;
     }
   };
-  if (!kTwoPhase) {
+  if constexpr (kVariant == 0) {
     for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
       const float4 o = __ldg(spos + q);
       const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
       const float r2 = (dx * dx + dy * dy) + dz * dz;
       if (r2 < h2) accept(q, r2);
     });
-  } else for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e) {
+  } else if constexpr (kVariant == 2) {
+    for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int r) {
+      // the row's candidates [s, e) lie inside staged range r (see above): candidate q sits
+      // at s_pos[q - q0 + sb], computed modulo 2^32 as q + shift
+      const uint32_t shift = staged ? s_sb[r] - s_q0[r] : 0u;
+      for (uint32_t q = s; q < e; q++) {
+        const float4 o = staged ? s_pos[q + shift] : __ldg(spos + q);
+        const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+        const float r2 = (dx * dx + dy * dy) + dz * dz;
+        if (r2 < h2) accept(q, r2);
+      }
+    });
+  } else for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int) {
     for (uint32_t base = s; base < e; base += 32u) {
       const uint32_t n = min(32u, e - base);
       uint32_t m = 0;
@@ -1125,18 +1213,6 @@ __device__ __forceinline__ float bits_sd(uint32_t u) { return __uint_as_float((u
 __device__ __forceinline__ uint32_t enc_key(float sd, float bw) {
   float v = clampf(__fdiv_rn(sd, bw), -1.0f, 1.0f);
   return static_cast<uint32_t>((v + 1.0f) * 32767.5f);
-}
-
-// A disc's distance max(plane, sqrt(len2) - radius) (splat.ts:177-184) with the square root
-// taken only where it can decide the maximum. With u = plane + radius > 0 and len2 below
-// u * u * 0.99999f (all rounded), sqrt(len2) is below u * (1 - 4.8e-6) even after its own
-// rounding, and u exceeds plane + radius by at most one rounding, so sqrt(len2) - radius is
-// below plane before and after rounding: the maximum is the plane term, exactly what the
-// full expression gives.
-__device__ __forceinline__ float disc_sd(float pl, float len2, float radius) {
-  const float u = pl + radius;
-  if (u > 0.0f && len2 < (u * u) * 0.99999f) return pl;
-  return fmaxf(pl, __fsqrt_rn(len2) - radius);
 }
 
 __device__ __forceinline__ bool cloud_live(const SplatDev& D, uint32_t idx, uint32_t& i) {
@@ -1607,7 +1683,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
                 t = t + dy2;
                 t = t + dz2;
                 const float thr = b[k] + radius;
-                if (thr > 0.0f && t < thr * thr * 1.00001f) b[k] = fminf(b[k], disc_sd(pl, t, radius));
+                if (thr > 0.0f && t < thr * thr * 1.00001f) b[k] = fminf(b[k], fmaxf(pl, __fsqrt_rn(t) - radius));
               }
             }
           }
@@ -1736,7 +1812,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
             if (pl < best) {
               float t = (dx * dx + dy * dy) + dz * dz;
               const float thr = best + radius;
-              if (thr > 0.0f && t < thr * thr * 1.00001f) best = fminf(best, disc_sd(pl, t, radius));
+              if (thr > 0.0f && t < thr * thr * 1.00001f) best = fminf(best, fmaxf(pl, __fsqrt_rn(t) - radius));
             }
           }
         }
@@ -1760,7 +1836,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
           if (pl >= bw) return;
           float t = (dx * dx + dy * dy) + dz * dz;
           if (t >= reach2_hi) return;
-          float sd = has_n ? disc_sd(pl, t, radius) : __fsqrt_rn(t) - radius;
+          float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
           if (sd < bw) emit(x, y, z, sd);
         };
         if (use_st) {
@@ -1814,7 +1890,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
             if (pl >= bw) continue;
             const float t = (tx.y + ty.y) + tz.y;
             if (t >= reach2_hi) continue;
-            const float sd = has_n ? disc_sd(pl, t, radius) : __fsqrt_rn(t) - radius;
+            const float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
             if (sd < bw) {
               const int rx = static_cast<int>(ex) - 8, ry = static_cast<int>(ey) - 8, rz = static_cast<int>(ez) - 8;
               if (use_acc) atomicMin(&s_acc[abase + sx * rx + asy * ry + asz * rz], sd_bits(sd));

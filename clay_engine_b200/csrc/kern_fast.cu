@@ -7,9 +7,10 @@
 namespace clay {
 
 cudaError_t L_density_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
-                           bool two_phase) {
-  if (two_phase) k_density<true, true><<<blocks, threads, 0, st>>>(s, w, sub);
-  else k_density<true, false><<<blocks, threads, 0, st>>>(s, w, sub);
+                           int variant) {
+  if (variant == 1) k_density<true, 1><<<blocks, threads, 0, st>>>(s, w, sub);
+  else if (variant == 2) k_density<true, 2><<<blocks, threads, 0, st>>>(s, w, sub);
+  else k_density<true, 0><<<blocks, threads, 0, st>>>(s, w, sub);
   count_launch();
   return cudaPeekAtLastError();
 }

@@ -45,9 +45,10 @@ cudaError_t L_cell_order(const SceneDev* s, const Work* w, int blocks, int threa
   CLAY_LAUNCH(k_cell_order, blocks, threads, st, s, w, sub);
 }
 cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
-                          bool two_phase) {
-  if (two_phase) k_density<false, true><<<blocks, threads, 0, st>>>(s, w, sub);
-  else k_density<false, false><<<blocks, threads, 0, st>>>(s, w, sub);
+                          int variant) {
+  if (variant == 1) k_density<false, 1><<<blocks, threads, 0, st>>>(s, w, sub);
+  else if (variant == 2) k_density<false, 2><<<blocks, threads, 0, st>>>(s, w, sub);
+  else k_density<false, 0><<<blocks, threads, 0, st>>>(s, w, sub);
   count_launch();
   return cudaPeekAtLastError();
 }

@@ -20,8 +20,9 @@ void count_launches(uint64_t n);  // kernels replayed by a graph launch
 
 // Threads per block of the particle passes when no tuning overrides it.
 constexpr int kBlock = 256;
-// The density variant used when no tuning overrides it.
-constexpr bool kDensityTwoPhase = false;
+// The density variant used when no tuning overrides it (0: one loop, 1: two phases, 2: one
+// loop over neighbour positions staged in shared memory).
+constexpr int kDensityVariant = 0;
 
 cudaError_t L_emit(const SceneDev* s, const Work* w, int blocks, int threads, cudaStream_t st);
 cudaError_t L_cell_key(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
@@ -31,12 +32,12 @@ cudaError_t L_scan_final(const SceneDev* s, const Work* w, int blocks, int sub, 
 cudaError_t L_cell_scatter(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
 cudaError_t L_cell_order(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
 // Reference mode (kern_ref.cu) and fast mode (kern_fast.cu) of the neighbour passes.
-// `two_phase` selects the density variant (both give the same visiting order).
+// `variant` selects the density variant (all give the same visiting order).
 cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
-                          bool two_phase = kDensityTwoPhase);
+                          int variant = kDensityVariant);
 cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
 cudaError_t L_density_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
-                           bool two_phase = kDensityTwoPhase);
+                           int variant = kDensityVariant);
 cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
 // `blocks_y` = mip levels when w == nullptr.
 // acc_voxels: size of the shared-memory minimum tile (dynamic shared memory, 4 B per voxel).

@@ -454,7 +454,8 @@ int clay_batch_set_bucket_blocks(clay_batch* b, const int64_t* upper, const int3
  * time between the passes' strategies. */
 typedef struct clay_bucket_tuning {
   int32_t sph_block;          /* threads per block of the particle passes, 64..256, multiple of 32 */
-  int32_t density_two_phase;  /* 1: distance tests, then the accepted neighbours; 0: one loop (default) */
+  int32_t density_variant;    /* 0: one loop (default); 1: distance tests, then the accepted
+                                  neighbours; 2: one loop over neighbours staged in shared memory */
   int32_t splat_tile_ratio;   /* sphere blocks take the tile walk up to this many times their pairs (6) */
   int32_t splat_walk_weight;  /* blocks take the block walk up to this many times their pairs (3) */
 } clay_bucket_tuning;
