@@ -724,10 +724,11 @@ def main():
         fixed = dict(autotune.DEFAULT)
         for kv in args.set:
             k, v = kv.split("=")
-            if k not in autotune.KNOBS:
+            if k not in autotune.KNOBS and k != "lanes":
                 raise SystemExit(f"--set: unknown knob {k}")
             fixed[k] = int(v)
-        tuned = {"uppers": list(autotune.BUCKETS), "tunings": [dict(fixed) for _ in range(n_b)],
+        lanes = int(fixed.pop("lanes", autotune.DEFAULT_LANES))
+        tuned = {"uppers": list(autotune.BUCKETS), "tunings": [dict(fixed) for _ in range(n_b)], "lanes": lanes,
                  "changed": [{k: v for k, v in fixed.items() if v != autotune.DEFAULT[k]}] if fixed != autotune.DEFAULT
                  else [], "gain": 0.0}
         tune_report = {"trials": []}
@@ -956,7 +957,7 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
             "roofline": roof,
-            "autotune": {"changed": tuned["changed"], "gain": r3(tuned["gain"]),
+            "autotune": {"changed": tuned["changed"], "lanes": tuned.get("lanes", 1), "gain": r3(tuned["gain"]),
                          "trials": len(tune_report.get("trials", []))},
             "configs": cfgs,
             "plain": {"value": plain_value, "ratio_batched_over_plain": (value / plain_value) if plain_value else None},

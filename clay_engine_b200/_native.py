@@ -211,6 +211,7 @@ SIGNATURES = {
     "clay_batch_get_tuning": (I, [P, C.POINTER(BatchTuning)]),
     "clay_batch_set_bucket_blocks": (I, [P, P, P, I]),
     "clay_batch_set_bucket_tuning": (I, [P, P, P, I]),
+    "clay_batch_set_lanes": (I, [P, I]),
     "clay_batch_step": (I, [P, P]),
     "clay_batch_step_subset": (I, [P, P, I, P]),
     "clay_batch_read_contacts_async": (I, [P, P, P]),

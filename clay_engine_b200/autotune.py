@@ -1,10 +1,11 @@
 """Autotuner: picks, per scene-size bucket, the launch shapes and strategies of the frame.
 
 Scenes are grouped by capacity into buckets. The knobs of a bucket are the thread-block size of
-the particle passes, the density pass's variant (one loop, or distance tests then the accepted
-neighbours) and the splat's strategy thresholds (how much larger than the particles' own voxel
+the particle passes, the density pass's variant (one loop; distance tests then the accepted
+neighbours; one loop over neighbours staged in shared memory) and the splat's strategy thresholds (how much larger than the particles' own voxel
 boxes a block's union box may be and still take the register-blocked tile walk, or the block
-walk). Every setting gives the same results (reference mode bit for bit); they only move time
+walk); the batch as a whole also picks how many lanes (groups of scenes whose chains of
+launches run side by side) it steps. Every setting gives the same results (reference mode bit for bit); they only move time
 between code paths, so the choice is a pure timing decision.
 
 Search: coordinate descent, knob after knob, first for every bucket at once (a setting that
@@ -34,6 +35,9 @@ KNOBS = {
     "splat_walk_weight": (2, 3, 6),
 }
 DEFAULT = {"sph_block": 256, "density_variant": 0, "splat_tile_ratio": 6, "splat_walk_weight": 3}
+# knobs of the whole batch: the number of lanes the scenes are split into (clay_batch_set_lanes)
+LANES = (1, 2, 3, 4)
+DEFAULT_LANES = 1
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_build", "autotune.json")
 
 
@@ -64,13 +68,13 @@ def _time(batch, stream, frames):
     return a.elapsed_time(z) / frames
 
 
-def _trial(root, sims, extra, snaps, choice, stream, frames):
+def _trial(root, sims, extra, snaps, choice, lanes, stream, frames):
     # every trial from the same state: stepping moves the fluid, and a later, more spread-out
     # state would cost more whatever the setting
     for s, snap in zip(sims, snaps):
         s.upload(snap)
     batch = Batch(root, sims, extra_splats=extra, sph_block=choice[len(BUCKETS)]["sph_block"], use_graph=True)
-    apply(batch, {"uppers": list(BUCKETS), "tunings": [choice[i] for i in range(len(BUCKETS) + 1)]})
+    apply(batch, {"uppers": list(BUCKETS), "tunings": [choice[i] for i in range(len(BUCKETS) + 1)], "lanes": lanes})
     ms = _time(batch, stream, frames)
     batch.destroy()
     return ms
@@ -93,11 +97,12 @@ def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=
         return cache[sig], {"cached": True, "signature": sig}
     present = sorted({bucket_index(s.capacity) for s in sims})
     choice = {i: dict(DEFAULT) for i in range(len(BUCKETS) + 1)}
+    lanes = DEFAULT_LANES
     snaps = [s.download() for s in sims]
     report = {"signature": sig, "trials": []}
 
-    def timed(ch):
-        return _trial(root, sims, extra, snaps, ch, stream, frames)
+    def timed(ch, ln=None):
+        return _trial(root, sims, extra, snaps, ch, lanes if ln is None else ln, stream, frames)
 
     def consider(buckets, knob, label):
         nonlocal choice
@@ -116,6 +121,17 @@ def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=
                 choice = cand
 
     try:
+        # the lanes first, for the whole batch
+        for v in LANES:
+            if v == lanes:
+                continue
+            before = timed(choice)
+            ms = timed(choice, v)
+            after = timed(choice)
+            cur = 0.5 * (before + after)
+            report["trials"].append({"bucket": "batch", "lanes": v, "ms": round(ms, 4), "current_ms": round(cur, 4)})
+            if ms < cur * (1.0 - min_gain):
+                lanes = v
         everyone = list(range(len(BUCKETS) + 1))
         for knob in KNOBS:
             consider(everyone, knob, "all")
@@ -125,13 +141,13 @@ def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=
                     consider([bi], knob, bi)
         # the chosen settings against the defaults, timed again side by side
         default = {i: dict(DEFAULT) for i in range(len(BUCKETS) + 1)}
-        t_default = timed(default)
+        t_default = timed(default, DEFAULT_LANES)
         t_tuned = timed(choice)
     finally:
         torch.cuda.synchronize()
         for s, snap in zip(sims, snaps):
             s.upload(snap)
-    result = {"uppers": list(BUCKETS), "tunings": [choice[i] for i in range(len(BUCKETS) + 1)],
+    result = {"uppers": list(BUCKETS), "tunings": [choice[i] for i in range(len(BUCKETS) + 1)], "lanes": lanes,
               "default_ms": t_default, "tuned_ms": t_tuned, "gain": t_default / t_tuned - 1.0,
               "changed": [{"bucket": i, **{k: v for k, v in choice[i].items() if v != DEFAULT[k]}}
                           for i in present if choice[i] != DEFAULT],
@@ -146,3 +162,4 @@ def tune(root, sims, extra=(), stream=None, frames=10, use_cache=True, min_gain=
 
 def apply(batch, result):
     batch.set_bucket_tuning(result["uppers"], result["tunings"])
+    batch.set_lanes(result.get("lanes", DEFAULT_LANES))

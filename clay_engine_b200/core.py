@@ -677,6 +677,10 @@ class Batch:
                                   int(d["splat_walk_weight"]))
         check(lib().clay_batch_set_bucket_tuning(self.handle, u, t, len(uppers)))
 
+    def set_lanes(self, lanes: int):
+        """Step the scenes as `lanes` groups whose passes run side by side (same results)."""
+        check(lib().clay_batch_set_lanes(self.handle, int(lanes)))
+
     def step(self, pass_=None):
         check(lib().clay_batch_step(self.handle, stream_handle(pass_)))
 

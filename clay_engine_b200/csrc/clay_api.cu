@@ -1370,6 +1370,18 @@ struct clay_batch {
     int density_variant;
   };
   std::vector<PartGroup> groups;
+  // The scenes split into lanes, each stepped as its own chain of launches on its own stream
+  // (forked from the frame's stream, joined at its end): the lanes' kernels run side by side,
+  // so one lane's latency-bound passes overlap another's issue-bound ones and each pass's tail.
+  struct Lane {
+    std::vector<PartGroup> groups;
+    Work *w_emit = nullptr, *w_scan = nullptr, *w_ssplat = nullptr, *w_sres = nullptr;
+    int n_part = 0, n_emit = 0, n_scan = 0, n_ssplat = 0, n_sres = 0;
+    cudaStream_t stream = nullptr;  // lane 0 runs on the frame's stream
+    cudaEvent_t done = nullptr;
+  };
+  std::vector<Lane> lanes;
+  int n_lanes = 1;
   int bucket_of(int64_t capacity) const {
     for (size_t i = 0; i < bucket_upper.size(); i++)
       if (capacity < bucket_upper[i]) return static_cast<int>(i);
@@ -1419,6 +1431,10 @@ struct clay_batch {
     if (side) cudaStreamDestroy(side);
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
+    for (auto& l : lanes) {
+      if (l.stream) cudaStreamDestroy(l.stream);
+      if (l.done) cudaEventDestroy(l.done);
+    }
     for (int k = 0; k < 2; k++) {
       if (h_params[k]) cudaFreeHost(h_params[k]);
       if (params_ev[k]) cudaEventDestroy(params_ev[k]);
@@ -1544,6 +1560,57 @@ int batch_build(clay_batch* b) {
     if ((rc = b->upload_table(&w, by_block[g]))) return rc;
     b->groups.push_back({w, static_cast<int>(by_block[g].size()), blocks[g].first, blocks[g].second});
   }
+  // lanes: scenes dealt largest first to the lane with the fewest particles so far
+  {
+    const int nl = std::max(1, std::min(b->n_lanes, static_cast<int>(std::max<size_t>(b->sims.size(), 1))));
+    std::vector<int> lane_of(b->sims.size(), 0);
+    std::vector<int64_t> load(static_cast<size_t>(nl), 0);
+    std::vector<size_t> by_size(b->sims.size());
+    for (size_t i = 0; i < by_size.size(); i++) by_size[i] = i;
+    std::stable_sort(by_size.begin(), by_size.end(),
+                     [&](size_t x, size_t y) { return b->sims[x]->capacity > b->sims[y]->capacity; });
+    for (size_t i : by_size) {
+      const int l = static_cast<int>(std::min_element(load.begin(), load.end()) - load.begin());
+      lane_of[i] = l;
+      load[static_cast<size_t>(l)] += b->sims[i]->capacity;
+    }
+    const size_t old_lanes = b->lanes.size();
+    for (size_t l = static_cast<size_t>(nl); l < old_lanes; l++) {
+      if (b->lanes[l].stream) cudaStreamDestroy(b->lanes[l].stream);
+      if (b->lanes[l].done) cudaEventDestroy(b->lanes[l].done);
+    }
+    b->lanes.resize(static_cast<size_t>(nl));
+    for (size_t l = old_lanes; l < b->lanes.size(); l++) b->lanes[l] = clay_batch::Lane{};
+    for (int l = 0; l < nl; l++) {
+      clay_batch::Lane& ln = b->lanes[static_cast<size_t>(l)];
+      auto mine = [&](const std::vector<Work>& all) {
+        std::vector<Work> out;
+        for (const Work& w : all)
+          if (lane_of[w.obj] == l) out.push_back(w);
+        return out;
+      };
+      ln.groups.clear();
+      ln.n_part = 0;
+      for (size_t g = 0; g < blocks.size(); g++) {
+        std::vector<Work> wl = mine(by_block[g]);
+        if (wl.empty()) continue;
+        Work* w = nullptr;
+        if ((rc = b->upload_table(&w, wl))) return rc;
+        ln.groups.push_back({w, static_cast<int>(wl.size()), blocks[g].first, blocks[g].second});
+        ln.n_part += static_cast<int>(wl.size());
+      }
+      const std::vector<Work> le = mine(we), lsc = mine(wsc), lss = mine(wss), lsr = mine(wsr);
+      if ((rc = b->upload_table(&ln.w_emit, le)) || (rc = b->upload_table(&ln.w_scan, lsc)) ||
+          (rc = b->upload_table(&ln.w_ssplat, lss)) || (rc = b->upload_table(&ln.w_sres, lsr)))
+        return rc;
+      ln.n_emit = static_cast<int>(le.size());
+      ln.n_scan = static_cast<int>(lsc.size());
+      ln.n_ssplat = static_cast<int>(lss.size());
+      ln.n_sres = static_cast<int>(lsr.size());
+      if (l > 0 && !ln.stream) CK(cudaStreamCreateWithFlags(&ln.stream, cudaStreamNonBlocking));
+      if (l > 0 && !ln.done) CK(cudaEventCreateWithFlags(&ln.done, cudaEventDisableTiming));
+    }
+  }
   b->n_emit = static_cast<int>(we.size());
   b->n_scan = static_cast<int>(wsc.size());
   b->n_xsplat = static_cast<int>(wxs.size());
@@ -1562,11 +1629,11 @@ int batch_build(clay_batch* b) {
 int batch_enqueue(clay_batch* b, cudaStream_t s) {
   const int T = b->tune.sph_block;
   const SceneDev* d = b->d_scenes;
+  const bool multi = b->lanes.size() > 1;
   // the extra clouds' bake: on the side stream when there are fluids to overlap it with
   const bool fork = b->n_xsplat && b->n_part && b->max_substeps > 0;
-  bool joined = !fork;
-  if (fork) {  // the stream and events exist from batch_build on (never created inside a capture)
-    CK(cudaEventRecord(b->ev_fork, s));
+  if (fork || multi) CK(cudaEventRecord(b->ev_fork, s));  // the stream and events exist from batch_build on
+  if (fork) {
     CK(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
     CK(L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, kSplatAccVoxelsDiscs, b->side));
     if (b->n_xres) CK(L_resolve(b->d_extra, b->w_xres, b->n_xres, b->side));
@@ -1575,32 +1642,40 @@ int batch_enqueue(clay_batch* b, cudaStream_t s) {
     if (b->n_xsplat) CK(L_splat(b->d_extra, b->w_xsplat, b->n_xsplat, 1, kSplatAccVoxelsDiscs, s));
     if (b->n_xres) CK(L_resolve(b->d_extra, b->w_xres, b->n_xres, s));
   }
-  if (b->n_part) {
-    CK(L_emit(d, b->w_emit, b->n_emit, T, s));
-    for (int sub = 0; sub < b->max_substeps; sub++) {
-      for (auto& g : b->groups) CK(L_cell_key(d, g.w, g.n, g.T, sub, s));
-      for (auto& g : b->groups) CK(L_cell_count(d, g.w, g.n, g.T, sub, s));
-      CK(L_scan_partial(d, b->w_scan, b->n_scan, sub, s));
-      CK(L_scan_final(d, b->w_scan, b->n_scan, sub, s));
-      for (auto& g : b->groups) CK(L_cell_scatter(d, g.w, g.n, g.T, sub, s));
-      for (auto& g : b->groups) CK(L_cell_order(d, g.w, g.n, g.T, sub, s));
-      for (auto& g : b->groups) {
-        if (b->mode == CLAY_MODE_REFERENCE) CK(L_density_ref(d, g.w, g.n, g.T, sub, s, g.density_variant));
-        else CK(L_density_fast(d, g.w, g.n, g.T, sub, s, g.density_variant));
-      }
-      if (!joined) {  // the fluids collide with the bodies' volumes from here on
-        CK(cudaStreamWaitEvent(s, b->ev_join, 0));
-        joined = true;
-      }
-      for (auto& g : b->groups) {
-        if (b->mode == CLAY_MODE_REFERENCE) CK(L_forces_ref(d, g.w, g.n, g.T, sub, s));
-        else CK(L_forces_fast(d, g.w, g.n, g.T, sub, s));
+  for (size_t li = 0; li < b->lanes.size(); li++) {
+    clay_batch::Lane& ln = b->lanes[li];
+    cudaStream_t ls = li == 0 ? s : ln.stream;
+    if (li > 0) CK(cudaStreamWaitEvent(ls, b->ev_fork, 0));
+    bool joined = !fork;
+    if (ln.n_part) {
+      CK(L_emit(d, ln.w_emit, ln.n_emit, T, ls));
+      for (int sub = 0; sub < b->max_substeps; sub++) {
+        for (auto& g : ln.groups) CK(L_cell_key(d, g.w, g.n, g.T, sub, ls));
+        for (auto& g : ln.groups) CK(L_cell_count(d, g.w, g.n, g.T, sub, ls));
+        CK(L_scan_partial(d, ln.w_scan, ln.n_scan, sub, ls));
+        CK(L_scan_final(d, ln.w_scan, ln.n_scan, sub, ls));
+        for (auto& g : ln.groups) CK(L_cell_scatter(d, g.w, g.n, g.T, sub, ls));
+        for (auto& g : ln.groups) CK(L_cell_order(d, g.w, g.n, g.T, sub, ls));
+        for (auto& g : ln.groups) {
+          if (b->mode == CLAY_MODE_REFERENCE) CK(L_density_ref(d, g.w, g.n, g.T, sub, ls, g.density_variant));
+          else CK(L_density_fast(d, g.w, g.n, g.T, sub, ls, g.density_variant));
+        }
+        if (!joined) {  // the fluids collide with the bodies' volumes from here on
+          CK(cudaStreamWaitEvent(ls, b->ev_join, 0));
+          joined = true;
+        }
+        for (auto& g : ln.groups) {
+          if (b->mode == CLAY_MODE_REFERENCE) CK(L_forces_ref(d, g.w, g.n, g.T, sub, ls));
+          else CK(L_forces_fast(d, g.w, g.n, g.T, sub, ls));
+        }
       }
     }
+    if (!joined) CK(cudaStreamWaitEvent(ls, b->ev_join, 0));
+    if (ln.n_ssplat) CK(L_splat(b->d_surf, ln.w_ssplat, ln.n_ssplat, 1, kSplatAccVoxels, ls));
+    if (ln.n_sres) CK(L_resolve(b->d_surf, ln.w_sres, ln.n_sres, ls));
+    if (li > 0) CK(cudaEventRecord(ln.done, ls));
   }
-  if (!joined) CK(cudaStreamWaitEvent(s, b->ev_join, 0));
-  if (b->n_ssplat) CK(L_splat(b->d_surf, b->w_ssplat, b->n_ssplat, 1, kSplatAccVoxels, s));
-  if (b->n_sres) CK(L_resolve(b->d_surf, b->w_sres, b->n_sres, s));
+  for (size_t li = 1; li < b->lanes.size(); li++) CK(cudaStreamWaitEvent(s, b->lanes[li].done, 0));
   return CLAY_OK;
 }
 
@@ -1660,6 +1735,13 @@ int clay_batch_set_bucket_blocks(clay_batch* b, const int64_t* upper, const int3
   b->bucket_upper.assign(upper, upper + n);
   b->bucket_block.assign(blocks, blocks + n);
   b->bucket_tune.clear();
+  b->release();
+  return CLAY_OK;
+}
+
+int clay_batch_set_lanes(clay_batch* b, int lanes) {
+  if (!b || lanes < 1 || lanes > 8) return fail(CLAY_EINVAL, "clay_batch_set_lanes: lanes must be in 1..8");
+  b->n_lanes = lanes;
   b->release();
   return CLAY_OK;
 }

@@ -460,6 +460,10 @@ typedef struct clay_bucket_tuning {
   int32_t splat_walk_weight;  /* blocks take the block walk up to this many times their pairs (3) */
 } clay_bucket_tuning;
 int clay_batch_set_bucket_tuning(clay_batch* b, const int64_t* upper, const clay_bucket_tuning* t, int n);
+/* No counterpart in the reference: split the scenes into `lanes` (1..8, default 1) groups of
+ * about equal particle counts, each stepped as its own chain of launches on its own stream
+ * inside the frame, so the groups' passes run side by side on the GPU. Same results. */
+int clay_batch_set_lanes(clay_batch* b, int lanes);
 /* One frame for every scene: host bookkeeping of each sim (as clay_fluid_step), then the
  * batched passes (or the captured graph) on `stream`. */
 int clay_batch_step(clay_batch* b, void* stream);

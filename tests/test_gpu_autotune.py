@@ -44,7 +44,9 @@ def test_tuning_restores_state_and_keeps_results(root):
     # makes the earlier current value a candidate again
     per_pass = sum(len(v) - 1 for v in autotune.KNOBS.values())
     per_pass_max = sum(len(v) for v in autotune.KNOBS.values())
-    assert per_pass <= len(report["trials"]) <= per_pass_max * (1 + n_buckets)
+    lanes = len(autotune.LANES) - 1
+    assert per_pass + lanes <= len(report["trials"]) <= per_pass_max * (1 + n_buckets) + lanes + 1
+    assert result["lanes"] in autotune.LANES
     assert all(t["ms"] > 0 and t["current_ms"] > 0 for t in report["trials"])
     assert result["default_ms"] > 0 and result["tuned_ms"] > 0
     for s, snap in zip(a, before):
@@ -66,7 +68,7 @@ def test_tuning_restores_state_and_keeps_results(root):
         o.destroy()
 
 
-@pytest.mark.parametrize("knob", sorted(__import__("clay_engine_b200.autotune", fromlist=["KNOBS"]).KNOBS))
+@pytest.mark.parametrize("knob", sorted(__import__("clay_engine_b200.autotune", fromlist=["KNOBS"]).KNOBS) + ["lanes"])
 def test_every_setting_is_bit_exact_in_reference_mode(root, knob):
     """Each value of each knob, applied to every bucket, against the defaults: same particle
     state and bake after two frames (a batch with spheres and a clay-body shell of discs)."""
@@ -90,8 +92,10 @@ def test_every_setting_is_bit_exact_in_reference_mode(root, knob):
                               worldSize=32 * 0.083)
         shell.setCenter((1.0, 0.0, 0.0))
         b = ce.Batch(root, sims, extra_splats=[shell])
+        setting = dict(setting)
+        lanes = setting.pop("lanes", autotune.DEFAULT_LANES)
         tun = [dict(autotune.DEFAULT, **setting) for _ in range(len(autotune.BUCKETS) + 1)]
-        autotune.apply(b, {"uppers": list(autotune.BUCKETS), "tunings": tun})
+        autotune.apply(b, {"uppers": list(autotune.BUCKETS), "tunings": tun, "lanes": lanes})
         for _ in range(2):
             b.step(stream)
         torch.cuda.synchronize()
@@ -103,8 +107,9 @@ def test_every_setting_is_bit_exact_in_reference_mode(root, knob):
         return out
 
     ref = run({})
-    for v in autotune.KNOBS[knob]:
-        if v == autotune.DEFAULT[knob]:
+    values = autotune.LANES if knob == "lanes" else autotune.KNOBS[knob]
+    for v in values:
+        if v == (autotune.DEFAULT_LANES if knob == "lanes" else autotune.DEFAULT[knob]):
             continue
         got = run({knob: v})
         for (ga, gd), (ra, rd) in zip(got, ref):

@@ -29,9 +29,10 @@ def scene(root, counts, seed, mode, collider):
     return sims
 
 
+@pytest.mark.parametrize("lanes", [1, 3])
 @pytest.mark.parametrize("mode", ["reference", "fast"])
 @pytest.mark.parametrize("use_graph", [True, False])
-def test_batched_equals_alone(root, mode, use_graph):
+def test_batched_equals_alone(root, mode, use_graph, lanes):
     import clay_engine_b200 as ce
     from clay_engine_b200 import scenes
 
@@ -46,6 +47,7 @@ def test_batched_equals_alone(root, mode, use_graph):
     for s in alone:
         s.spawn(50, (0.0, 5.0, 0.0), (0.0, -1.0, 0.0))
     b = ce.Batch(root, batch_sims, use_graph=use_graph)
+    b.set_lanes(lanes)
     for frame in range(3):
         b.step()
         for s in alone:
