@@ -3,7 +3,7 @@
 Scenes are grouped by capacity into buckets. The knobs of a bucket are the thread-block size of
 the particle passes, the density pass's variant (one loop; distance tests then the accepted
 neighbours; one loop over neighbours staged in shared memory; in fast mode, the cells ordered by
-eighths along x and each neighbour row trimmed to the eighths within reach) and the splat's strategy thresholds (how much larger than the particles' own voxel
+half-cell and only the half-cells within reach visited) and the splat's strategy thresholds (how much larger than the particles' own voxel
 boxes a block's union box may be and still take the register-blocked tile walk, or the block
 walk); the batch as a whole also picks how many lanes (groups of scenes whose chains of
 launches run side by side) it steps. Every setting gives the same results (reference mode bit for bit); they only move time

@@ -1499,11 +1499,11 @@ int batch_build(clay_batch* b) {
     clay_fluid* f = b->sims[i];
     scenes.push_back(f->hs);
     {
-      // slice order for the fast density variant 3 (a tag of 3 bits over the index, cell
+      // half-cell order for the fast density variant 3 (a tag of 3 bits over the index, cell
       // counts up to 255 in the byte ends)
       const clay_bucket_tuning bt = b->tuning_of(f->capacity);
       scenes.back().subcells = (b->mode == CLAY_MODE_FAST && bt.density_variant == 3 &&
-                                f->capacity <= static_cast<int64_t>(kSliceMask) + 1 && f->bucket <= 255)
+                                f->capacity <= static_cast<int64_t>(kHalfMask) + 1 && f->bucket <= 255)
                                    ? 1
                                    : 0;
     }

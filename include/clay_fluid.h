@@ -457,9 +457,8 @@ typedef struct clay_bucket_tuning {
   int32_t sph_block;          /* threads per block of the particle passes, 64..256, multiple of 32 */
   int32_t density_variant;    /* 0: one loop (default); 1: distance tests, then the accepted
                                   neighbours; 2: one loop over neighbours staged in shared memory;
-                                  3: fast mode only, cells ordered by eighths along x and each
-                                  neighbour row trimmed to the eighths within reach (reference
-                                  mode runs 0) */
+                                  3: fast mode only, cells ordered by half-cell and only the
+                                  half-cells within reach visited (reference mode runs 0) */
   int32_t splat_tile_ratio;   /* sphere blocks take the tile walk up to this many times their pairs (6) */
   int32_t splat_walk_weight;  /* blocks take the block walk up to this many times their pairs (3) */
 } clay_bucket_tuning;

@@ -1,6 +1,6 @@
-"""Fast-mode density over trimmed rows (density variant 3): the cells are ordered by their eighths
-along x and each neighbour row is trimmed to the eighths within reach of the particle along x.
-It must find exactly the neighbours the reference's 27-cell scan accepts, so one frame from the same state stays within the fast-mode
+"""Fast-mode density over half-cells (density variant 3): the cells are ordered by half-cell and
+each particle visits only the half-cells within reach. It must find exactly the neighbours the
+reference's 27-cell scan accepts, so one frame from the same state stays within the fast-mode
 tolerance of the f32 oracle, with particles outside the grid, and a scene whose cells overflow
 (which reads whole cells, as the reference's bucket rule needs) in the same batch."""
 import numpy as np
@@ -16,7 +16,7 @@ FAST_REL_TOL_PRESSURE = 2e-4
 FAST_REL_TOL_VELOCITY = 1e-4
 
 
-def test_trimmed_row_density_within_tolerance(root, oracle):
+def test_half_cell_density_within_tolerance(root, oracle):
     import clay_engine_b200 as ce
     from clay_engine_b200 import autotune, scenes
 
