@@ -2,8 +2,7 @@
 
 Scenes are grouped by capacity into buckets. The knobs of a bucket are the thread-block size of
 the particle passes, the density pass's variant (one loop; distance tests then the accepted
-neighbours; one loop over neighbours staged in shared memory; in fast mode, the cells ordered by
-half-cell and only the half-cells within reach visited) and the splat's strategy thresholds (how much larger than the particles' own voxel
+neighbours; one loop over neighbours staged in shared memory) and the splat's strategy thresholds (how much larger than the particles' own voxel
 boxes a block's union box may be and still take the register-blocked tile walk, or the block
 walk); the batch as a whole also picks how many lanes (groups of scenes whose chains of
 launches run side by side) it steps. Every setting gives the same results (reference mode bit for bit); they only move time
@@ -31,7 +30,7 @@ from .core import Batch
 BUCKETS = (4096, 16384, 65536)       # capacity < 4k, < 16k, < 64k, and the rest
 KNOBS = {
     "sph_block": (64, 128, 192, 256),
-    "density_variant": (0, 1, 2, 3),
+    "density_variant": (0, 1, 2),
     "splat_tile_ratio": (3, 6, 12),
     "splat_walk_weight": (2, 3, 6),
 }

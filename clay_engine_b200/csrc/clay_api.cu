@@ -957,8 +957,7 @@ int clay_fluid_estimate_bytes(const clay_fluid_opts* opts, uint64_t* out) {
   const uint64_t C = static_cast<uint64_t>(f.capacity);
   const uint64_t cells = static_cast<uint64_t>(f.G) * f.G * f.G;
   uint64_t b = C * (sizeof(ParticleDev) + 4 * sizeof(uint32_t) + 4 * sizeof(float4) + (kMaxNbr / 4) * sizeof(uint4)) +
-               (cells + 1) * sizeof(uint32_t) + (cells + 2) * sizeof(uint32_t) + (cells + 1) * sizeof(uint2) +
-               sizeof(ParamsDev) + sizeof(ContactsDev) +
+               (cells + 1) * sizeof(uint32_t) + (cells + 2) * sizeof(uint32_t) + sizeof(ParamsDev) + sizeof(ContactsDev) +
                sizeof(GridState) + sizeof(SceneDev);
   uint64_t t = 0;
   for (int m = 0; m < f.bake_mips; m++) {
@@ -1019,7 +1018,6 @@ int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_o
       (rc = f->alloc(&f->hs.svel, C)) || (rc = f->alloc(&f->hs.sdp, C)) || (rc = f->alloc(&f->hs.spx, C)) ||
       (rc = f->alloc(&f->hs.nbr, C * (kMaxNbr / 4))) ||
       (rc = f->alloc(&f->hs.counts, cells + 1)) || (rc = f->alloc(&f->hs.cell_start, cells + 2)) ||
-      (rc = f->alloc(&f->hs.substart, cells + 1)) ||
       (rc = f->alloc(&f->d_scene, 1))) {
     clay_fluid_destroy(f);
     return rc;
@@ -1032,7 +1030,6 @@ int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_o
   CK(cudaMemset(f->contacts, 0, sizeof(ContactsDev)));
   CK(cudaMemset(f->hs.counts, 0, sizeof(uint32_t) * (cells + 1)));
   CK(cudaMemset(f->hs.cell_start, 0, sizeof(uint32_t) * (cells + 2)));
-  CK(cudaMemset(f->hs.substart, 0, sizeof(uint2) * (cells + 1)));
   {
     GridState gsh;
     std::memset(&gsh, 0, sizeof(gsh));
@@ -1498,15 +1495,6 @@ int batch_build(clay_batch* b) {
   for (size_t i = 0; i < b->sims.size(); i++) {
     clay_fluid* f = b->sims[i];
     scenes.push_back(f->hs);
-    {
-      // half-cell order for the fast density variant 3 (a tag of 3 bits over the index, cell
-      // counts up to 255 in the byte ends)
-      const clay_bucket_tuning bt = b->tuning_of(f->capacity);
-      scenes.back().subcells = (b->mode == CLAY_MODE_FAST && bt.density_variant == 3 &&
-                                f->capacity <= static_cast<int64_t>(kHalfMask) + 1 && f->bucket <= 255)
-                                   ? 1
-                                   : 0;
-    }
     b->max_substeps = std::max(b->max_substeps, f->substeps);
     uint32_t obj = static_cast<uint32_t>(i);
     const clay_bucket_tuning bt = b->tuning_of(f->capacity);
@@ -1763,8 +1751,8 @@ int clay_batch_set_bucket_tuning(clay_batch* b, const int64_t* upper, const clay
   for (int i = 0; i <= n; i++) {
     if (t[i].sph_block < 64 || t[i].sph_block > 256 || (t[i].sph_block & 31))
       return fail(CLAY_EINVAL, "bucket block %d must be a multiple of 32 in 64..256", t[i].sph_block);
-    if (t[i].density_variant < 0 || t[i].density_variant > 3)
-      return fail(CLAY_EINVAL, "bucket density variant %d is not 0..3", t[i].density_variant);
+    if (t[i].density_variant < 0 || t[i].density_variant > 2)
+      return fail(CLAY_EINVAL, "bucket density variant %d is not 0, 1 or 2", t[i].density_variant);
     if (t[i].splat_tile_ratio < 1 || t[i].splat_tile_ratio > 64 || t[i].splat_walk_weight < 1 || t[i].splat_walk_weight > 64)
       return fail(CLAY_EINVAL, "bucket splat thresholds must be in 1..64");
     if (i > 0 && i < n && upper[i] <= upper[i - 1]) return fail(CLAY_EINVAL, "bucket bounds must increase");

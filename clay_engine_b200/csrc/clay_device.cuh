@@ -18,8 +18,6 @@ constexpr int kMaxLeaves = 8;
 constexpr int kMaxParts = 64;
 constexpr int kMaxMips = 8;
 constexpr uint32_t kMaxNbr = 64;  // neighbour-list slots per particle
-// the cell build's temporary index array carries a particle's half-cell in its top bits
-constexpr uint32_t kHalfShift = 29, kHalfMask = (1u << kHalfShift) - 1u;
 constexpr int kSplatWarps = 8;  // warps per block of the splat pass
 constexpr int kSplatItems = 2048;  // compacted (brick, slice) items of the sphere block walk
 constexpr int kSplatStencil = 2048;  // voxel offsets of the own-box walk's stencil (8 KB of shared memory)
@@ -141,19 +139,13 @@ struct __align__(16) SceneDev {
   uint4* nbr;  // accepted neighbours of the density pass, 4 per entry, slot-major: nbr[(j / 4) * capacity + k]
   uint32_t* counts;
   uint32_t* cell_start;
-  // Per cell, where each of its eight half-cells begins inside its range (bytes 1-8 of two
-  // words: the ends of half-cells 0..7, indexed x + 2y + 4z), written by the order pass when
-  // `subcells` is set and no cell overflowed; the fast density pass then visits only the
-  // half-cells that can lie within h of a particle.
-  uint2* substart;
   const FieldDev* world;
   float h, h2, inv_h, h6, mass, mass_poly6, spiky, rest, rest_floor, radius;
   float gorig[3], wlo[3], whi[3];
   int32_t G;
   uint32_t capacity, bucket, parts_scan;
   int32_t substeps;
-  int32_t subcells;  // fast mode: order each cell by half-cell, then index (see substart)
-  int32_t pad_[2];
+  int32_t pad_[3];
 };
 
 // A ParticleCloud plus the SplatField it bakes into (splat.ts:136-276).
@@ -516,17 +508,6 @@ __device__ __forceinline__ void cell_of(const SceneDev& S, float px, float py, f
   cz = f2i(floorf((pz - S.gorig[2]) * S.inv_h));
 }
 
-// The half of its cell a position lies in, per axis (bit 0 x, 1 y, 2 z): floor(2u) - 2 floor(u)
-// of the cell coordinate u = (p - gridOrigin) / h as cellOf computes it (doubling is exact, so
-// the half agrees with the cell).
-__device__ __forceinline__ uint32_t half_cell_of(const SceneDev& S, float4 p) {
-  const float ux = (p.x - S.gorig[0]) * S.inv_h, uy = (p.y - S.gorig[1]) * S.inv_h, uz = (p.z - S.gorig[2]) * S.inv_h;
-  const uint32_t hx = static_cast<uint32_t>(floorf(ux * 2.0f) - 2.0f * floorf(ux));
-  const uint32_t hy = static_cast<uint32_t>(floorf(uy * 2.0f) - 2.0f * floorf(uy));
-  const uint32_t hz = static_cast<uint32_t>(floorf(uz * 2.0f) - 2.0f * floorf(uz));
-  return (hx & 1u) | ((hy & 1u) << 1) | ((hz & 1u) << 2);
-}
-
 struct BoxInfo {
   int x0, y0, z0;
   uint32_t bx, by, bz, L;
@@ -786,11 +767,7 @@ __global__ void k_cell_scatter(const SceneDev* __restrict__ scenes, const Work* 
   uint32_t count = work_count(S);
   uint32_t i = w.first + threadIdx.x;
   if (i >= count || threadIdx.x >= w.n) return;
-  // with half-cells the index carries its half-cell in the top three bits, so that the order
-  // pass sorts a cell by (half-cell, index) with one comparison
-  uint32_t tag = 0;
-  if (S.subcells && !S.gs->overflow) tag = half_cell_of(S, S.parts[i].a) << kHalfShift;
-  S.tmp[S.cell_start[S.key[i]] + S.rank[i]] = i | tag;
+  S.tmp[S.cell_start[S.key[i]] + S.rank[i]] = i;
 }
 
 // Cell build, pass 5: deterministic order inside each cell (ascending particle index, so
@@ -803,27 +780,12 @@ __global__ void k_cell_order(const SceneDev* __restrict__ scenes, const Work* __
   uint32_t count = work_count(S);
   uint32_t k = w.first + threadIdx.x;
   if (k >= count || threadIdx.x >= w.n) return;
-  const uint32_t t = S.tmp[k];  // the index, tagged with its half-cell when S.subcells is on
-  uint32_t id = t & kHalfMask;
+  uint32_t id = S.tmp[k];
   uint32_t l = S.key[id];
   uint32_t s = S.cell_start[l], e = S.cell_start[l + 1];
   uint32_t r = 0;
-  for (uint32_t q = s; q < e; q++) r += (S.tmp[q] < t) ? 1u : 0u;
+  for (uint32_t q = s; q < e; q++) r += (S.tmp[q] < id) ? 1u : 0u;
   uint32_t f = s + r;
-  if (r == 0 && S.subcells && !S.gs->overflow && l < S.gs->L) {
-    // the cell's first particle publishes where its half-cells end (a cell holds at most
-    // `bucket` <= 255 particles here, so every end fits a byte)
-    uint32_t c[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    for (uint32_t q = s; q < e; q++) c[S.tmp[q] >> kHalfShift]++;
-    uint32_t run = 0, lo = 0, hi = 0;
-#pragma unroll
-    for (int h = 0; h < 8; h++) {
-      run += c[h];
-      if (h < 4) lo |= run << (8 * h);
-      else hi |= run << (8 * (h - 4));
-    }
-    S.substart[l] = make_uint2(lo, hi);
-  }
   S.sorted_id[f] = id;
   const ParticleDev& P = S.parts[id];
   S.spos[f] = P.a;
@@ -911,68 +873,6 @@ __device__ __forceinline__ void for_neighbour_ranges(const SceneDev& S, const Bo
   }
 }
 
-// Fast mode over half-cells: the candidates of the 27 cells restricted to the half-cells that
-// can hold a point within h of the particle. Per axis, a neighbour cell's far half is more
-// than h away unless the particle sits in the half of its own cell that faces it; the test
-// keeps a margin of 1e-3 of a cell over the rounding of the cell coordinates, so every pair
-// the reference accepts (r^2 < h^2) is visited. f(s, e) per run of a cell's half-cells along x.
-// Needs the cells ordered by half-cell (S.subcells) with no cell overflowed.
-template <class F>
-__device__ __forceinline__ void for_half_cell_ranges(const SceneDev& S, const BoxInfo& b, float4 me, int cx, int cy,
-                                                     int cz, F&& f) {
-  const int G = S.G;
-  const float ux = (me.x - S.gorig[0]) * S.inv_h, uy = (me.y - S.gorig[1]) * S.inv_h, uz = (me.z - S.gorig[2]) * S.inv_h;
-  const float fx = ux - floorf(ux), fy = uy - floorf(uy), fz = uz - floorf(uz);
-  // the halves [lo, hi] of the neighbour at offset d (0: the low half, 1: the high half)
-  auto halves = [](int d, float fr, int& lo, int& hi) {
-    lo = 0;
-    hi = 1;
-    if (d < 0) lo = fr < 0.501f ? 0 : 1;
-    if (d > 0) hi = fr >= 0.499f ? 1 : 0;
-  };
-  cx = min(max(cx, -2), G + 1);
-  cy = min(max(cy, -2), G + 1);
-  cz = min(max(cz, -2), G + 1);
-  const int x1b = b.x0 + static_cast<int>(b.bx) - 1;
-  const int y1b = b.y0 + static_cast<int>(b.by) - 1;
-  const int z1b = b.z0 + static_cast<int>(b.bz) - 1;
-  if (b.L == 0) return;
-  const int xl = max(cx - 1, b.x0), xh = min(cx + 1, x1b);
-  if (xl > xh) return;
-  for (int dz = -1; dz <= 1; dz++) {
-    const int z = cz + dz;
-    if (z < b.z0 || z > z1b) continue;
-    int zlo, zhi;
-    halves(dz, fz, zlo, zhi);
-    for (int dy = -1; dy <= 1; dy++) {
-      const int y = cy + dy;
-      if (y < b.y0 || y > y1b) continue;
-      int ylo, yhi;
-      halves(dy, fy, ylo, yhi);
-      const uint32_t row = b.bx * (static_cast<uint32_t>(y - b.y0) + b.by * static_cast<uint32_t>(z - b.z0));
-      for (int x = xl; x <= xh; x++) {
-        const uint32_t l = row + static_cast<uint32_t>(x - b.x0);
-        const uint32_t s = __ldg(S.cell_start + l), e = __ldg(S.cell_start + l + 1);
-        if (s == e) continue;
-        int xlo, xhi;
-        halves(x - cx, fx, xlo, xhi);
-        const uint2 o = __ldg(S.substart + l);
-        // end of half-cell h (0..7) inside the cell; the end of "half-cell -1" is 0
-        auto end_of = [&](int h) -> uint32_t {
-          if (h < 0) return 0u;
-          const uint32_t wv = h < 4 ? o.x : o.y;
-          return (wv >> (8 * (h & 3))) & 0xffu;
-        };
-        for (int hz = zlo; hz <= zhi; hz++)
-          for (int hy = ylo; hy <= yhi; hy++) {
-            const int h0 = xlo + 2 * hy + 4 * hz, h1 = xhi + 2 * hy + 4 * hz;
-            f(s + end_of(h0 - 1), s + end_of(h1));
-          }
-      }
-    }
-  }
-}
-
 // The local cell index (the cell build's order key) of a position: L, the out-of-grid bucket,
 // outside the grid (fluid.ts:318-322), else its place in the box of occupied cells.
 __device__ __forceinline__ uint32_t local_cell(const SceneDev& S, const BoxInfo& b, float4 p) {
@@ -986,7 +886,7 @@ constexpr int kDensityStage = 3040;  // staged neighbour positions per block (47
 
 // density (fluid.ts:333-368). kFast accumulates with Kahan compensation.
 //
-// Four variants; 0, 1 and 2 visit, sum and list the neighbours in the same order, 3 in its own:
+// Three variants, which visit, sum and list the neighbours in the same order:
 //  - kVariant 0: one loop, the accept work inside the distance-test loop;
 //  - kVariant 1: the candidates of a range 32 at a time in two phases: the distance test of
 //    every candidate, which leaves a bit mask of the accepted ones, then the accepted ones
@@ -994,8 +894,6 @@ constexpr int kDensityStage = 3040;  // staged neighbour positions per block (47
 //    warp's lanes accept at different candidates, so running the accept work inside the test
 //    loop keeps most lanes idle through it; in the second phase every lane with a pending
 //    neighbour works;
-//  - kVariant 3 (fast mode): variant 0 over half-cells (for_half_cell_ranges), when the
-//    scene's cells are ordered by half-cell; else as variant 0;
 //  - kVariant 2: variant 0 reading the candidates from shared memory. The block's particles
 //    are consecutive in the cell order, so their cells span a run [l0, l1] of local cell
 //    indices, and the neighbour row (dz, dy) of any of them lies in the cells
@@ -1106,25 +1004,6 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
       const float r2 = (dx * dx + dy * dy) + dz * dz;
       if (r2 < h2) accept(q, r2);
     });
-  } else if constexpr (kVariant == 3) {
-    // half-cells (fast mode with S.subcells): any other case reads the whole cells
-    if (kFast && S.subcells && !overflow) {
-      for_half_cell_ranges(S, b, me, cx, cy, cz, [&](uint32_t s, uint32_t e) {
-        for (uint32_t q = s; q < e; q++) {
-          const float4 o = __ldg(spos + q);
-          const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
-          const float r2 = (dx * dx + dy * dy) + dz * dz;
-          if (r2 < h2) accept(q, r2);
-        }
-      });
-    } else {
-      for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
-        const float4 o = __ldg(spos + q);
-        const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
-        const float r2 = (dx * dx + dy * dy) + dz * dz;
-        if (r2 < h2) accept(q, r2);
-      });
-    }
   } else if constexpr (kVariant == 2) {
     for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int r) {
       // the row's candidates [s, e) lie inside staged range r (see above): candidate q sits

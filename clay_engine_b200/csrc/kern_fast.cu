@@ -10,7 +10,6 @@ cudaError_t L_density_fast(const SceneDev* s, const Work* w, int blocks, int thr
                            int variant) {
   if (variant == 1) k_density<true, 1><<<blocks, threads, 0, st>>>(s, w, sub);
   else if (variant == 2) k_density<true, 2><<<blocks, threads, 0, st>>>(s, w, sub);
-  else if (variant == 3) k_density<true, 3><<<blocks, threads, 0, st>>>(s, w, sub);
   else k_density<true, 0><<<blocks, threads, 0, st>>>(s, w, sub);
   count_launch();
   return cudaPeekAtLastError();

@@ -21,8 +21,7 @@ void count_launches(uint64_t n);  // kernels replayed by a graph launch
 // Threads per block of the particle passes when no tuning overrides it.
 constexpr int kBlock = 256;
 // The density variant used when no tuning overrides it (0: one loop, 1: two phases, 2: one
-// loop over neighbour positions staged in shared memory, 3: fast mode over half-cells; the
-// reference mode runs 0 for 3).
+// loop over neighbour positions staged in shared memory).
 constexpr int kDensityVariant = 0;
 
 cudaError_t L_emit(const SceneDev* s, const Work* w, int blocks, int threads, cudaStream_t st);

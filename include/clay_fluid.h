@@ -450,15 +450,12 @@ int clay_batch_get_tuning(const clay_batch* b, clay_batch_tuning* t);
 int clay_batch_set_bucket_blocks(clay_batch* b, const int64_t* upper, const int32_t* blocks, int n);
 /* The autotuner's full output, per scene-size bucket: bucket i < n holds the scenes whose
  * capacity is below upper[i] (and not below upper[i-1]); bucket n the rest, so `t` has n + 1
- * entries. Every choice gives the same results (reference mode bit for bit; density variant 3
- * visits the neighbours in another order, which fast mode allows): they only move time
- * between the passes' strategies. */
+ * entries. Every choice gives the same results (reference mode bit for bit): they only move
+ * time between the passes' strategies. */
 typedef struct clay_bucket_tuning {
   int32_t sph_block;          /* threads per block of the particle passes, 64..256, multiple of 32 */
   int32_t density_variant;    /* 0: one loop (default); 1: distance tests, then the accepted
-                                  neighbours; 2: one loop over neighbours staged in shared memory;
-                                  3: fast mode only, cells ordered by half-cell and only the
-                                  half-cells within reach visited (reference mode runs 0) */
+                                  neighbours; 2: one loop over neighbours staged in shared memory */
   int32_t splat_tile_ratio;   /* sphere blocks take the tile walk up to this many times their pairs (6) */
   int32_t splat_walk_weight;  /* blocks take the block walk up to this many times their pairs (3) */
 } clay_bucket_tuning;
