@@ -68,7 +68,7 @@ class CloudDesc(C.Structure):
 
 class BucketTuning(C.Structure):
     _fields_ = [("sph_block", C.c_int32), ("density_variant", C.c_int32), ("splat_tile_ratio", C.c_int32),
-                ("splat_walk_weight", C.c_int32)]
+                ("splat_walk_weight", C.c_int32), ("forces_split", C.c_int32)]
 
 
 class Census(C.Structure):

@@ -33,8 +33,9 @@ KNOBS = {
     "density_variant": (0, 1, 2),
     "splat_tile_ratio": (3, 6, 12),
     "splat_walk_weight": (2, 3, 6),
+    "forces_split": (0, 1),
 }
-DEFAULT = {"sph_block": 256, "density_variant": 0, "splat_tile_ratio": 6, "splat_walk_weight": 3}
+DEFAULT = {"sph_block": 256, "density_variant": 0, "splat_tile_ratio": 6, "splat_walk_weight": 3, "forces_split": 0}
 # knobs of the whole batch: the number of lanes the scenes are split into (clay_batch_set_lanes)
 LANES = (1, 2, 3, 4)
 DEFAULT_LANES = 1

@@ -669,12 +669,12 @@ class Batch:
     def set_bucket_tuning(self, uppers, tunings):
         """Per scene-size bucket settings: `tunings` has len(uppers) + 1 dicts (the last for the
         scenes above every bound) with keys sph_block, density_variant, splat_tile_ratio,
-        splat_walk_weight."""
+        splat_walk_weight and forces_split."""
         u = (C.c_int64 * max(len(uppers), 1))(*[int(x) for x in uppers])
         t = (N.BucketTuning * len(tunings))()
         for i, d in enumerate(tunings):
             t[i] = N.BucketTuning(int(d["sph_block"]), int(d["density_variant"]), int(d["splat_tile_ratio"]),
-                                  int(d["splat_walk_weight"]))
+                                  int(d["splat_walk_weight"]), int(d.get("forces_split", 0)))
         check(lib().clay_batch_set_bucket_tuning(self.handle, u, t, len(uppers)))
 
     def set_lanes(self, lanes: int):

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/clay_fluid.h"
@@ -1368,6 +1369,7 @@ struct clay_batch {
     int n;
     int T;
     int density_variant;
+    bool forces_split;
   };
   std::vector<PartGroup> groups;
   // The scenes split into lanes, each stepped as its own chain of launches on its own stream
@@ -1397,6 +1399,7 @@ struct clay_batch {
     clay_bucket_tuning t{};
     t.sph_block = block_of(capacity);
     t.density_variant = kDensityVariant;
+    t.forces_split = 0;
     t.splat_tile_ratio = static_cast<int32_t>(kSplatTileRatio);
     t.splat_walk_weight = static_cast<int32_t>(kSplatWalkWeight);
     return t;
@@ -1490,7 +1493,7 @@ int batch_build(clay_batch* b) {
   std::vector<Work> wp, we, wsc;
   b->max_substeps = 0;
   // one group of particle-pass launches per distinct (block size, density variant)
-  std::vector<std::pair<int, int>> blocks;
+  std::vector<std::tuple<int, int, int>> blocks;
   std::vector<std::vector<Work>> by_block;
   for (size_t i = 0; i < b->sims.size(); i++) {
     clay_fluid* f = b->sims[i];
@@ -1499,7 +1502,7 @@ int batch_build(clay_batch* b) {
     uint32_t obj = static_cast<uint32_t>(i);
     const clay_bucket_tuning bt = b->tuning_of(f->capacity);
     const int Ts = bt.sph_block;
-    const std::pair<int, int> key(Ts, bt.density_variant);
+    const std::tuple<int, int, int> key(Ts, bt.density_variant, bt.forces_split != 0 ? 1 : 0);
     size_t gi = std::find(blocks.begin(), blocks.end(), key) - blocks.begin();
     if (gi == blocks.size()) {
       blocks.push_back(key);
@@ -1558,7 +1561,8 @@ int batch_build(clay_batch* b) {
   for (size_t g = 0; g < blocks.size(); g++) {
     Work* w = nullptr;
     if ((rc = b->upload_table(&w, by_block[g]))) return rc;
-    b->groups.push_back({w, static_cast<int>(by_block[g].size()), blocks[g].first, blocks[g].second});
+    b->groups.push_back({w, static_cast<int>(by_block[g].size()), std::get<0>(blocks[g]), std::get<1>(blocks[g]),
+                         std::get<2>(blocks[g]) != 0});
   }
   // lanes: scenes dealt largest first to the lane with the fewest particles so far
   {
@@ -1596,7 +1600,8 @@ int batch_build(clay_batch* b) {
         if (wl.empty()) continue;
         Work* w = nullptr;
         if ((rc = b->upload_table(&w, wl))) return rc;
-        ln.groups.push_back({w, static_cast<int>(wl.size()), blocks[g].first, blocks[g].second});
+        ln.groups.push_back({w, static_cast<int>(wl.size()), std::get<0>(blocks[g]), std::get<1>(blocks[g]),
+                             std::get<2>(blocks[g]) != 0});
         ln.n_part += static_cast<int>(wl.size());
       }
       const std::vector<Work> le = mine(we), lsc = mine(wsc), lss = mine(wss), lsr = mine(wsr);
@@ -1665,8 +1670,8 @@ int batch_enqueue(clay_batch* b, cudaStream_t s) {
           joined = true;
         }
         for (auto& g : ln.groups) {
-          if (b->mode == CLAY_MODE_REFERENCE) CK(L_forces_ref(d, g.w, g.n, g.T, sub, ls));
-          else CK(L_forces_fast(d, g.w, g.n, g.T, sub, ls));
+          if (b->mode == CLAY_MODE_REFERENCE) CK(L_forces_ref(d, g.w, g.n, g.T, sub, ls, g.forces_split));
+          else CK(L_forces_fast(d, g.w, g.n, g.T, sub, ls, g.forces_split));
         }
       }
     }
@@ -1905,7 +1910,8 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
           return rc;
       for (auto& g : b->groups)
         if ((rc = timed("forces_integrate", [&] {
-               return ref ? L_forces_ref(d, g.w, g.n, g.T, sub, s) : L_forces_fast(d, g.w, g.n, g.T, sub, s);
+               return ref ? L_forces_ref(d, g.w, g.n, g.T, sub, s, g.forces_split)
+                          : L_forces_fast(d, g.w, g.n, g.T, sub, s, g.forces_split);
              })))
           return rc;
     }

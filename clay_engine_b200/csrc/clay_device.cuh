@@ -1045,11 +1045,52 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   S.svel[k].w = pres;
 }
 
+// integrate (fluid.ts:449-491) of cell-ordered particle k: advance with the new velocity, collide
+// with the world field (push out along its normal, drop the inward velocity, record a contact),
+// clamp to the bake volume's walls, and write the particle's record.
+__device__ __forceinline__ void integrate_particle(const SceneDev& S, const ParamsDev& P, uint32_t k, const float4 me,
+                                                   const float4 mdp, float vx, float vy, float vz) {
+  const float nvx = vx, nvy = vy, nvz = vz;
+  float px = me.x + vx * P.dt, py = me.y + vy * P.dt, pz = me.z + vz * P.dt;
+  const FieldDev* world = S.world;
+  if (world && world->n > 0) {
+    float sx, sy;
+    int child = field_pick(world, px, py, pz, sx, sy);
+    float dw = sx;
+    if (dw < S.radius) {
+      float nx, ny, nz;
+      field_normal(world, child, px, py, pz, nx, ny, nz);
+      float push = S.radius - dw;
+      px = px + nx * push;
+      py = py + ny * push;
+      pz = pz + nz * push;
+      float vn = fminf(dot3(vx, vy, vz, nx, ny, nz), 0.0f);
+      vx = vx - nx * vn;
+      vy = vy - ny * vn;
+      vz = vz - nz * vn;
+      if (dw < P.contact_depth) {
+        uint32_t slot = atomicAdd(&S.contacts->count, 1u);
+        if (slot < 32u) S.contacts->points[slot] = make_float4(px, py, pz, len3(vx, vy, vz));
+      }
+    }
+  }
+  float clx = clampf(px, S.wlo[0], S.whi[0]), cly = clampf(py, S.wlo[1], S.whi[1]), clz = clampf(pz, S.wlo[2], S.whi[2]);
+  ParticleDev out;
+  out.a = make_float4(clx, cly, clz, mdp.x);
+  out.b = make_float4(clx == px ? vx : 0.0f, cly == py ? vy : 0.0f, clz == pz ? vz : 0.0f, mdp.y);
+  out.c = make_float4(nvx, nvy, nvz, 0.0f);
+  S.parts[S.sorted_id[k]] = out;
+}
+
 // forces (fluid.ts:370-439) fused with integrate (fluid.ts:449-491). The neighbour pass
 // reads only the cell-ordered copies made by the cell build, and writes only the particle
 // records, so no neighbour can observe a half-updated particle.
-template <bool kFast>
-__global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+//
+// kSplit leaves the integrate to k_integrate, a launch of its own: without the collider
+// sampling the neighbour loop needs fewer registers, and five blocks fit an SM instead of four.
+template <bool kFast, bool kSplit>
+__global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const SceneDev* __restrict__ scenes,
+                                                                          const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
   if (substep >= S.substeps) return;
@@ -1151,37 +1192,28 @@ __global__ void __launch_bounds__(256, 4) k_forces_integrate(const SceneDev* __r
     vy = vy * sc;
     vz = vz * sc;
   }
-  const float nvx = vx, nvy = vy, nvz = vz;
-  // integrate
-  float px = me.x + vx * P.dt, py = me.y + vy * P.dt, pz = me.z + vz * P.dt;
-  const FieldDev* world = S.world;
-  if (world && world->n > 0) {
-    float sx, sy;
-    int child = field_pick(world, px, py, pz, sx, sy);
-    float dw = sx;
-    if (dw < S.radius) {
-      float nx, ny, nz;
-      field_normal(world, child, px, py, pz, nx, ny, nz);
-      float push = S.radius - dw;
-      px = px + nx * push;
-      py = py + ny * push;
-      pz = pz + nz * push;
-      float vn = fminf(dot3(vx, vy, vz, nx, ny, nz), 0.0f);
-      vx = vx - nx * vn;
-      vy = vy - ny * vn;
-      vz = vz - nz * vn;
-      if (dw < P.contact_depth) {
-        uint32_t slot = atomicAdd(&S.contacts->count, 1u);
-        if (slot < 32u) S.contacts->points[slot] = make_float4(px, py, pz, len3(vx, vy, vz));
-      }
-    }
+  if constexpr (kSplit) {
+    // the integrate pass runs as its own launch: the new velocity waits in the first entry of
+    // this particle's neighbour list, which no other particle reads
+    reinterpret_cast<float4*>(S.nbr)[k] = make_float4(vx, vy, vz, 0.0f);
+  } else {
+    integrate_particle(S, P, k, me, mdp, vx, vy, vz);
   }
-  float clx = clampf(px, S.wlo[0], S.whi[0]), cly = clampf(py, S.wlo[1], S.whi[1]), clz = clampf(pz, S.wlo[2], S.whi[2]);
-  ParticleDev out;
-  out.a = make_float4(clx, cly, clz, mdp.x);
-  out.b = make_float4(clx == px ? vx : 0.0f, cly == py ? vy : 0.0f, clz == pz ? vz : 0.0f, mdp.y);
-  out.c = make_float4(nvx, nvy, nvz, 0.0f);
-  S.parts[S.sorted_id[k]] = out;
+}
+
+// The integrate half of a split forces pass (see k_forces_integrate), compiled with the same
+// contraction rule as the fused pass of its mode.
+template <bool kFast>
+__global__ void __launch_bounds__(256) k_integrate(const SceneDev* __restrict__ scenes, const Work* __restrict__ work,
+                                                    int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  uint32_t count = work_count(S);
+  uint32_t k = w.first + threadIdx.x;
+  if (k >= count || threadIdx.x >= w.n) return;
+  const float4 v = reinterpret_cast<const float4*>(S.nbr)[k];
+  integrate_particle(S, *S.prm, k, S.spos[k], S.sdp[k], v.x, v.y, v.z);
 }
 
 // ---------------------------------------------------------------------------------------

@@ -14,8 +14,15 @@ cudaError_t L_density_fast(const SceneDev* s, const Work* w, int blocks, int thr
   count_launch();
   return cudaPeekAtLastError();
 }
-cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
-  k_forces_integrate<true><<<blocks, threads, 0, st>>>(s, w, sub);
+cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
+                          bool split) {
+  if (split) {
+    k_forces_integrate<true, true><<<blocks, threads, 0, st>>>(s, w, sub);
+    count_launch();
+    k_integrate<true><<<blocks, threads, 0, st>>>(s, w, sub);
+  } else {
+    k_forces_integrate<true, false><<<blocks, threads, 0, st>>>(s, w, sub);
+  }
   count_launch();
   return cudaPeekAtLastError();
 }

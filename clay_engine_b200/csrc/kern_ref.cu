@@ -52,8 +52,17 @@ cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int thre
   count_launch();
   return cudaPeekAtLastError();
 }
-cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
-  CLAY_LAUNCH(k_forces_integrate<false>, blocks, threads, st, s, w, sub);
+cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
+                         bool split) {
+  if (split) {
+    k_forces_integrate<false, true><<<blocks, threads, 0, st>>>(s, w, sub);
+    count_launch();
+    k_integrate<false><<<blocks, threads, 0, st>>>(s, w, sub);
+  } else {
+    k_forces_integrate<false, false><<<blocks, threads, 0, st>>>(s, w, sub);
+  }
+  count_launch();
+  return cudaPeekAtLastError();
 }
 cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, uint32_t acc_voxels, cudaStream_t st) {
   // The splat's shared memory exceeds the default per-block limit; the opt-in is a property

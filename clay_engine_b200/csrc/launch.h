@@ -35,10 +35,13 @@ cudaError_t L_cell_order(const SceneDev* s, const Work* w, int blocks, int threa
 // `variant` selects the density variant (all give the same visiting order).
 cudaError_t L_density_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
                           int variant = kDensityVariant);
-cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+// `split`: the forces pass without the integrate, then the integrate as a second launch.
+cudaError_t L_forces_ref(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
+                         bool split = false);
 cudaError_t L_density_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
                            int variant = kDensityVariant);
-cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
+cudaError_t L_forces_fast(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st,
+                          bool split = false);
 // `blocks_y` = mip levels when w == nullptr.
 // acc_voxels: size of the shared-memory minimum tile (dynamic shared memory, 4 B per voxel).
 cudaError_t L_splat(const SplatDev* d, const Work* w, int blocks, int blocks_y, uint32_t acc_voxels, cudaStream_t st);

@@ -458,6 +458,8 @@ typedef struct clay_bucket_tuning {
                                   neighbours; 2: one loop over neighbours staged in shared memory */
   int32_t splat_tile_ratio;   /* sphere blocks take the tile walk up to this many times their pairs (6) */
   int32_t splat_walk_weight;  /* blocks take the block walk up to this many times their pairs (3) */
+  int32_t forces_split;       /* 1: the forces pass without the integrate, then the integrate as a
+                                  launch of its own; 0: one fused pass (default) */
 } clay_bucket_tuning;
 int clay_batch_set_bucket_tuning(clay_batch* b, const int64_t* upper, const clay_bucket_tuning* t, int n);
 /* No counterpart in the reference: split the scenes into `lanes` (1..8, default 1) groups of
