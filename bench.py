@@ -669,9 +669,9 @@ BYTES_PER_PARTICLE = {
     "forces_integrate": 16 + 16 + 16 + 4 + 48,  # pos, vel, density record, id in; particle record out
 }
 # DRAM bytes (read + written) per particle of one k_splat launch over the fluid surfaces (3
-# levels), from the ncu capture summarised in profiles/k_splat_batched_128_scenes.md:
-# 107,440,128 + 6,127,360 bytes for 1,940,550 particles.
-SPLAT_TRAFFIC_PER_PARTICLE = (107440128 + 6127360) / 1940550
+# levels), from one ncu capture of that launch in the 128-scene batch (dram__bytes_read.sum +
+# dram__bytes_write.sum): 107,400,960 + 6,086,144 bytes for 1,940,550 particles.
+SPLAT_TRAFFIC_PER_PARTICLE = (107400960 + 6086144) / 1940550
 
 
 def main():
