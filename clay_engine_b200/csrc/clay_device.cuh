@@ -22,7 +22,7 @@ constexpr int kSplatWarps = 8;  // warps per block of the splat pass
 constexpr int kSplatItems = 2048;  // compacted (brick, slice) items of the sphere block walk
 constexpr int kSplatStencil = 2048;  // voxel offsets of the own-box walk's stencil (8 KB of shared memory)
 constexpr int kSplatAccVoxels = 4096;   // shared-memory minimum tile of the splat pass (spheres)
-constexpr int kSplatAccVoxelsDiscs = 8192;  // the same for oriented-disc clouds (their warp walks only)
+constexpr int kSplatAccVoxelsDiscs = 4096;  // the same for oriented-disc clouds
 // the tile walk decodes items (< tile voxels x warps) by multiplication, exact below 2^16
 static_assert(kSplatAccVoxels <= 4096 && kSplatAccVoxels * kSplatWarps <= 65536, "item decode range");
 
@@ -1453,7 +1453,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     // lengths share dx*dx, dy*dy, dz*dz and dx*dx + dy*dy across the brick (the reference's
     // rounding order is kept), minima go to the shared tile as float bits (non-negative
     // floats order like their bit patterns), and the tile is turned into keys at the end.
-    if (!has_n && bnu <= min(acc_cap, static_cast<uint32_t>(kSplatAccVoxels)) && bnu * nlive <= s_cost * D.tile_ratio) {
+    if (!has_n && bnu <= acc_cap && bnu * nlive <= s_cost * D.tile_ratio) {
       extern __shared__ uint32_t s_tile[];
       const uint32_t nbu = static_cast<uint32_t>(bnu);
       for (uint32_t v = threadIdx.x; v < nbu; v += blockDim.x) s_tile[v] = 0x7f800000u;
@@ -1922,18 +1922,11 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
             if (pl >= bw) continue;
             const float t = (tx.y + ty.y) + tz.y;
             if (t >= reach2_hi) continue;
-            const int rx = static_cast<int>(ex) - 8, ry = static_cast<int>(ey) - 8, rz = static_cast<int>(ez) - 8;
-            if (use_acc) {
-              // the distance is at least the plane term: a voxel that already holds no more than
-              // it cannot be lowered (a value read before another lane lowers it only means the
-              // pair is not skipped)
-              const int a = abase + sx * rx + asy * ry + asz * rz;
-              if (has_n && s_acc[a] <= sd_bits(pl)) continue;
-              const float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
-              if (sd < bw) atomicMin(&s_acc[a], sd_bits(sd));
-            } else {
-              const float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
-              if (sd < bw) atomicMin(keys + (gbase + (sx * rx + gsy * ry + gsz * rz)), sd_bits(sd));
+            const float sd = fmaxf(pl, __fsqrt_rn(t) - radius);
+            if (sd < bw) {
+              const int rx = static_cast<int>(ex) - 8, ry = static_cast<int>(ey) - 8, rz = static_cast<int>(ez) - 8;
+              if (use_acc) atomicMin(&s_acc[abase + sx * rx + asy * ry + asz * rz], sd_bits(sd));
+              else atomicMin(keys + (gbase + (sx * rx + gsy * ry + gsz * rz)), sd_bits(sd));
             }
           }
           __syncwarp();  // the tables are rewritten for the next particle
