@@ -1555,7 +1555,17 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
         __syncthreads();
       }
       const uint32_t nwork = compact ? s_nitems : nall;
-      for (uint32_t i = threadIdx.x; i < nwork; i += blockDim.x) {
+      // Work units: the items of the last partial round are split into their slices' two halves,
+      // so that round's threads carry half an item each rather than some a whole one and the
+      // rest none; the block waits for its slowest thread at the barrier below. A voxel's
+      // minimum is the same over the halves as over the whole slice.
+      const uint32_t full = (nwork / blockDim.x) * blockDim.x;
+      const uint32_t rest = nwork - full;
+      const bool split = rest > 0 && 2u * rest <= blockDim.x;
+      const uint32_t nunits = split ? full + 2u * rest : nwork;
+      for (uint32_t u = threadIdx.x; u < nunits; u += blockDim.x) {
+        const bool half_unit = split && u >= full;
+        const uint32_t i = half_unit ? full + ((u - full) >> 1) : u;
         const uint32_t it = compact ? static_cast<uint32_t>(s_items[i]) : i;
         uint32_t sl, lx0, ly0, lz0;
         brick_of(it, sl, lx0, ly0, lz0);
@@ -1602,8 +1612,13 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
               for (int zz = 0; zz < 2; zz++) u[xx + 4 * yy + 8 * zz] = __float_as_uint(t + dz2[zz]);
             }
         };
-        const uint32_t j1 = min(nlive, (sl + 1u) * per);
+        uint32_t j1 = min(nlive, (sl + 1u) * per);
         uint32_t j = sl * per;
+        if (half_unit) {  // this unit's half of the slice
+          const uint32_t mid = j + ((j1 - min(j, j1)) >> 1);
+          if ((u - full) & 1u) j = mid;
+          else j1 = mid;
+        }
         for (; j + 1u < j1; j += 2u) {
           uint32_t ua[16], ub[16];
           lengths(s_cp[j], ua);
