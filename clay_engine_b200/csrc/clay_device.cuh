@@ -136,7 +136,9 @@ struct __align__(16) SceneDev {
   // what the forces pass reads of a neighbour, in two 16-byte records: spx = position and
   // 1/density (written by the density pass), svel = velocity and pressure (.w written by it)
   float4* spx;
-  uint4* nbr;  // accepted neighbours of the density pass, 4 per entry, slot-major: nbr[(j / 4) * capacity + k]
+  // accepted neighbours of the density pass as 16-bit offsets from the particle's own index,
+  // 8 per entry, slot-major: neighbour j of particle k is half j % 8 of nbr[(j / 8) * capacity + k]
+  uint4* nbr;
   uint32_t* counts;
   uint32_t* cell_start;
   const FieldDev* world;
@@ -972,15 +974,22 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float h2 = S.h2, mp6 = S.mass_poly6;
   float rho = 0.0f, comp = 0.0f;
   const float4* __restrict__ spos = S.spos;
-  // The accepted neighbours, in visiting order, for the forces pass: entry j of particle k is
-  // word j % 4 of nbr[(j / 4) * capacity + k], so the forces pass reads 4 at a time and a
-  // warp's lanes at one slot as contiguous lines.
-  uint32_t* __restrict__ nl = reinterpret_cast<uint32_t*>(S.nbr + k);
-  const uint32_t stride = 4u * S.capacity;
+  // The accepted neighbours, in visiting order, for the forces pass, each as its offset q - k
+  // in 16 bits: entry j of particle k is half j % 8 of nbr[(j / 8) * capacity + k], so the
+  // forces pass reads 8 at a time and a warp's lanes at one slot as contiguous lines. A
+  // neighbour farther than 32,767 places in the cell order (a very large scene's next layer of
+  // cells) leaves the particle without a list: its forces pass scans the cells.
+  int16_t* __restrict__ nl = reinterpret_cast<int16_t*>(S.nbr + k);
+  const uint32_t stride = 8u * S.capacity;
   uint32_t cnt = 0;
+  bool fits = true;
   // one accepted neighbour q at squared length r2, in visiting order
   auto accept = [&](uint32_t q, float r2) {
-    if (cnt < kMaxNbr) nl[(cnt >> 2) * stride + (cnt & 3u)] = q;
+    if (cnt < kMaxNbr) {
+      const int d = static_cast<int>(q) - static_cast<int>(k);
+      fits = fits && d >= -32768 && d <= 32767;
+      nl[(cnt >> 3) * stride + (cnt & 7u)] = static_cast<int16_t>(d);
+    }
     cnt++;
     // fast mode may contract a recomputed length differently from the test: a pair at the
     // boundary then adds a term of order (h^2 * 1e-7)^3, not a missing neighbour
@@ -1039,7 +1048,8 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float stiff = S.prm->stiffness;
   const float dens = fmaxf(rho, S.rest_floor);
   const float pres = fmaxf(stiff * (rho - S.rest), 0.0f), inv = __frcp_rn(dens);
-  S.sdp[k] = make_float4(dens, pres, inv, __uint_as_float(cnt));
+  // the neighbour count for the forces pass; all bits set when the list cannot be used
+  S.sdp[k] = make_float4(dens, pres, inv, __uint_as_float(fits ? cnt : 0xffffffffu));
   // the neighbour view of this particle for the forces pass (svel is not read in this pass)
   S.spx[k] = make_float4(me.x, me.y, me.z, inv);
   S.svel[k].w = pres;
@@ -1154,11 +1164,15 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
   if (cnt <= kMaxNbr) {
     const uint4* __restrict__ nl = S.nbr + k;
     const uint32_t stride = S.capacity;
-    for (uint32_t j = 0; j < cnt; j += 4) {
-      const uint4 e = __ldg(nl + (j / 4u) * stride);
-      const uint32_t qa[4] = {e.x, e.y, e.z, e.w};
+    for (uint32_t j = 0; j < cnt; j += 8) {
+      const uint4 e = __ldg(nl + (j / 8u) * stride);
+      const uint32_t ew[4] = {e.x, e.y, e.z, e.w};
+      uint32_t qa[8];
 #pragma unroll
-      for (int g = 0; g < 4; g += kForceLoads) {
+      for (int h = 0; h < 8; h++)
+        qa[h] = k + static_cast<uint32_t>(static_cast<int>(static_cast<int16_t>((ew[h >> 1] >> (16 * (h & 1))) & 0xffffu)));
+#pragma unroll
+      for (int g = 0; g < 8; g += kForceLoads) {
         float4 o[kForceLoads], v[kForceLoads];
 #pragma unroll
         for (int u = 0; u < kForceLoads; u++) {
