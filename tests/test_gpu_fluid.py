@@ -234,3 +234,30 @@ def test_density_error_against_f64(root, oracle):
         rel = np.abs(g["density"].astype(np.float64) - d64[:, 0]) / np.abs(d64[:, 0])
         assert rel.max() <= 1e-4, f"{mode}: density rel err {rel.max():.3g}"
         sim.destroy()
+
+
+def test_neighbours_beyond_the_list_offsets_fall_back_bit_exact(root, oracle):
+    """A wide vertical sheet (130 x 130 x 4 particles, 13 m x 13 m in x and y): the cells of the
+    next z layer lie more than 32,767 places away in the cell order, beyond the neighbour
+    list's 16-bit offsets, so those particles scan the cells in the forces pass. Reference mode
+    stays bit for bit the oracle's."""
+    import numpy as np
+
+    from clay_engine_b200 import scenes
+
+    rng = np.random.default_rng(12)
+    xs = (np.arange(130) - 64.5) * 0.1
+    zs = (np.arange(4) - 1.5) * 0.1
+    z, y, x = np.meshgrid(zs, xs + 3.0, xs, indexing="ij")
+    pos = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
+    pos += rng.uniform(-0.01, 0.01, pos.shape)
+    p = np.zeros(len(pos), scenes.PARTICLE_DTYPE)
+    p["pos"] = pos.astype(np.float32)
+    p["vel"] = (0.0, -0.5, 0.2)
+    opts = dict(CFG1, capacity=len(p))
+    sim, ref, keep = make_pair(root, oracle, opts, p, with_collider=False)
+    for frame in range(2):
+        sim.step()
+        ref.step()
+        assert_state_equal(sim.download(), ref.parts, sim.particleCount, f"frame {frame}: ")
+    sim.destroy()
