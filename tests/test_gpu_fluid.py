@@ -237,18 +237,18 @@ def test_density_error_against_f64(root, oracle):
 
 
 def test_neighbours_beyond_the_list_offsets_fall_back_bit_exact(root, oracle):
-    """A wide vertical sheet (130 x 130 x 4 particles, 13 m x 13 m in x and y): the cells of the
-    next z layer lie more than 32,767 places away in the cell order, beyond the neighbour
-    list's 16-bit offsets, so those particles scan the cells in the forces pass. Reference mode
-    stays bit for bit the oracle's."""
+    """A wide vertical sheet (160 x 160 x 4 particles, 16 m x 16 m in x and y): the cells of the
+    next z layer lie about 40,000 places away in the cell order, beyond the neighbour list's
+    16-bit offsets, so those particles scan the cells in the forces pass. Reference mode stays
+    bit for bit the oracle's."""
     import numpy as np
 
     from clay_engine_b200 import scenes
 
     rng = np.random.default_rng(12)
-    xs = (np.arange(130) - 64.5) * 0.1
+    xs = (np.arange(160) - 79.5) * 0.1
     zs = (np.arange(4) - 1.5) * 0.1
-    z, y, x = np.meshgrid(zs, xs + 3.0, xs, indexing="ij")
+    z, y, x = np.meshgrid(zs, xs + 6.0, xs, indexing="ij")
     pos = np.stack([x.ravel(), y.ravel(), z.ravel()], 1)
     pos += rng.uniform(-0.01, 0.01, pos.shape)
     p = np.zeros(len(pos), scenes.PARTICLE_DTYPE)
