@@ -979,16 +979,19 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   // forces pass reads 8 at a time and a warp's lanes at one slot as contiguous lines. A
   // neighbour farther than 32,767 places in the cell order (a very large scene's next layer of
   // cells) leaves the particle without a list: its forces pass scans the cells.
-  int16_t* __restrict__ nl = reinterpret_cast<int16_t*>(S.nbr + k);
-  const uint32_t stride = 8u * S.capacity;
+  uint32_t* __restrict__ nl = reinterpret_cast<uint32_t*>(S.nbr + k);
+  const uint32_t stride = 4u * S.capacity;
   uint32_t cnt = 0;
   bool fits = true;
+  uint32_t pending = 0;  // an even entry's offset, stored with the odd one after it as one word
   // one accepted neighbour q at squared length r2, in visiting order
   auto accept = [&](uint32_t q, float r2) {
     if (cnt < kMaxNbr) {
       const int d = static_cast<int>(q) - static_cast<int>(k);
       fits = fits && d >= -32768 && d <= 32767;
-      nl[(cnt >> 3) * stride + (cnt & 7u)] = static_cast<int16_t>(d);
+      const uint32_t h = static_cast<uint32_t>(d) & 0xffffu;
+      if (cnt & 1u) nl[(cnt >> 3) * stride + ((cnt & 7u) >> 1)] = pending | (h << 16);
+      else pending = h;
     }
     cnt++;
     // fast mode may contract a recomputed length differently from the test: a pair at the
@@ -1048,6 +1051,8 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float stiff = S.prm->stiffness;
   const float dens = fmaxf(rho, S.rest_floor);
   const float pres = fmaxf(stiff * (rho - S.rest), 0.0f), inv = __frcp_rn(dens);
+  // an odd count leaves the last offset pending
+  if ((cnt & 1u) && cnt <= kMaxNbr) nl[((cnt - 1u) >> 3) * stride + (((cnt - 1u) & 7u) >> 1)] = pending;
   // the neighbour count for the forces pass; all bits set when the list cannot be used
   S.sdp[k] = make_float4(dens, pres, inv, __uint_as_float(fits ? cnt : 0xffffffffu));
   // the neighbour view of this particle for the forces pass (svel is not read in this pass)
