@@ -979,20 +979,18 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   // forces pass reads 8 at a time and a warp's lanes at one slot as contiguous lines. A
   // neighbour farther than 32,767 places in the cell order (a very large scene's next layer of
   // cells) leaves the particle without a list: its forces pass scans the cells.
-  uint32_t* __restrict__ nl = reinterpret_cast<uint32_t*>(S.nbr + k);
-  const uint32_t stride = 4u * S.capacity;
+  int16_t* __restrict__ nl = reinterpret_cast<int16_t*>(S.nbr + k);
+  const uint32_t stride = 8u * S.capacity;
   uint32_t cnt = 0;
+  // whether every candidate's offset fits 16 bits, checked once per range [s, e) (the accept
+  // path below runs for nearly every candidate of a warp, so it stays as short as it can)
   bool fits = true;
-  uint32_t pending = 0;  // an even entry's offset, stored with the odd one after it as one word
+  auto range_fits = [&](uint32_t s, uint32_t e) {
+    if (e > s) fits = fits && static_cast<int>(s) - static_cast<int>(k) >= -32768 && static_cast<int>(e - 1u) - static_cast<int>(k) <= 32767;
+  };
   // one accepted neighbour q at squared length r2, in visiting order
   auto accept = [&](uint32_t q, float r2) {
-    if (cnt < kMaxNbr) {
-      const int d = static_cast<int>(q) - static_cast<int>(k);
-      fits = fits && d >= -32768 && d <= 32767;
-      const uint32_t h = static_cast<uint32_t>(d) & 0xffffu;
-      if (cnt & 1u) nl[(cnt >> 3) * stride + ((cnt & 7u) >> 1)] = pending | (h << 16);
-      else pending = h;
-    }
+    if (cnt < kMaxNbr) nl[(cnt >> 3) * stride + (cnt & 7u)] = static_cast<int16_t>(q - k);
     cnt++;
     // fast mode may contract a recomputed length differently from the test: a pair at the
     // boundary then adds a term of order (h^2 * 1e-7)^3, not a missing neighbour
@@ -1010,14 +1008,18 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
     }
   };
   if constexpr (kVariant == 0) {
-    for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
-      const float4 o = __ldg(spos + q);
-      const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
-      const float r2 = (dx * dx + dy * dy) + dz * dz;
-      if (r2 < h2) accept(q, r2);
+    for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int) {
+      range_fits(s, e);
+      for (uint32_t q = s; q < e; q++) {
+        const float4 o = __ldg(spos + q);
+        const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+        const float r2 = (dx * dx + dy * dy) + dz * dz;
+        if (r2 < h2) accept(q, r2);
+      }
     });
   } else if constexpr (kVariant == 2) {
     for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int r) {
+      range_fits(s, e);
       // the row's candidates [s, e) lie inside staged range r (see above): candidate q sits
       // at s_pos[q - q0 + sb], computed modulo 2^32 as q + shift
       const uint32_t shift = staged ? s_sb[r] - s_q0[r] : 0u;
@@ -1029,6 +1031,7 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
       }
     });
   } else for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int) {
+    range_fits(s, e);
     for (uint32_t base = s; base < e; base += 32u) {
       const uint32_t n = min(32u, e - base);
       uint32_t m = 0;
@@ -1051,8 +1054,6 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float stiff = S.prm->stiffness;
   const float dens = fmaxf(rho, S.rest_floor);
   const float pres = fmaxf(stiff * (rho - S.rest), 0.0f), inv = __frcp_rn(dens);
-  // an odd count leaves the last offset pending
-  if ((cnt & 1u) && cnt <= kMaxNbr) nl[((cnt - 1u) >> 3) * stride + (((cnt - 1u) & 7u) >> 1)] = pending;
   // the neighbour count for the forces pass; all bits set when the list cannot be used
   S.sdp[k] = make_float4(dens, pres, inv, __uint_as_float(fits ? cnt : 0xffffffffu));
   // the neighbour view of this particle for the forces pass (svel is not read in this pass)
