@@ -992,10 +992,12 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   auto accept = [&](uint32_t q, float r2) {
     if (cnt < kMaxNbr) nl[(cnt >> 3) * stride + (cnt & 7u)] = static_cast<int16_t>(q - k);
     cnt++;
-    // fast mode may contract a recomputed length differently from the test: a pair at the
-    // boundary then adds a term of order (h^2 * 1e-7)^3, not a missing neighbour
-    const float wv = fmaxf(h2 - r2, 0.0f);
-    const float term = mp6 * ((wv * wv) * wv);
+    // variant 1 recomputes the length: fast mode may contract it differently from the test,
+    // and a pair at the boundary then adds a term of order (h^2 * 1e-7)^3, not a missing one
+    const float wv = kVariant == 1 ? fmaxf(h2 - r2, 0.0f) : h2 - r2;
+    // fast mode sums (h^2 - r^2)^3 and scales the sum by mass * poly6 once at the end; the
+    // reference mode scales every term, as the reference does
+    const float term = kFast ? (wv * wv) * wv : mp6 * ((wv * wv) * wv);
     if (kFast) {
       // Kahan: explicit round-to-nearest operations so nothing is contracted into an FMA
       // (every term is positive, so the running sum bounds each term after the first)
@@ -1050,7 +1052,7 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
       }
     }
   });
-  if (kFast) rho = __fsub_rn(rho, comp);
+  if (kFast) rho = mp6 * __fsub_rn(rho, comp);
   const float stiff = S.prm->stiffness;
   const float dens = fmaxf(rho, S.rest_floor);
   const float pres = fmaxf(stiff * (rho - S.rest), 0.0f), inv = __frcp_rn(dens);
