@@ -957,7 +957,7 @@ int clay_fluid_estimate_bytes(const clay_fluid_opts* opts, uint64_t* out) {
   // the allocations of clay_fluid_create: per particle, per grid cell, fixed, then the surface
   const uint64_t C = static_cast<uint64_t>(f.capacity);
   const uint64_t cells = static_cast<uint64_t>(f.G) * f.G * f.G;
-  uint64_t b = C * (sizeof(ParticleDev) + 4 * sizeof(uint32_t) + 4 * sizeof(float4) + (kMaxNbr / 8) * sizeof(uint4)) +
+  uint64_t b = C * (sizeof(ParticleDev) + 4 * sizeof(uint32_t) + 4 * sizeof(float4) + (kMaxNbr / 4) * sizeof(uint4)) +
                (cells + 1) * sizeof(uint32_t) + (cells + 2) * sizeof(uint32_t) + sizeof(ParamsDev) + sizeof(ContactsDev) +
                sizeof(GridState) + sizeof(SceneDev);
   uint64_t t = 0;
@@ -1017,7 +1017,7 @@ int clay_fluid_create(clay_ctx* ctx, const clay_field* world, const clay_fluid_o
       (rc = f->alloc(&f->gs, 1)) || (rc = f->alloc(&f->hs.key, C)) || (rc = f->alloc(&f->hs.rank, C)) ||
       (rc = f->alloc(&f->hs.tmp, C)) || (rc = f->alloc(&f->hs.sorted_id, C)) || (rc = f->alloc(&f->hs.spos, C)) ||
       (rc = f->alloc(&f->hs.svel, C)) || (rc = f->alloc(&f->hs.sdp, C)) || (rc = f->alloc(&f->hs.spx, C)) ||
-      (rc = f->alloc(&f->hs.nbr, C * (kMaxNbr / 8))) ||
+      (rc = f->alloc(&f->hs.nbr, C * (kMaxNbr / 4))) ||
       (rc = f->alloc(&f->hs.counts, cells + 1)) || (rc = f->alloc(&f->hs.cell_start, cells + 2)) ||
       (rc = f->alloc(&f->d_scene, 1))) {
     clay_fluid_destroy(f);

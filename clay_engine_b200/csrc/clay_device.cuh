@@ -136,9 +136,7 @@ struct __align__(16) SceneDev {
   // what the forces pass reads of a neighbour, in two 16-byte records: spx = position and
   // 1/density (written by the density pass), svel = velocity and pressure (.w written by it)
   float4* spx;
-  // accepted neighbours of the density pass as 16-bit offsets from the particle's own index,
-  // 8 per entry, slot-major: neighbour j of particle k is half j % 8 of nbr[(j / 8) * capacity + k]
-  uint4* nbr;
+  uint4* nbr;  // accepted neighbours of the density pass, 4 per entry, slot-major: nbr[(j / 4) * capacity + k]
   uint32_t* counts;
   uint32_t* cell_start;
   const FieldDev* world;
@@ -974,23 +972,15 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float h2 = S.h2, mp6 = S.mass_poly6;
   float rho = 0.0f, comp = 0.0f;
   const float4* __restrict__ spos = S.spos;
-  // The accepted neighbours, in visiting order, for the forces pass, each as its offset q - k
-  // in 16 bits: entry j of particle k is half j % 8 of nbr[(j / 8) * capacity + k], so the
-  // forces pass reads 8 at a time and a warp's lanes at one slot as contiguous lines. A
-  // neighbour farther than 32,767 places in the cell order (a very large scene's next layer of
-  // cells) leaves the particle without a list: its forces pass scans the cells.
-  int16_t* __restrict__ nl = reinterpret_cast<int16_t*>(S.nbr + k);
-  const uint32_t stride = 8u * S.capacity;
+  // The accepted neighbours, in visiting order, for the forces pass: entry j of particle k is
+  // word j % 4 of nbr[(j / 4) * capacity + k], so the forces pass reads 4 at a time and a
+  // warp's lanes at one slot as contiguous lines.
+  uint32_t* __restrict__ nl = reinterpret_cast<uint32_t*>(S.nbr + k);
+  const uint32_t stride = 4u * S.capacity;
   uint32_t cnt = 0;
-  // whether every candidate's offset fits 16 bits, checked once per range [s, e) (the accept
-  // path below runs for nearly every candidate of a warp, so it stays as short as it can)
-  bool fits = true;
-  auto range_fits = [&](uint32_t s, uint32_t e) {
-    if (e > s) fits = fits && static_cast<int>(s) - static_cast<int>(k) >= -32768 && static_cast<int>(e - 1u) - static_cast<int>(k) <= 32767;
-  };
   // one accepted neighbour q at squared length r2, in visiting order
   auto accept = [&](uint32_t q, float r2) {
-    if (cnt < kMaxNbr) nl[(cnt >> 3) * stride + (cnt & 7u)] = static_cast<int16_t>(q - k);
+    if (cnt < kMaxNbr) nl[(cnt >> 2) * stride + (cnt & 3u)] = q;
     cnt++;
     // variant 1 recomputes the length: fast mode may contract it differently from the test,
     // and a pair at the boundary then adds a term of order (h^2 * 1e-7)^3, not a missing one
@@ -1010,18 +1000,14 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
     }
   };
   if constexpr (kVariant == 0) {
-    for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int) {
-      range_fits(s, e);
-      for (uint32_t q = s; q < e; q++) {
-        const float4 o = __ldg(spos + q);
-        const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
-        const float r2 = (dx * dx + dy * dy) + dz * dz;
-        if (r2 < h2) accept(q, r2);
-      }
+    for_neighbours(S, b, overflow, cx, cy, cz, [&](uint32_t q) {
+      const float4 o = __ldg(spos + q);
+      const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+      const float r2 = (dx * dx + dy * dy) + dz * dz;
+      if (r2 < h2) accept(q, r2);
     });
   } else if constexpr (kVariant == 2) {
     for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int r) {
-      range_fits(s, e);
       // the row's candidates [s, e) lie inside staged range r (see above): candidate q sits
       // at s_pos[q - q0 + sb], computed modulo 2^32 as q + shift
       const uint32_t shift = staged ? s_sb[r] - s_q0[r] : 0u;
@@ -1033,7 +1019,6 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
       }
     });
   } else for_neighbour_ranges(S, b, overflow, cx, cy, cz, [&](uint32_t s, uint32_t e, int) {
-    range_fits(s, e);
     for (uint32_t base = s; base < e; base += 32u) {
       const uint32_t n = min(32u, e - base);
       uint32_t m = 0;
@@ -1056,8 +1041,7 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float stiff = S.prm->stiffness;
   const float dens = fmaxf(rho, S.rest_floor);
   const float pres = fmaxf(stiff * (rho - S.rest), 0.0f), inv = __frcp_rn(dens);
-  // the neighbour count for the forces pass; all bits set when the list cannot be used
-  S.sdp[k] = make_float4(dens, pres, inv, __uint_as_float(fits ? cnt : 0xffffffffu));
+  S.sdp[k] = make_float4(dens, pres, inv, __uint_as_float(cnt));
   // the neighbour view of this particle for the forces pass (svel is not read in this pass)
   S.spx[k] = make_float4(me.x, me.y, me.z, inv);
   S.svel[k].w = pres;
@@ -1155,6 +1139,29 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
       fz = fz - (dz * ir) * s;
     }
   };
+  // Fast mode, a neighbour from the list: the density pass accepted it (r^2 < h^2, up to how
+  // each pass contracts the length: a pair on the boundary adds a term of order
+  // (h^2 * 1e-7)^3), and the particle itself is on its own list at r = 0, where its XSPH
+  // term is the (h^2)^3 the reference starts the sums with and no pressure force applies. So
+  // the list loop tests neither q == k nor r^2 < h^2.
+  auto accum_listed = [&](const float4 o, const float4 ov) {
+    const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
+    const float r2 = (dx * dx + dy * dy) + dz * dz;
+    const float w0 = h2 - r2;
+    const float wv = (w0 * w0) * w0;
+    vsx = vsx + ov.x * wv;
+    vsy = vsy + ov.y * wv;
+    vsz = vsz + ov.z * wv;
+    wsum = wsum + wv;
+    if (r2 > 1e-12f) {  // r > 1e-6
+      const float irs = rsqrtf(r2);
+      const float hr = h - r2 * irs;
+      const float s = mass * (mp + ov.w) * 0.5f * o.w * spiky * (hr * hr);
+      fx = fx - (dx * irs) * s;
+      fy = fy - (dy * irs) * s;
+      fz = fz - (dz * irs) * s;
+    }
+  };
   auto pair = [&](uint32_t q) {
     if (q == k) return;
     const float4 o = __ldg(spx + q);
@@ -1172,15 +1179,17 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
   if (cnt <= kMaxNbr) {
     const uint4* __restrict__ nl = S.nbr + k;
     const uint32_t stride = S.capacity;
-    for (uint32_t j = 0; j < cnt; j += 8) {
-      const uint4 e = __ldg(nl + (j / 8u) * stride);
-      const uint32_t ew[4] = {e.x, e.y, e.z, e.w};
-      uint32_t qa[8];
+    if (kFast) {  // the particle's own entry brings its term
+      vsx = 0.0f;
+      vsy = 0.0f;
+      vsz = 0.0f;
+      wsum = 0.0f;
+    }
+    for (uint32_t j = 0; j < cnt; j += 4) {
+      const uint4 e = __ldg(nl + (j / 4u) * stride);
+      const uint32_t qa[4] = {e.x, e.y, e.z, e.w};
 #pragma unroll
-      for (int h = 0; h < 8; h++)
-        qa[h] = k + static_cast<uint32_t>(static_cast<int>(static_cast<int16_t>((ew[h >> 1] >> (16 * (h & 1))) & 0xffffu)));
-#pragma unroll
-      for (int g = 0; g < 8; g += kForceLoads) {
+      for (int g = 0; g < 4; g += kForceLoads) {
         float4 o[kForceLoads], v[kForceLoads];
 #pragma unroll
         for (int u = 0; u < kForceLoads; u++) {
@@ -1190,8 +1199,12 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
           }
         }
 #pragma unroll
-        for (int u = 0; u < kForceLoads; u++)
-          if (j + g + u < cnt) accum(qa[g + u], o[u], v[u]);
+        for (int u = 0; u < kForceLoads; u++) {
+          if (j + g + u < cnt) {
+            if (kFast) accum_listed(o[u], v[u]);
+            else accum(qa[g + u], o[u], v[u]);
+          }
+        }
       }
     }
   } else {

@@ -33,17 +33,17 @@ def test_autotune_buckets():
     assert all(autotune.DEFAULT[k] in v for k, v in autotune.KNOBS.items())
 
 
-def test_estimate_counts_256_bytes_per_particle():
+def test_estimate_counts_384_bytes_per_particle():
     """Per particle a scene holds its 48-byte record, key/rank/scratch/order words (16 B), four
     cell-ordered float4 copies (position, velocity, density record, neighbour view: 64 B) and the
-    64-slot neighbour list of 16-bit offsets (128 B)."""
+    64-slot neighbour list (256 B)."""
     from clay_engine_b200 import core
 
     base = dict(spacing=0.1, radius=0.05, substeps=2, worldSize=24.0, origin=(-12.0, -4.0, -12.0),
                 bakeResolution=64, bakeMipLevels=3, bakeBand=4.0)
     a = core.fluid_estimate_bytes(dict(base, capacity=1000))
     b = core.fluid_estimate_bytes(dict(base, capacity=3000))
-    assert b - a == 2000 * 256
+    assert b - a == 2000 * 384
     c = core.fluid_estimate_bytes(dict(base, capacity=1000, bakeResolution=128, bakeMipLevels=4))
     voxels = lambda r, m: sum((r >> i) ** 3 for i in range(m))
     assert c - a == (voxels(128, 4) - voxels(64, 3)) * 8  # f16 distance + f16 material + u32 scratch
