@@ -236,11 +236,11 @@ def test_density_error_against_f64(root, oracle):
         sim.destroy()
 
 
-def test_neighbours_beyond_the_list_offsets_fall_back_bit_exact(root, oracle):
-    """A wide vertical sheet (160 x 160 x 4 particles, 16 m x 16 m in x and y): the cells of the
-    next z layer lie about 40,000 places away in the cell order, beyond the neighbour list's
-    16-bit offsets, so those particles scan the cells in the forces pass. Reference mode stays
-    bit for bit the oracle's."""
+def test_wide_sheet_bit_exact(root, oracle):
+    """A wide vertical sheet (160 x 160 x 4 particles, 16 m x 16 m in x and y): a particle's
+    neighbours in the next z layer of cells lie about 40,000 places away from it in the cell
+    order, and its nine neighbour rows span a box of occupied cells 160 wide. Reference mode
+    stays bit for bit the oracle's."""
     import numpy as np
 
     from clay_engine_b200 import scenes
