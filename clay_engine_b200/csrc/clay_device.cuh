@@ -1144,6 +1144,9 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
   // (h^2 * 1e-7)^3), and the particle itself is on its own list at r = 0, where its XSPH
   // term is the (h^2)^3 the reference starts the sums with and no pressure force applies. So
   // the list loop tests neither q == k nor r^2 < h^2.
+  // The pressure factor mass * (p_i + p_j) / 2 / rho_j * spiky * (h - r)^2 / r is formed with
+  // the constants folded into one (fast mode rounds it differently from the reference's order).
+  const float half_mass_spiky = (mass * 0.5f) * spiky;
   auto accum_listed = [&](const float4 o, const float4 ov) {
     const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
     const float r2 = (dx * dx + dy * dy) + dz * dz;
@@ -1156,10 +1159,10 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
     if (r2 > 1e-12f) {  // r > 1e-6
       const float irs = rsqrtf(r2);
       const float hr = h - r2 * irs;
-      const float s = mass * (mp + ov.w) * 0.5f * o.w * spiky * (hr * hr);
-      fx = fx - (dx * irs) * s;
-      fy = fy - (dy * irs) * s;
-      fz = fz - (dz * irs) * s;
+      const float t = half_mass_spiky * ((mp + ov.w) * o.w) * ((hr * hr) * irs);
+      fx = fx - dx * t;
+      fy = fy - dy * t;
+      fz = fz - dz * t;
     }
   };
   auto pair = [&](uint32_t q) {
@@ -1185,7 +1188,9 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
       vsz = 0.0f;
       wsum = 0.0f;
     }
-    for (uint32_t j = 0; j < cnt; j += 4) {
+    // the entries of slot j / 4 below `lim` (entries past the count hold no index); the full
+    // slots pass lim = 4, which needs no test once the lambda is inlined
+    auto slot = [&](uint32_t j, uint32_t lim) {
       const uint4 e = __ldg(nl + (j / 4u) * stride);
       const uint32_t qa[4] = {e.x, e.y, e.z, e.w};
 #pragma unroll
@@ -1193,20 +1198,23 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
         float4 o[kForceLoads], v[kForceLoads];
 #pragma unroll
         for (int u = 0; u < kForceLoads; u++) {
-          if (j + g + u < cnt) {  // entries past the count hold no index
+          if (static_cast<uint32_t>(g + u) < lim) {
             o[u] = __ldg(spx + qa[g + u]);
             v[u] = __ldg(svel + qa[g + u]);
           }
         }
 #pragma unroll
         for (int u = 0; u < kForceLoads; u++) {
-          if (j + g + u < cnt) {
+          if (static_cast<uint32_t>(g + u) < lim) {
             if (kFast) accum_listed(o[u], v[u]);
             else accum(qa[g + u], o[u], v[u]);
           }
         }
       }
-    }
+    };
+    uint32_t j = 0;
+    for (; j + 4u <= cnt; j += 4) slot(j, 4u);
+    if (j < cnt) slot(j, cnt - j);
   } else {
     for_neighbours(S, b, overflow, cx, cy, cz, pair);
   }
