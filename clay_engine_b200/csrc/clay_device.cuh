@@ -1042,9 +1042,11 @@ __global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__
   const float dens = fmaxf(rho, S.rest_floor);
   const float pres = fmaxf(stiff * (rho - S.rest), 0.0f), inv = __frcp_rn(dens);
   S.sdp[k] = make_float4(dens, pres, inv, __uint_as_float(cnt));
-  // the neighbour view of this particle for the forces pass (svel is not read in this pass)
+  // the neighbour view of this particle for the forces pass (svel is not read in this pass);
+  // fast mode stores p / rho beside the velocity, so that the forces pass forms a neighbour's
+  // (p_i + p_j) / rho_j as one multiply-add, p_i * (1 / rho_j) + p_j / rho_j
   S.spx[k] = make_float4(me.x, me.y, me.z, inv);
-  S.svel[k].w = pres;
+  S.svel[k].w = kFast ? pres * inv : pres;
 }
 
 // integrate (fluid.ts:449-491) of cell-ordered particle k: advance with the new velocity, collide
@@ -1114,7 +1116,11 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
   float wsum = S.h6;
   const float4* __restrict__ spx = S.spx;
   const float4* __restrict__ svel = S.svel;
-  // one neighbour q: o = position and 1/density, ov = velocity and pressure
+  // Fast mode forms the pressure factor mass * (p_i + p_j) / 2 / rho_j * spiky * (h - r)^2 / r
+  // with the constants folded into one and (p_i + p_j) / rho_j = p_i * (1 / rho_j) + p_j / rho_j
+  // (the density pass stored p_j / rho_j), rounding differently from the reference's order.
+  const float half_mass_spiky = (mass * 0.5f) * spiky;
+  // one neighbour q: o = position and 1/density, ov = velocity and pressure (p / rho in fast mode)
   auto accum = [&](uint32_t q, const float4 o, const float4 ov) {
     if (q == k) return;
     float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
@@ -1132,7 +1138,7 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
     const float r = kFast ? r2 * irs : __fsqrt_rn(r2);
     if (r > 1e-6f) {
       float hr = h - r;
-      float s = mass * (mp + ov.w) * 0.5f * inv * spiky * (hr * hr);
+      float s = kFast ? half_mass_spiky * fmaf(mp, inv, ov.w) * (hr * hr) : mass * (mp + ov.w) * 0.5f * inv * spiky * (hr * hr);
       float ir = kFast ? irs : __frcp_rn(r);
       fx = fx - (dx * ir) * s;
       fy = fy - (dy * ir) * s;
@@ -1144,9 +1150,6 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
   // (h^2 * 1e-7)^3), and the particle itself is on its own list at r = 0, where its XSPH
   // term is the (h^2)^3 the reference starts the sums with and no pressure force applies. So
   // the list loop tests neither q == k nor r^2 < h^2.
-  // The pressure factor mass * (p_i + p_j) / 2 / rho_j * spiky * (h - r)^2 / r is formed with
-  // the constants folded into one (fast mode rounds it differently from the reference's order).
-  const float half_mass_spiky = (mass * 0.5f) * spiky;
   auto accum_listed = [&](const float4 o, const float4 ov) {
     const float dx = me.x - o.x, dy = me.y - o.y, dz = me.z - o.z;
     const float r2 = (dx * dx + dy * dy) + dz * dz;
@@ -1159,7 +1162,7 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
     if (r2 > 1e-12f) {  // r > 1e-6
       const float irs = rsqrtf(r2);
       const float hr = h - r2 * irs;
-      const float t = half_mass_spiky * ((mp + ov.w) * o.w) * ((hr * hr) * irs);
+      const float t = half_mass_spiky * fmaf(mp, o.w, ov.w) * ((hr * hr) * irs);
       fx = fx - dx * t;
       fy = fy - dy * t;
       fz = fz - dz * t;
