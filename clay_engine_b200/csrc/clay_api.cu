@@ -1243,13 +1243,10 @@ int clay_fluid_download(const clay_fluid* f, clay_fluid_particle* host, int64_t 
   return CLAY_OK;
 }
 
-int clay_fluid_cell_indices(clay_fluid* f, uint32_t* host, void* stream) {
-  if (!f || !host) return fail(CLAY_EINVAL, "clay_fluid_cell_indices: NULL argument");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (f->live == 0) return CLAY_OK;
-  TempDev<uint32_t> d;
-  CK(d.alloc(static_cast<size_t>(f->live)));
-  // the uniform's count must be current for the kernel
+// The sim's own uniform with its current live count, for the hooks that launch on the sim's
+// own scene record: a batch steps the sim through the batch's copy of the uniform, so the
+// sim's own may hold an older count.
+static int fluid_sync_count(clay_fluid* f, cudaStream_t s) {
   clay_fluid_params p = f->frozen;
   p.count = static_cast<uint32_t>(f->live);
   p.emit_base = static_cast<uint32_t>(f->cursor);
@@ -1260,6 +1257,17 @@ int clay_fluid_cell_indices(clay_fluid* f, uint32_t* host, void* stream) {
     f->written = p;
     f->written_valid = true;
   }
+  return CLAY_OK;
+}
+
+int clay_fluid_cell_indices(clay_fluid* f, uint32_t* host, void* stream) {
+  if (!f || !host) return fail(CLAY_EINVAL, "clay_fluid_cell_indices: NULL argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (f->live == 0) return CLAY_OK;
+  TempDev<uint32_t> d;
+  CK(d.alloc(static_cast<size_t>(f->live)));
+  int rc = fluid_sync_count(f, s);
+  if (rc) return rc;
   CK(L_cell_index(f->d_scene, d.p, static_cast<int>(f->live), s));
   CK(cudaMemcpyAsync(host, d.p, sizeof(uint32_t) * f->live, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -1284,11 +1292,13 @@ int clay_fluid_census(clay_fluid* f, void* stream, clay_census* out) {
   out->particles = static_cast<uint64_t>(f->live);
   if (f->live == 0) return CLAY_OK;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int rc = fluid_sync_count(f, s);
+  if (rc) return rc;
   TempDev<unsigned long long> d;
   CK(d.alloc(3));
   CK(cudaMemsetAsync(d.p, 0, 3 * sizeof(unsigned long long), s));
   CK(L_census_nbr(f->d_scene, static_cast<int>(f->live), d.p, s));
-  int rc = census_splat(f->surface, d.p + 2, s);
+  rc = census_splat(f->surface, d.p + 2, s);
   if (rc) return rc;
   unsigned long long h[3] = {0, 0, 0};
   CK(cudaMemcpyAsync(h, d.p, sizeof(h), cudaMemcpyDeviceToHost, s));

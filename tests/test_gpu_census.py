@@ -88,3 +88,28 @@ def test_splat_census_counts_the_bake_pairs(root):
     s = ce.SplatField(root, cloud, radius=0.11, resolution=64, mipLevels=2, band=4.0, worldSize=24.0, origin=ORIGIN)
     assert s.census() == brute_splat_pairs(pos, 64, 2, 4.0, 0.11, 24.0, ORIGIN)
     s.destroy()
+
+
+def test_fluid_census_after_batched_frames(root):
+    """A sim stepped only through a Batch (whose frames read the batch's copy of every scene's
+    uniform, not the sim's own) reports the census of the same sim stepped alone."""
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    opts = dict(capacity=4096, spacing=0.1, radius=0.05, substeps=2, gravity=(0, -9.8, 0), bakeResolution=64,
+                bakeMipLevels=3, bakeBand=4.0, worldSize=24.0, origin=ORIGIN)
+    p = scenes.jittered_lattice(16, 0.1, (0.0, 3.0, 0.0), 1)
+    p["vel"] = (0.3, -1.0, 0.1)
+    alone, batched = ce.FluidSim(root, None, opts), ce.FluidSim(root, None, opts)
+    alone.upload(p)
+    batched.upload(p)
+    batch = ce.Batch(root, [batched])
+    for _ in range(2):
+        alone.step()
+        batch.step()
+    a, b = alone.census(), batched.census()
+    assert a["candidates"] > 4096 * 20 and a["splat_pairs"] > 4096 * 100
+    assert a == b
+    batch.destroy()
+    alone.destroy()
+    batched.destroy()
