@@ -22,6 +22,7 @@ constexpr int kSplatWarps = 8;  // warps per block of the splat pass
 constexpr int kSplatItems = 2048;  // compacted (brick, slice) items of the sphere block walk
 constexpr int kSplatStencil = 2048;  // voxel offsets of the own-box walk's stencil (8 KB of shared memory)
 constexpr int kSplatAccVoxels = 4096;   // shared-memory minimum tile of the splat pass (spheres)
+constexpr int kSplatSubtiles = 8;       // sub-boxes of that tile a sphere block's union box may take
 constexpr int kSplatAccVoxelsDiscs = 4096;  // the same for oriented-disc clouds
 // the tile walk decodes items (< tile voxels x warps) by multiplication, exact below 2^16
 static_assert(kSplatAccVoxels <= 4096 && kSplatAccVoxels * kSplatWarps <= 65536, "item decode range");
@@ -1494,18 +1495,18 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     // their relative cost (the block walk's pair is ~3x cheaper for spheres, ~1.5x for discs)
     const uint64_t lhs = bnu * nlive * (has_n ? 2ull : 1ull);
     const uint64_t rhs = s_cost * D.walk_weight;
-    // Spheres, union box within the shared tile: register-blocked block walk. A work item is
-    // a brick of 4 x 2 x 2 voxels against a slice of the block's particles; the squared
-    // lengths share dx*dx, dy*dy, dz*dz and dx*dx + dy*dy across the brick (the reference's
-    // rounding order is kept), minima go to the shared tile as float bits (non-negative
-    // floats order like their bit patterns), and the tile is turned into keys at the end.
-    if (!has_n && bnu <= acc_cap && bnu * nlive <= s_cost * D.tile_ratio) {
+    // Spheres: register-blocked block walk. A work item is a brick of 4 x 2 x 2 voxels against
+    // a slice of the block's particles; the squared lengths share dx*dx, dy*dy, dz*dz and
+    // dx*dx + dy*dy across the brick (the reference's rounding order is kept), minima go to the
+    // shared tile as float bits (non-negative floats order like their bit patterns), and the
+    // tile is turned into keys at the end. A union box larger than the tile (a block whose
+    // particles cross from one layer of cells to the next, or a splash) is walked as sub-boxes
+    // of at most acc_cap voxels, one after another through the same tile: every brick still
+    // meets only the slices within reach of it, and a voxel's minimum is the same.
+    const bool tile_fits = bnu <= acc_cap;
+    const bool subtiled = !tile_fits && bnu <= static_cast<uint64_t>(kSplatSubtiles) * acc_cap && bnx * 4u <= acc_cap;
+    if (!has_n && ((tile_fits && bnu * nlive <= s_cost * D.tile_ratio) || subtiled)) {
       extern __shared__ uint32_t s_tile[];
-      const uint32_t nbu = static_cast<uint32_t>(bnu);
-      for (uint32_t v = threadIdx.x; v < nbu; v += blockDim.x) s_tile[v] = 0x7f800000u;
-      const uint32_t ux = static_cast<uint32_t>(bnx), uy = static_cast<uint32_t>(bny), uz = static_cast<uint32_t>(bnz);
-      const uint32_t ngx = (ux + 3u) >> 2, ngy = (uy + 1u) >> 1, ngz = (uz + 1u) >> 1;
-      const uint32_t ngroups = ngx * ngy * ngz;
       // slices of ~32 consecutive (cell-ordered, so spatially close) particles, each with its
       // own bounding box: a brick out of reach of a slice's box skips that slice
       const uint32_t nsl = max(1u, (nlive + 31u) >> 5);  // <= kSplatWarps
@@ -1545,160 +1546,194 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       const float cull2 = cull * cull;
       __shared__ uint16_t s_items[kSplatItems];
       __shared__ uint32_t s_nitems;
-      if (threadIdx.x == 0) s_nitems = 0u;
-      __syncthreads();
-      const uint32_t nall = ngroups * nsl;
-      // Item decode by multiplication: for x < 2^16 and 1 <= d < 2^15, floor(x * ceil(2^32 / d)
-      // / 2^32) == x / d (the excess x * (ceil - 2^32 / d) / 2^32 stays below 2^-16 < 1 / d).
-      // Items number below ngroups * nsl <= 4096 * 8 and tile voxels below 4096, so every
-      // operand is in range.
-      const uint64_t m_groups = static_cast<uint64_t>(0xffffffffu / ngroups) + 1u;
-      const uint64_t m_gx = static_cast<uint64_t>(0xffffffffu / ngx) + 1u;
-      const uint64_t m_gy = static_cast<uint64_t>(0xffffffffu / ngy) + 1u;
-      const uint64_t m_ux = static_cast<uint64_t>(0xffffffffu / ux) + 1u;
-      const uint64_t m_uy = static_cast<uint64_t>(0xffffffffu / uy) + 1u;
       auto divm = [](uint32_t x, uint64_t m) { return static_cast<uint32_t>((static_cast<uint64_t>(x) * m) >> 32); };
-      auto brick_of = [&](uint32_t it, uint32_t& sl, uint32_t& lx0, uint32_t& ly0, uint32_t& lz0) {
-        sl = divm(it, m_groups);
-        const uint32_t g = it - sl * ngroups;
-        const uint32_t rest = divm(g, m_gx);
-        lx0 = (g - rest * ngx) * 4u;  // brick corner in the union box
-        const uint32_t rz = divm(rest, m_gy);
-        ly0 = (rest - rz * ngy) * 2u;
-        lz0 = rz * 2u;
-      };
-      // a brick farther than the reach from a slice's bounding box: nothing to lower
-      auto culled = [&](uint32_t sl, uint32_t lx0, uint32_t ly0, uint32_t lz0) {
-        const float* sb = s_sb[sl];
-        const float x0f = (static_cast<float>(bx0 + static_cast<int>(lx0)) + 0.5f) * voxel;
-        const float y0f = (static_cast<float>(by0 + static_cast<int>(ly0)) + 0.5f) * voxel;
-        const float z0f = (static_cast<float>(bz0 + static_cast<int>(lz0)) + 0.5f) * voxel;
-        const float x1f = (static_cast<float>(bx0 + static_cast<int>(lx0) + 3) + 0.5f) * voxel;
-        const float y1f = (static_cast<float>(by0 + static_cast<int>(ly0) + 1) + 0.5f) * voxel;
-        const float z1f = (static_cast<float>(bz0 + static_cast<int>(lz0) + 1) + 0.5f) * voxel;
-        const float ex = fmaxf(fmaxf(sb[0] - x1f, x0f - sb[3]), 0.0f);
-        const float ey = fmaxf(fmaxf(sb[1] - y1f, y0f - sb[4]), 0.0f);
-        const float ez = fmaxf(fmaxf(sb[2] - z1f, z0f - sb[5]), 0.0f);
-        return ex * ex + ey * ey + ez * ez > cull2;
-      };
-      // the (brick, slice) items that survive the cull, compacted so that lanes stay busy
-      const bool compact = nall <= static_cast<uint32_t>(kSplatItems);
-      if (compact) {
-        for (uint32_t base = 0; base < nall; base += blockDim.x) {
-          const uint32_t it = base + threadIdx.x;
-          bool keep = false;
-          if (it < nall) {
-            uint32_t sl, lx0, ly0, lz0;
-            brick_of(it, sl, lx0, ly0, lz0);
-            keep = !culled(sl, lx0, ly0, lz0);
-          }
-          const uint32_t m = __ballot_sync(0xffffffffu, keep);
-          uint32_t o = 0;
-          if (lane == 0 && m) o = atomicAdd(&s_nitems, static_cast<uint32_t>(__popc(m)));
-          o = __shfl_sync(0xffffffffu, o, 0);
-          if (keep) s_items[o + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(it);
-        }
-        __syncthreads();
+      // Sub-boxes: the full x extent (at most acc_cap / 4 voxels, checked above) times an even
+      // number of rows and of layers, so that bricks never straddle two sub-boxes and each
+      // sub-box holds at most acc_cap voxels.
+      // The sub-box being walked lives in shared memory (its first row and layer in the union
+      // box, and the rows and layers per sub-box), so that no loop state stays in registers
+      // through the walk.
+      __shared__ uint32_t s_subbox[4];
+      if (threadIdx.x == 0) {
+        const uint32_t fx = static_cast<uint32_t>(bnx), fy = static_cast<uint32_t>(bny), fz = static_cast<uint32_t>(bnz);
+        const uint32_t sub_y = tile_fits ? fy : min(fy, max(2u, (acc_cap / (2u * fx)) & ~1u));
+        s_subbox[0] = 0u;
+        s_subbox[1] = 0u;
+        s_subbox[2] = sub_y;
+        s_subbox[3] = tile_fits ? fz : min(fz, max(2u, (acc_cap / (fx * sub_y)) & ~1u));
       }
-      const uint32_t nwork = compact ? s_nitems : nall;
-      // Work units: the items of the last partial round are split into their slices' two halves,
-      // so that round's threads carry half an item each rather than some a whole one and the
-      // rest none; the block waits for its slowest thread at the barrier below. A voxel's
-      // minimum is the same over the halves as over the whole slice.
-      const uint32_t full = (nwork / blockDim.x) * blockDim.x;
-      const uint32_t rest = nwork - full;
-      const bool split = rest > 0 && 2u * rest <= blockDim.x;
-      const uint32_t nunits = split ? full + 2u * rest : nwork;
-      for (uint32_t u = threadIdx.x; u < nunits; u += blockDim.x) {
-        const bool half_unit = split && u >= full;
-        const uint32_t i = half_unit ? full + ((u - full) >> 1) : u;
-        const uint32_t it = compact ? static_cast<uint32_t>(s_items[i]) : i;
-        uint32_t sl, lx0, ly0, lz0;
-        brick_of(it, sl, lx0, ly0, lz0);
-        if (!compact && culled(sl, lx0, ly0, lz0)) continue;
-        const int x0 = bx0 + static_cast<int>(lx0), y0 = by0 + static_cast<int>(ly0), z0 = bz0 + static_cast<int>(lz0);
-        // voxel centres (x + 0.5) * voxel: one conversion per axis, since float(x0) + (k + 0.5)
-        // equals float(x0 + k) + 0.5 exactly for grid coordinates (integers far below 2^23)
-        float cx[4], cy[2], cz[2];
-        const float fx0 = static_cast<float>(x0), fy0 = static_cast<float>(y0), fz0 = static_cast<float>(z0);
-#pragma unroll
-        for (int k = 0; k < 4; k++) cx[k] = (fx0 + (static_cast<float>(k) + 0.5f)) * voxel;
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-          cy[k] = (fy0 + (static_cast<float>(k) + 0.5f)) * voxel;
-          cz[k] = (fz0 + (static_cast<float>(k) + 0.5f)) * voxel;
-        }
-        // Minima of squared lengths as float bits (non-negative floats order like their bit
-        // patterns), two particles per step: the squared lengths keep the reference's rounding
-        // order (dx*dx + dy*dy) + dz*dz, and one three-input minimum folds both particles into
-        // a voxel's running minimum.
-        uint32_t b[16];
-#pragma unroll
-        for (int k = 0; k < 16; k++) b[k] = 0x7f800000u;
-        // the 16 squared lengths of one particle, indexed xx + 4 * yy + 8 * zz
-        auto lengths = [&](const float4 q, uint32_t (&u)[16]) {
-          float dx2[4], dy2[2], dz2[2];
-#pragma unroll
-          for (int k = 0; k < 4; k++) {
-            const float d = cx[k] - q.x;
-            dx2[k] = d * d;
+      for (;;) {
+        __syncthreads();  // the previous sub-box's write-out has read the tile; the next one is published
+        const uint32_t oy = s_subbox[0], oz = s_subbox[1];
+        const uint32_t ux = static_cast<uint32_t>(s_box[3] - s_box[0] + 1);
+        const uint32_t fy = static_cast<uint32_t>(s_box[4] - s_box[1] + 1), fz = static_cast<uint32_t>(s_box[5] - s_box[2] + 1);
+        if (oz >= fz) break;
+        const int bx0 = s_box[0], by0 = s_box[1] + static_cast<int>(oy), bz0 = s_box[2] + static_cast<int>(oz);
+        const uint32_t uy = min(s_subbox[2], fy - oy), uz = min(s_subbox[3], fz - oz);
+        const uint32_t nbu = ux * uy * uz;
+        for (uint32_t v = threadIdx.x; v < nbu; v += blockDim.x) s_tile[v] = 0x7f800000u;
+        const uint32_t ngx = (ux + 3u) >> 2, ngy = (uy + 1u) >> 1, ngz = (uz + 1u) >> 1;
+        const uint32_t ngroups = ngx * ngy * ngz;
+        if (threadIdx.x == 0) s_nitems = 0u;
+        __syncthreads();
+        const uint32_t nall = ngroups * nsl;
+        // Item decode by multiplication: for x < 2^16 and 1 <= d < 2^15, floor(x * ceil(2^32 / d)
+        // / 2^32) == x / d (the excess x * (ceil - 2^32 / d) / 2^32 stays below 2^-16 < 1 / d).
+        // Items number below ngroups * nsl <= 4096 * 8 and tile voxels below 4096, so every
+        // operand is in range.
+        const uint64_t m_groups = static_cast<uint64_t>(0xffffffffu / ngroups) + 1u;
+        const uint64_t m_gx = static_cast<uint64_t>(0xffffffffu / ngx) + 1u;
+        const uint64_t m_gy = static_cast<uint64_t>(0xffffffffu / ngy) + 1u;
+        const uint64_t m_ux = static_cast<uint64_t>(0xffffffffu / ux) + 1u;
+        const uint64_t m_uy = static_cast<uint64_t>(0xffffffffu / uy) + 1u;
+        auto brick_of = [&](uint32_t it, uint32_t& sl, uint32_t& lx0, uint32_t& ly0, uint32_t& lz0) {
+          sl = divm(it, m_groups);
+          const uint32_t g = it - sl * ngroups;
+          const uint32_t rest = divm(g, m_gx);
+          lx0 = (g - rest * ngx) * 4u;  // brick corner in the union box
+          const uint32_t rz = divm(rest, m_gy);
+          ly0 = (rest - rz * ngy) * 2u;
+          lz0 = rz * 2u;
+        };
+        // a brick farther than the reach from a slice's bounding box: nothing to lower
+        auto culled = [&](uint32_t sl, uint32_t lx0, uint32_t ly0, uint32_t lz0) {
+          const float* sb = s_sb[sl];
+          const float x0f = (static_cast<float>(bx0 + static_cast<int>(lx0)) + 0.5f) * voxel;
+          const float y0f = (static_cast<float>(by0 + static_cast<int>(ly0)) + 0.5f) * voxel;
+          const float z0f = (static_cast<float>(bz0 + static_cast<int>(lz0)) + 0.5f) * voxel;
+          const float x1f = (static_cast<float>(bx0 + static_cast<int>(lx0) + 3) + 0.5f) * voxel;
+          const float y1f = (static_cast<float>(by0 + static_cast<int>(ly0) + 1) + 0.5f) * voxel;
+          const float z1f = (static_cast<float>(bz0 + static_cast<int>(lz0) + 1) + 0.5f) * voxel;
+          const float ex = fmaxf(fmaxf(sb[0] - x1f, x0f - sb[3]), 0.0f);
+          const float ey = fmaxf(fmaxf(sb[1] - y1f, y0f - sb[4]), 0.0f);
+          const float ez = fmaxf(fmaxf(sb[2] - z1f, z0f - sb[5]), 0.0f);
+          return ex * ex + ey * ey + ez * ez > cull2;
+        };
+        // the (brick, slice) items that survive the cull, compacted so that lanes stay busy
+        const bool compact = nall <= static_cast<uint32_t>(kSplatItems);
+        if (compact) {
+          for (uint32_t base = 0; base < nall; base += blockDim.x) {
+            const uint32_t it = base + threadIdx.x;
+            bool keep = false;
+            if (it < nall) {
+              uint32_t sl, lx0, ly0, lz0;
+              brick_of(it, sl, lx0, ly0, lz0);
+              keep = !culled(sl, lx0, ly0, lz0);
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, keep);
+            uint32_t o = 0;
+            if (lane == 0 && m) o = atomicAdd(&s_nitems, static_cast<uint32_t>(__popc(m)));
+            o = __shfl_sync(0xffffffffu, o, 0);
+            if (keep) s_items[o + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(it);
           }
+          __syncthreads();
+        }
+        const uint32_t nwork = compact ? s_nitems : nall;
+        // Work units: the items of the last partial round are split into their slices' two halves,
+        // so that round's threads carry half an item each rather than some a whole one and the
+        // rest none; the block waits for its slowest thread at the barrier below. A voxel's
+        // minimum is the same over the halves as over the whole slice.
+        const uint32_t full = (nwork / blockDim.x) * blockDim.x;
+        const uint32_t rest = nwork - full;
+        const bool split = rest > 0 && 2u * rest <= blockDim.x;
+        const uint32_t nunits = split ? full + 2u * rest : nwork;
+        for (uint32_t u = threadIdx.x; u < nunits; u += blockDim.x) {
+          const bool half_unit = split && u >= full;
+          const uint32_t i = half_unit ? full + ((u - full) >> 1) : u;
+          const uint32_t it = compact ? static_cast<uint32_t>(s_items[i]) : i;
+          uint32_t sl, lx0, ly0, lz0;
+          brick_of(it, sl, lx0, ly0, lz0);
+          if (!compact && culled(sl, lx0, ly0, lz0)) continue;
+          const int x0 = bx0 + static_cast<int>(lx0), y0 = by0 + static_cast<int>(ly0), z0 = bz0 + static_cast<int>(lz0);
+          // voxel centres (x + 0.5) * voxel: one conversion per axis, since float(x0) + (k + 0.5)
+          // equals float(x0 + k) + 0.5 exactly for grid coordinates (integers far below 2^23)
+          float cx[4], cy[2], cz[2];
+          const float fx0 = static_cast<float>(x0), fy0 = static_cast<float>(y0), fz0 = static_cast<float>(z0);
+#pragma unroll
+          for (int k = 0; k < 4; k++) cx[k] = (fx0 + (static_cast<float>(k) + 0.5f)) * voxel;
 #pragma unroll
           for (int k = 0; k < 2; k++) {
-            const float dy = cy[k] - q.y, dz = cz[k] - q.z;
-            dy2[k] = dy * dy;
-            dz2[k] = dz * dz;
+            cy[k] = (fy0 + (static_cast<float>(k) + 0.5f)) * voxel;
+            cz[k] = (fz0 + (static_cast<float>(k) + 0.5f)) * voxel;
+          }
+          // Minima of squared lengths as float bits (non-negative floats order like their bit
+          // patterns), two particles per step: the squared lengths keep the reference's rounding
+          // order (dx*dx + dy*dy) + dz*dz, and one three-input minimum folds both particles into
+          // a voxel's running minimum.
+          uint32_t b[16];
+#pragma unroll
+          for (int k = 0; k < 16; k++) b[k] = 0x7f800000u;
+          // the 16 squared lengths of one particle, indexed xx + 4 * yy + 8 * zz
+          auto lengths = [&](const float4 q, uint32_t (&u)[16]) {
+            float dx2[4], dy2[2], dz2[2];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+              const float d = cx[k] - q.x;
+              dx2[k] = d * d;
+            }
+#pragma unroll
+            for (int k = 0; k < 2; k++) {
+              const float dy = cy[k] - q.y, dz = cz[k] - q.z;
+              dy2[k] = dy * dy;
+              dz2[k] = dz * dz;
+            }
+#pragma unroll
+            for (int yy = 0; yy < 2; yy++)
+#pragma unroll
+              for (int xx = 0; xx < 4; xx++) {
+                const float t = dx2[xx] + dy2[yy];
+#pragma unroll
+                for (int zz = 0; zz < 2; zz++) u[xx + 4 * yy + 8 * zz] = __float_as_uint(t + dz2[zz]);
+              }
+          };
+          uint32_t j1 = min(nlive, (sl + 1u) * per);
+          uint32_t j = sl * per;
+          if (half_unit) {  // this unit's half of the slice
+            const uint32_t mid = j + ((j1 - min(j, j1)) >> 1);
+            if ((u - full) & 1u) j = mid;
+            else j1 = mid;
+          }
+          for (; j + 1u < j1; j += 2u) {
+            uint32_t ua[16], ub[16];
+            lengths(s_cp[j], ua);
+            lengths(s_cp[j + 1u], ub);
+#pragma unroll
+            for (int k = 0; k < 16; k++) b[k] = __vimin3_u32(b[k], ua[k], ub[k]);
+          }
+          if (j < j1) {
+            uint32_t ua[16];
+            lengths(s_cp[j], ua);
+#pragma unroll
+            for (int k = 0; k < 16; k++) b[k] = min(b[k], ua[k]);
           }
 #pragma unroll
-          for (int yy = 0; yy < 2; yy++)
+          for (int zz = 0; zz < 2; zz++)
 #pragma unroll
-            for (int xx = 0; xx < 4; xx++) {
-              const float t = dx2[xx] + dy2[yy];
+            for (int yy = 0; yy < 2; yy++)
 #pragma unroll
-              for (int zz = 0; zz < 2; zz++) u[xx + 4 * yy + 8 * zz] = __float_as_uint(t + dz2[zz]);
-            }
-        };
-        uint32_t j1 = min(nlive, (sl + 1u) * per);
-        uint32_t j = sl * per;
-        if (half_unit) {  // this unit's half of the slice
-          const uint32_t mid = j + ((j1 - min(j, j1)) >> 1);
-          if ((u - full) & 1u) j = mid;
-          else j1 = mid;
+              for (int xx = 0; xx < 4; xx++) {
+                const uint32_t lx = lx0 + xx, ly = ly0 + yy, lz = lz0 + zz;
+                const uint32_t v = b[xx + 4 * yy + 8 * zz];
+                if (lx < ux && ly < uy && lz < uz && v < 0x7f800000u) atomicMin(&s_tile[lx + ux * (ly + uy * lz)], v);
+              }
         }
-        for (; j + 1u < j1; j += 2u) {
-          uint32_t ua[16], ub[16];
-          lengths(s_cp[j], ua);
-          lengths(s_cp[j + 1u], ub);
-#pragma unroll
-          for (int k = 0; k < 16; k++) b[k] = __vimin3_u32(b[k], ua[k], ub[k]);
+        __syncthreads();
+        for (uint32_t v = threadIdx.x; v < nbu; v += blockDim.x) {
+          const uint32_t bits = s_tile[v];
+          if (bits == 0x7f800000u) continue;
+          const float sd = __fsqrt_rn(__uint_as_float(bits)) - radius;
+          if (sd < bw) {
+            const uint32_t vy = divm(v, m_ux), vz = divm(vy, m_uy);  // v < 4096: decode by multiplication
+            const int x = bx0 + static_cast<int>(v - vy * ux), y = by0 + static_cast<int>(vy - vz * uy), z = bz0 + static_cast<int>(vz);
+            atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
+                      sd_bits(sd));
+          }
         }
-        if (j < j1) {
-          uint32_t ua[16];
-          lengths(s_cp[j], ua);
-#pragma unroll
-          for (int k = 0; k < 16; k++) b[k] = min(b[k], ua[k]);
-        }
-#pragma unroll
-        for (int zz = 0; zz < 2; zz++)
-#pragma unroll
-          for (int yy = 0; yy < 2; yy++)
-#pragma unroll
-            for (int xx = 0; xx < 4; xx++) {
-              const uint32_t lx = lx0 + xx, ly = ly0 + yy, lz = lz0 + zz;
-              const uint32_t v = b[xx + 4 * yy + 8 * zz];
-              if (lx < ux && ly < uy && lz < uz && v < 0x7f800000u) atomicMin(&s_tile[lx + ux * (ly + uy * lz)], v);
-            }
-      }
-      __syncthreads();
-      for (uint32_t v = threadIdx.x; v < nbu; v += blockDim.x) {
-        const uint32_t bits = s_tile[v];
-        if (bits == 0x7f800000u) continue;
-        const float sd = __fsqrt_rn(__uint_as_float(bits)) - radius;
-        if (sd < bw) {
-          const uint32_t vy = divm(v, m_ux), vz = divm(vy, m_uy);  // v < 4096: decode by multiplication
-          const int x = bx0 + static_cast<int>(v - vy * ux), y = by0 + static_cast<int>(vy - vz * uy), z = bz0 + static_cast<int>(vz);
-          atomicMin(keys + (static_cast<long long>(x) + static_cast<long long>(R) * (y + static_cast<long long>(R) * z)),
-                    sd_bits(sd));
+        if (threadIdx.x == 0) {  // the next sub-box: along y, then along z
+          const uint32_t ny = s_subbox[0] + s_subbox[2];
+          const bool wrap = ny >= static_cast<uint32_t>(s_box[4] - s_box[1] + 1);
+          s_subbox[0] = wrap ? 0u : ny;
+          s_subbox[1] = wrap ? s_subbox[1] + s_subbox[3] : s_subbox[1];
         }
       }
       return;
@@ -2055,7 +2090,7 @@ __device__ __forceinline__ void resolve_block(const SplatDev& D, const Work w) {
 }
 
 #ifndef CLAY_ONLY_NEIGHBOUR_PASSES
-__global__ void __launch_bounds__(32 * kSplatWarps) k_splat(const SplatDev* __restrict__ splats, const Work* __restrict__ work,
+__global__ void __launch_bounds__(32 * kSplatWarps, 4) k_splat(const SplatDev* __restrict__ splats, const Work* __restrict__ work,
                                                              uint32_t acc_cap) {
   const Work w = get_work(work);
   const SplatDev& D = splats[w.obj];

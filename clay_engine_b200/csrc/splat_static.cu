@@ -46,7 +46,7 @@ __global__ void k_static_clear(uint32_t* __restrict__ keys, long long n) {
   if (i < n) keys[i] = kNoHit;
 }
 
-__global__ void __launch_bounds__(32 * kSplatWarps) k_static_splat(const __grid_constant__ SplatDev D, float ox, float oy,
+__global__ void __launch_bounds__(32 * kSplatWarps, 4) k_static_splat(const __grid_constant__ SplatDev D, float ox, float oy,
                                                                      float oz) {
   Work w;
   w.obj = 0;

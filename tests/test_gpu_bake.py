@@ -105,6 +105,20 @@ def test_sparse_incoherent_cloud(root, oracle):
     assert_bake_equal(bake_both(root, oracle, p, 0.5, 32, 2, 2.0))
 
 
+def test_blocks_whose_union_box_exceeds_the_shared_tile(root, oracle):
+    """Consecutive particles alternate between small clusters far apart, so a block's union box
+    at level 0 spans several shared tiles (up to the sub-box limit, and beyond it for the wider
+    spacing): the walk goes through the box in sub-boxes of the tile, or falls back to the
+    other walks, and the keys stay the oracle's."""
+    rng = np.random.default_rng(21)
+    for span in ((8.0, 0.0, 4.0), (10.0, 2.0, 6.0), (20.0, 6.0, 20.0)):
+        n = 4096
+        k = np.arange(n)
+        corner = np.stack([(k % 2) * span[0], ((k // 2) % 2) * span[1], ((k // 4) % 2) * span[2]], 1)
+        pos = (rng.normal(size=(n, 3)) * 0.3 + corner + (-8.0, -2.0, -8.0)).astype(np.float32)
+        assert_bake_equal(bake_both(root, oracle, pos, 0.11, 64, 3, 4.0))
+
+
 @pytest.mark.parametrize("band", [2.0, 4.0])
 def test_band_and_radius(root, oracle, band):
     p = fluid_blob(8, 0.3, center=(1.0, 2.0, -1.0), seed=5)
