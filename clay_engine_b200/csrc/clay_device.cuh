@@ -1366,7 +1366,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   __shared__ float4 s_cp[32 * kSplatWarps];
   __shared__ float4 s_cn[32 * kSplatWarps];
   __shared__ int s_box[6];
-  __shared__ float s_pb[6];  // bounding box of the block's live particle positions
+  __shared__ float s_wb[kSplatWarps][6];  // bounding box of each warp's live particle positions
   __shared__ unsigned long long s_cost;
   __shared__ uint32_t s_woff[kSplatWarps];
   __shared__ uint32_t s_nlive;
@@ -1414,7 +1414,6 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   s_lo[wid][lane] = make_int4(lx, ly, lz, 0);
   s_hi[wid][lane] = make_int4(hx, hy, hz, 0);
   if (threadIdx.x < 6) s_box[threadIdx.x] = threadIdx.x < 3 ? 0x7fffffff : -1;
-  if (threadIdx.x < 6) reinterpret_cast<int*>(s_pb)[threadIdx.x] = threadIdx.x < 3 ? 0x7fffffff : (-0x7fffffff - 1);
   if (threadIdx.x == 0) s_cost = 0ull;
   __syncthreads();
   // warp then block union box, live counts and the sum of the particles' own box sizes
@@ -1429,7 +1428,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   const uint32_t cost_ind = __reduce_add_sync(0xffffffffu, (own + 31u) >> 5);
   const uint32_t wsum = __reduce_add_sync(0xffffffffu, own);
   {
-    // particle bounding box: warp reduction, then one float min/max per warp in shared memory
+    // the warp's particle bounding box (+inf / -inf when it has no live particle)
     float a0 = live ? px : __int_as_float(0x7f800000), a1 = live ? py : __int_as_float(0x7f800000),
           a2 = live ? pz : __int_as_float(0x7f800000);
     float b0 = live ? px : -__int_as_float(0x7f800000), b1 = live ? py : -__int_as_float(0x7f800000),
@@ -1443,15 +1442,13 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       b1 = fmaxf(b1, __shfl_xor_sync(0xffffffffu, b1, o));
       b2 = fmaxf(b2, __shfl_xor_sync(0xffffffffu, b2, o));
     }
-    if (lane == 0 && active) {
-      // positions are finite for live particles; order-preserving integer min/max of floats
-      auto okey = [](float f) { int i = __float_as_int(f); return i >= 0 ? i : i ^ 0x7fffffff; };
-      atomicMin(reinterpret_cast<int*>(&s_pb[0]), okey(a0));
-      atomicMin(reinterpret_cast<int*>(&s_pb[1]), okey(a1));
-      atomicMin(reinterpret_cast<int*>(&s_pb[2]), okey(a2));
-      atomicMax(reinterpret_cast<int*>(&s_pb[3]), okey(b0));
-      atomicMax(reinterpret_cast<int*>(&s_pb[4]), okey(b1));
-      atomicMax(reinterpret_cast<int*>(&s_pb[5]), okey(b2));
+    if (lane == 0) {
+      s_wb[wid][0] = a0;
+      s_wb[wid][1] = a1;
+      s_wb[wid][2] = a2;
+      s_wb[wid][3] = b0;
+      s_wb[wid][4] = b1;
+      s_wb[wid][5] = b2;
     }
   }
   if (lane == 0) {
@@ -1480,7 +1477,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
   if (live) {
     uint32_t slot = s_woff[wid] + __popc(active & ((1u << lane) - 1u));
     s_cp[slot] = make_float4(px, py, pz, 0.0f);
-    s_cn[slot] = make_float4(nx, ny, nz, 0.0f);
+    if (has_n) s_cn[slot] = make_float4(nx, ny, nz, 0.0f);
   }
   __syncthreads();
   const uint32_t nlive = s_nlive;
@@ -1512,34 +1509,40 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       const uint32_t nsl = max(1u, (nlive + 31u) >> 5);  // <= kSplatWarps
       const uint32_t per = (nlive + nsl - 1u) / nsl;
       __shared__ float s_sb[kSplatWarps][6];
+      // with every particle of the block live, slice k is warp k and its box is the warp's
+      const bool warp_slices = nlive == 32u * kSplatWarps;
       if (static_cast<uint32_t>(wid) < nsl) {
-        const uint32_t j0 = static_cast<uint32_t>(wid) * per, j1 = min(nlive, j0 + per);
-        float a0 = __int_as_float(0x7f800000), a1 = a0, a2 = a0, b0 = -a0, b1 = -a0, b2 = -a0;
-        for (uint32_t j = j0 + lane; j < j1; j += 32) {
-          const float4 q = s_cp[j];
-          a0 = fminf(a0, q.x);
-          a1 = fminf(a1, q.y);
-          a2 = fminf(a2, q.z);
-          b0 = fmaxf(b0, q.x);
-          b1 = fmaxf(b1, q.y);
-          b2 = fmaxf(b2, q.z);
-        }
+        if (warp_slices) {
+          if (lane < 6) s_sb[wid][lane] = s_wb[wid][lane];
+        } else {
+          const uint32_t j0 = static_cast<uint32_t>(wid) * per, j1 = min(nlive, j0 + per);
+          float a0 = __int_as_float(0x7f800000), a1 = a0, a2 = a0, b0 = -a0, b1 = -a0, b2 = -a0;
+          for (uint32_t j = j0 + lane; j < j1; j += 32) {
+            const float4 q = s_cp[j];
+            a0 = fminf(a0, q.x);
+            a1 = fminf(a1, q.y);
+            a2 = fminf(a2, q.z);
+            b0 = fmaxf(b0, q.x);
+            b1 = fmaxf(b1, q.y);
+            b2 = fmaxf(b2, q.z);
+          }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          a0 = fminf(a0, __shfl_xor_sync(0xffffffffu, a0, o));
-          a1 = fminf(a1, __shfl_xor_sync(0xffffffffu, a1, o));
-          a2 = fminf(a2, __shfl_xor_sync(0xffffffffu, a2, o));
-          b0 = fmaxf(b0, __shfl_xor_sync(0xffffffffu, b0, o));
-          b1 = fmaxf(b1, __shfl_xor_sync(0xffffffffu, b1, o));
-          b2 = fmaxf(b2, __shfl_xor_sync(0xffffffffu, b2, o));
-        }
-        if (lane == 0) {
-          s_sb[wid][0] = a0;
-          s_sb[wid][1] = a1;
-          s_sb[wid][2] = a2;
-          s_sb[wid][3] = b0;
-          s_sb[wid][4] = b1;
-          s_sb[wid][5] = b2;
+          for (int o = 16; o > 0; o >>= 1) {
+            a0 = fminf(a0, __shfl_xor_sync(0xffffffffu, a0, o));
+            a1 = fminf(a1, __shfl_xor_sync(0xffffffffu, a1, o));
+            a2 = fminf(a2, __shfl_xor_sync(0xffffffffu, a2, o));
+            b0 = fmaxf(b0, __shfl_xor_sync(0xffffffffu, b0, o));
+            b1 = fmaxf(b1, __shfl_xor_sync(0xffffffffu, b1, o));
+            b2 = fmaxf(b2, __shfl_xor_sync(0xffffffffu, b2, o));
+          }
+          if (lane == 0) {
+            s_sb[wid][0] = a0;
+            s_sb[wid][1] = a1;
+            s_sb[wid][2] = a2;
+            s_sb[wid][3] = b0;
+            s_sb[wid][4] = b1;
+            s_sb[wid][5] = b2;
+          }
         }
       }
       const float cull = reach * 1.0001f + 1e-5f;
@@ -1612,19 +1615,53 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
         // the (brick, slice) items that survive the cull, compacted so that lanes stay busy
         const bool compact = nall <= static_cast<uint32_t>(kSplatItems);
         if (compact) {
-          for (uint32_t base = 0; base < nall; base += blockDim.x) {
-            const uint32_t it = base + threadIdx.x;
-            bool keep = false;
-            if (it < nall) {
-              uint32_t sl, lx0, ly0, lz0;
-              brick_of(it, sl, lx0, ly0, lz0);
-              keep = !culled(sl, lx0, ly0, lz0);
+          // One thread per row of bricks along x (a slice, a row and a layer of bricks): the
+          // y and z parts of the cull are formed once per row, then each brick of the row takes
+          // the same test as culled() (the same operations, so the same survivors). The row's
+          // survivors are counted, placed after the warp's earlier rows by a warp scan and one
+          // atomic per warp, and written (the items' order does not change any minimum).
+          const uint32_t nyz = ngy * ngz, nrows = nyz * nsl;
+          const uint64_t m_yz = static_cast<uint64_t>(0xffffffffu / nyz) + 1u;
+          for (uint32_t base = 0; base < nrows; base += blockDim.x) {
+            const uint32_t r = base + threadIdx.x;
+            uint32_t sl = 0, gyz = 0, keep = 0;
+            float ey2 = 0.0f, ez2 = 0.0f;
+            const float* sb = s_sb[0];
+            auto row_keeps = [&](uint32_t gx) {
+              const float x0f = (static_cast<float>(bx0 + static_cast<int>(gx * 4u)) + 0.5f) * voxel;
+              const float x1f = (static_cast<float>(bx0 + static_cast<int>(gx * 4u) + 3) + 0.5f) * voxel;
+              const float ex = fmaxf(fmaxf(sb[0] - x1f, x0f - sb[3]), 0.0f);
+              return !(ex * ex + ey2 + ez2 > cull2);
+            };
+            if (r < nrows) {
+              sl = divm(r, m_yz);
+              gyz = r - sl * nyz;
+              const uint32_t gz = divm(gyz, m_gy), gy = gyz - gz * ngy;
+              sb = s_sb[sl];
+              const float y0f = (static_cast<float>(by0 + static_cast<int>(gy * 2u)) + 0.5f) * voxel;
+              const float z0f = (static_cast<float>(bz0 + static_cast<int>(gz * 2u)) + 0.5f) * voxel;
+              const float y1f = (static_cast<float>(by0 + static_cast<int>(gy * 2u) + 1) + 0.5f) * voxel;
+              const float z1f = (static_cast<float>(bz0 + static_cast<int>(gz * 2u) + 1) + 0.5f) * voxel;
+              const float ey = fmaxf(fmaxf(sb[1] - y1f, y0f - sb[4]), 0.0f);
+              const float ez = fmaxf(fmaxf(sb[2] - z1f, z0f - sb[5]), 0.0f);
+              ey2 = ey * ey;
+              ez2 = ez * ez;
+              for (uint32_t gx = 0; gx < ngx; gx++) keep += row_keeps(gx) ? 1u : 0u;
             }
-            const uint32_t m = __ballot_sync(0xffffffffu, keep);
+            uint32_t incl = keep;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+              const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+              if (lane >= static_cast<uint32_t>(o)) incl += y;
+            }
             uint32_t o = 0;
-            if (lane == 0 && m) o = atomicAdd(&s_nitems, static_cast<uint32_t>(__popc(m)));
-            o = __shfl_sync(0xffffffffu, o, 0);
-            if (keep) s_items[o + __popc(m & ((1u << lane) - 1u))] = static_cast<uint16_t>(it);
+            if (lane == 31 && incl) o = atomicAdd(&s_nitems, incl);
+            o = __shfl_sync(0xffffffffu, o, 31) + incl - keep;
+            if (keep) {
+              const uint32_t it0 = sl * ngroups + ngx * gyz;
+              for (uint32_t gx = 0; gx < ngx; gx++)
+                if (row_keeps(gx)) s_items[o++] = static_cast<uint16_t>(it0 + gx);
+            }
           }
           __syncthreads();
         }
@@ -1742,10 +1779,16 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
       const uint32_t ngx = static_cast<uint32_t>((bnx + 3) >> 2);
       const uint32_t ngroups = ngx * static_cast<uint32_t>(bny * bnz);
       const int bhx = s_box[3];
-      auto ofloat = [](int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7fffffff); };
-      const int* pbk = reinterpret_cast<const int*>(s_pb);
-      const float pbx0 = ofloat(pbk[0]), pby0 = ofloat(pbk[1]), pbz0 = ofloat(pbk[2]);
-      const float pbx1 = ofloat(pbk[3]), pby1 = ofloat(pbk[4]), pbz1 = ofloat(pbk[5]);
+      // the block's particle bounding box from its warps' boxes
+      float pbx0 = s_wb[0][0], pby0 = s_wb[0][1], pbz0 = s_wb[0][2], pbx1 = s_wb[0][3], pby1 = s_wb[0][4], pbz1 = s_wb[0][5];
+      for (int k = 1; k < kSplatWarps; k++) {
+        pbx0 = fminf(pbx0, s_wb[k][0]);
+        pby0 = fminf(pby0, s_wb[k][1]);
+        pbz0 = fminf(pbz0, s_wb[k][2]);
+        pbx1 = fmaxf(pbx1, s_wb[k][3]);
+        pby1 = fmaxf(pby1, s_wb[k][4]);
+        pbz1 = fmaxf(pbz1, s_wb[k][5]);
+      }
       // A group of voxels farther than the reach from the particles' bounding box cannot be
       // lowered by any of them (sd >= bandWorld): skipped. The 1e-4 margin covers f32 rounding.
       const float cull = reach * 1.0001f + 1e-5f;
