@@ -670,8 +670,8 @@ BYTES_PER_PARTICLE = {
 }
 # DRAM bytes (read + written) per particle of one k_splat launch over the fluid surfaces (3
 # levels), from one ncu capture of that launch in the 128-scene batch (dram__bytes_read.sum +
-# dram__bytes_write.sum): 107,400,960 + 6,086,144 bytes for 1,940,550 particles.
-SPLAT_TRAFFIC_PER_PARTICLE = (107400960 + 6086144) / 1940550
+# dram__bytes_write.sum): 107,473,408 + 5,515,008 bytes for 1,940,550 particles.
+SPLAT_TRAFFIC_PER_PARTICLE = (107473408 + 5515008) / 1940550
 
 
 def main():
