@@ -938,7 +938,7 @@ constexpr int kDensityStage = 3040;  // staged neighbour positions per block (47
 //    positions, copied into shared memory once per block when they fit (else the block reads
 //    through the cache as variant 0 does).
 template <bool kFast, int kVariant>
-__global__ void __launch_bounds__(256, 4) k_density(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+__global__ void __launch_bounds__(256, 5) k_density(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
   if (substep >= S.substeps) return;
