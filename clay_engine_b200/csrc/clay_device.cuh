@@ -504,6 +504,19 @@ __device__ __forceinline__ Work get_work(const Work* work) {
   return w;
 }
 
+// The same work, the blocks taken in reverse order: a pass that reads what the previous pass
+// wrote (in forward block order) starts on the part written last, which is still in L2.
+__device__ __forceinline__ Work get_work_reversed(const Work* work) {
+  const uint32_t b = gridDim.x - 1u - blockIdx.x;
+  if (work) return work[b];
+  Work w;
+  w.obj = 0;
+  w.sub = blockIdx.y;
+  w.first = b * blockDim.x;
+  w.n = blockDim.x;
+  return w;
+}
+
 // cellOf (fluid.ts:253-257).
 __device__ __forceinline__ void cell_of(const SceneDev& S, float px, float py, float pz, int& cx, int& cy, int& cz) {
   cx = f2i(floorf((px - S.gorig[0]) * S.inv_h));
@@ -939,7 +952,7 @@ constexpr int kDensityStage = 3040;  // staged neighbour positions per block (47
 //    through the cache as variant 0 does).
 template <bool kFast, int kVariant>
 __global__ void __launch_bounds__(256, 5) k_density(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
-  Work w = get_work(work);
+  Work w = get_work_reversed(work);
   const SceneDev& S = scenes[w.obj];
   if (substep >= S.substeps) return;
   uint32_t count = work_count(S);
@@ -2174,7 +2187,7 @@ __device__ __forceinline__ void resolve_block(const SplatDev& D, const Work w) {
 #ifndef CLAY_ONLY_NEIGHBOUR_PASSES
 __global__ void __launch_bounds__(32 * kSplatWarps, 4) k_splat(const SplatDev* __restrict__ splats, const Work* __restrict__ work,
                                                              uint32_t acc_cap) {
-  const Work w = get_work(work);
+  const Work w = get_work_reversed(work);
   const SplatDev& D = splats[w.obj];
   splat_block(D, w, D.vp->origin[0], D.vp->origin[1], D.vp->origin[2], acc_cap);
 }
