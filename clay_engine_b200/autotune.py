@@ -10,7 +10,7 @@ between code paths, so the choice is a pure timing decision.
 
 Search: coordinate descent, knob after knob, first for every bucket at once (a setting that
 differs between buckets splits a pass into one launch per distinct setting, which costs a
-little by itself, so a knob is first judged without that cost), then bucket after bucket. A
+little by itself, so a knob is first tried without that cost), then bucket after bucket. A
 candidate is timed over real batched frames (CUDA graph replays, CUDA events on the launching
 stream) from the same saved particle state, between two timings of the current choice, and
 replaces it only when it is faster than their mean by more than `min_gain` of the frame, so a
