@@ -831,15 +831,16 @@ __global__ void k_cell_order(const SceneDev* __restrict__ scenes, const Work* __
   uint32_t k = w.first + threadIdx.x;
   if (k >= count || threadIdx.x >= w.n) return;
   uint32_t id = S.tmp[k];
+  // the record is gathered before the rank loop, so its load overlaps the loop
+  const float4 pa = S.parts[id].a, pb = S.parts[id].b;
   uint32_t l = S.key[id];
   uint32_t s = S.cell_start[l], e = S.cell_start[l + 1];
   uint32_t r = 0;
   for (uint32_t q = s; q < e; q++) r += (S.tmp[q] < id) ? 1u : 0u;
   uint32_t f = s + r;
   S.sorted_id[f] = id;
-  const ParticleDev& P = S.parts[id];
-  S.spos[f] = P.a;
-  S.svel[f] = P.b;
+  S.spos[f] = pa;
+  S.svel[f] = pb;
 }
 
 #endif  // CLAY_ONLY_NEIGHBOUR_PASSES
@@ -1268,6 +1269,10 @@ __global__ void __launch_bounds__(256, kSplit ? 5 : 4) k_forces_integrate(const 
         }
       }
     };
+    // the list's slots come from DRAM (the whole batch's lists do not fit in L2): ask for all of
+    // them at once, so that each slot's load waits on L2 rather than on DRAM
+    for (uint32_t p = 0; p < cnt; p += 4)
+      asm volatile("prefetch.global.L2 [%0];" ::"l"(nl + (p / 4u) * stride));
     uint32_t j = 0;
     for (; j + 4u <= cnt; j += 4) slot(j, 4u);
     if (j < cnt) slot(j, cnt - j);
