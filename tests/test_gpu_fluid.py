@@ -261,3 +261,29 @@ def test_wide_sheet_bit_exact(root, oracle):
         ref.step()
         assert_state_equal(sim.download(), ref.parts, sim.particleCount, f"frame {frame}: ")
     sim.destroy()
+
+
+def test_upload_far_away_after_stepping_bit_exact(root, oracle):
+    """The cell build starts from a box of occupied cells that the writes of positions keep
+    (emission, the integrate, and a box pass after an upload). A sim stepped at one place and
+    then given particles at another, far outside the old box, must still sort and step them
+    exactly as the oracle does; then a spawn adds particles outside the new box too."""
+    sim, ref, keep = make_pair(root, oracle, dict(CFG1), blob(12, center=(-6.0, 2.0, -6.0)), with_collider=False)
+    for frame in range(2):
+        sim.step()
+        ref.step()
+    far = blob(12, center=(6.0, 8.0, 5.0), seed=4, vel=(0.2, -0.5, 0.1))
+    sim.upload(far)
+    ref.upload(far)
+    for frame in range(2):
+        sim.step()
+        ref.step()
+        assert_state_equal(sim.download(), ref.parts, sim.particleCount, f"after the upload, frame {frame}: ")
+    for s in (sim, ref):
+        s.spawn(64, (-8.0, 1.0, 7.0), (0.0, -1.0, 0.0))
+    for frame in range(2):
+        sim.step()
+        ref.step()
+        assert sim.particleCount == ref.live
+        assert_state_equal(sim.download(), ref.parts, sim.particleCount, f"after the spawn, frame {frame}: ")
+    sim.destroy()
