@@ -1549,7 +1549,7 @@ __device__ __forceinline__ void splat_block(const SplatDev& D, const Work w, flo
     // their relative cost (the block walk's pair is ~3x cheaper for spheres, ~1.5x for discs)
     const uint64_t lhs = bnu * nlive * (has_n ? 2ull : 1ull);
     const uint64_t rhs = s_cost * D.walk_weight;
-    // Spheres: register-blocked block walk. A work item is a brick of 4 x 2 x 2 voxels against
+    // Spheres: register-blocked tile walk. A work item is a brick of 4 x 2 x 2 voxels against
     // a slice of the block's particles; the squared lengths share dx*dx, dy*dy, dz*dz and
     // dx*dx + dy*dy across the brick (the reference's rounding order is kept), minima go to the
     // shared tile as float bits (non-negative floats order like their bit patterns), and the
