@@ -96,3 +96,38 @@ def test_body_shell_baked_in_the_batch(root):
     b.destroy()
     for x in (s1, s2, sim):
         x.destroy()
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_upload_between_batched_frames(root, use_graph):
+    """Particles uploaded into a batch's scenes between frames (as a server's re-admission or
+    a restored state does), far from where the scenes were: the batch (its graph replayed as
+    captured) and the same scenes stepped alone stay bit for bit the same."""
+    import clay_engine_b200 as ce
+    from clay_engine_b200 import scenes
+
+    counts = [900, 2500, 300]
+    alone = scene(root, counts, 30, "reference", None)
+    batch_sims = scene(root, counts, 30, "reference", None)
+    b = ce.Batch(root, batch_sims, use_graph=use_graph)
+    for _ in range(2):
+        b.step()
+        for s in alone:
+            s.step()
+    for i, (s, t) in enumerate(zip(batch_sims, alone)):
+        p = scenes.lattice_block(counts[i], 0.1, (5.0 - 4.0 * i, 9.0, -6.0 + 5.0 * i), 77 + i)
+        p["vel"] = (-0.3, 0.5, 0.2)
+        s.upload(p)
+        t.upload(p)
+    for frame in range(2):
+        b.step()
+        for s in alone:
+            s.step()
+        for s, t in zip(batch_sims, alone):
+            g, a = s.download(), t.download()
+            for name in ("pos", "vel", "density", "pressure", "nvel"):
+                assert np.array_equal(np.ascontiguousarray(g[name]).view(np.uint32),
+                                      np.ascontiguousarray(a[name]).view(np.uint32)), (frame, name)
+    b.destroy()
+    for s in alone + batch_sims:
+        s.destroy()
