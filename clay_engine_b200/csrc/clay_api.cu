@@ -13,7 +13,6 @@
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
-#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -1166,6 +1165,7 @@ int fluid_substep_plain(clay_fluid* f, cudaStream_t s, int sub) {
   const SceneDev* d = f->d_scene;
   const int T = kBlock;
   int pb = static_cast<int>((f->live + T - 1) / T);
+  CK(L_cell_key(d, nullptr, pb, T, sub, s));
   CK(L_cell_count(d, nullptr, pb, T, sub, s));
   CK(L_scan_partial(d, nullptr, static_cast<int>(f->parts_scan), sub, s));
   CK(L_scan_final(d, nullptr, static_cast<int>(f->parts_scan), sub, s));
@@ -1229,10 +1229,6 @@ int clay_fluid_upload(clay_fluid* f, const clay_fluid_particle* host, int64_t co
                 static_cast<long long>(f->capacity));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (count > 0) CK(cudaMemcpyAsync(f->parts, host, sizeof(ParticleDev) * count, cudaMemcpyHostToDevice, s));
-  // the box of occupied cells that the next cell build starts from, from the new particles
-  static_assert(offsetof(GridState, hi_inv) == offsetof(GridState, lo) + 3 * sizeof(uint32_t), "box accumulators");
-  CK(cudaMemsetAsync(reinterpret_cast<char*>(f->gs) + offsetof(GridState, lo), 0xff, 6 * sizeof(uint32_t), s));
-  CK(L_cell_box(f->d_scene, static_cast<uint32_t>(count), s));
   f->live = count;
   f->cursor = count % f->capacity;
   f->pending = 0;
@@ -1669,6 +1665,7 @@ int batch_enqueue(clay_batch* b, cudaStream_t s) {
     if (ln.n_part) {
       CK(L_emit(d, ln.w_emit, ln.n_emit, T, ls));
       for (int sub = 0; sub < b->max_substeps; sub++) {
+        for (auto& g : ln.groups) CK(L_cell_key(d, g.w, g.n, g.T, sub, ls));
         for (auto& g : ln.groups) CK(L_cell_count(d, g.w, g.n, g.T, sub, ls));
         CK(L_scan_partial(d, ln.w_scan, ln.n_scan, sub, ls));
         CK(L_scan_final(d, ln.w_scan, ln.n_scan, sub, ls));
@@ -1906,6 +1903,7 @@ int clay_batch_profile(clay_batch* b, void* stream, clay_phase_time* out, int ca
     if ((rc = timed("emit", [&] { return L_emit(d, b->w_emit, b->n_emit, T, s); }))) return rc;
     for (int sub = 0; sub < b->max_substeps; sub++) {
       for (auto& g : b->groups)
+        if ((rc = timed("cell_key", [&] { return L_cell_key(d, g.w, g.n, g.T, sub, s); }))) return rc;
       for (auto& g : b->groups)
         if ((rc = timed("cell_count", [&] { return L_cell_count(d, g.w, g.n, g.T, sub, s); }))) return rc;
       if ((rc = timed("scan_partial", [&] { return L_scan_partial(d, b->w_scan, b->n_scan, sub, s); }))) return rc;
@@ -2075,6 +2073,7 @@ int clay_batch_step_subset(clay_batch* b, const int32_t* scenes, int n, void* st
   const bool ref = b->mode == CLAY_MODE_REFERENCE;
   if (n_emit) CK(L_emit(d, W + o_emit, n_emit, T, s));
   for (int sub = 0; sub < max_sub && n_part > 0; sub++) {
+    CK(L_cell_key(d, W + o_part, n_part, T, sub, s));
     CK(L_cell_count(d, W + o_part, n_part, T, sub, s));
     CK(L_scan_partial(d, W + o_scan, n_scan, sub, s));
     CK(L_scan_final(d, W + o_scan, n_scan, sub, s));

@@ -7,8 +7,6 @@
 // neighbour passes. Kernels take a table of scenes and a table of work items, so the same
 // code runs one scene per launch (the plain path) or every scene of a batch in one launch.
 #pragma once
-#include <cooperative_groups.h>
-#include <cooperative_groups/reduce.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -524,32 +522,6 @@ __device__ __forceinline__ void cell_of(const SceneDev& S, float px, float py, f
   cz = f2i(floorf((pz - S.gorig[2]) * S.inv_h));
 }
 
-__device__ __forceinline__ bool in_grid(const SceneDev& S, int cx, int cy, int cz) {
-  return cx >= 0 && cy >= 0 && cz >= 0 && cx < S.G && cy < S.G && cz < S.G;
-}
-
-// Adds the cell of a position written for the next cell build (by emission, by the integrate
-// of the last substep, or after an upload) to the scene's accumulated box of occupied cells:
-// the warp's converged lanes reduce first and their leader takes the six atomics.
-__device__ __forceinline__ void box_accumulate(GridState* gs, bool in, int cx, int cy, int cz) {
-  namespace cg = cooperative_groups;
-  const cg::coalesced_group g = cg::coalesced_threads();
-  const uint32_t lx = cg::reduce(g, in ? static_cast<uint32_t>(cx) : 0xffffffffu, cg::less<uint32_t>());
-  const uint32_t ly = cg::reduce(g, in ? static_cast<uint32_t>(cy) : 0xffffffffu, cg::less<uint32_t>());
-  const uint32_t lz = cg::reduce(g, in ? static_cast<uint32_t>(cz) : 0xffffffffu, cg::less<uint32_t>());
-  const uint32_t hx = cg::reduce(g, in ? ~static_cast<uint32_t>(cx) : 0xffffffffu, cg::less<uint32_t>());
-  const uint32_t hy = cg::reduce(g, in ? ~static_cast<uint32_t>(cy) : 0xffffffffu, cg::less<uint32_t>());
-  const uint32_t hz = cg::reduce(g, in ? ~static_cast<uint32_t>(cz) : 0xffffffffu, cg::less<uint32_t>());
-  if (g.thread_rank() == 0 && lx != 0xffffffffu) {
-    atomicMin(&gs->lo[0], lx);
-    atomicMin(&gs->lo[1], ly);
-    atomicMin(&gs->lo[2], lz);
-    atomicMin(&gs->hi_inv[0], hx);
-    atomicMin(&gs->hi_inv[1], hy);
-    atomicMin(&gs->hi_inv[2], hz);
-  }
-}
-
 struct BoxInfo {
   int x0, y0, z0;
   uint32_t bx, by, bz, L;
@@ -587,6 +559,12 @@ __device__ __forceinline__ BoxInfo box_from_state(const GridState* gs) {
   return b;
 }
 
+__device__ __forceinline__ uint32_t local_of(const BoxInfo& b, uint32_t key) {
+  if (key == kSentinel) return b.L;
+  int x = static_cast<int>(key & 1023u), y = static_cast<int>((key >> 10) & 1023u), z = static_cast<int>(key >> 20);
+  return static_cast<uint32_t>(x - b.x0) + b.bx * (static_cast<uint32_t>(y - b.y0) + b.by * static_cast<uint32_t>(z - b.z0));
+}
+
 #ifndef CLAY_ONLY_NEIGHBOUR_PASSES
 // ---------------------------------------------------------------------------------------
 // emit (fluid.ts:268-291). pow(r.x, 1/3) is taken in binary64 and rounded to f32;
@@ -610,27 +588,35 @@ __global__ void k_emit(const SceneDev* __restrict__ scenes, const Work* __restri
     q.b = make_float4(P.emit_vel[0], P.emit_vel[1], P.emit_vel[2], 0.0f);
     q.c = make_float4(P.emit_vel[0], P.emit_vel[1], P.emit_vel[2], 0.0f);
     S.parts[slot] = q;
-    int cx, cy, cz;
-    cell_of(S, q.a.x, q.a.y, q.a.z, cx, cy, cz);
-    box_accumulate(S.gs, in_grid(S, cx, cy, cz), cx, cy, cz);
     if (!work) break;
   }
 }
 
 // ---------------------------------------------------------------------------------------
-// The box of occupied cells of particles [0, n) from scratch (fluid.ts:318-322 for inGrid),
-// after an upload has replaced them; every other write of positions (emission, the integrate)
-// adds its cells to the accumulators itself. The caller clears the accumulators first.
-__global__ void k_cell_box(const SceneDev* __restrict__ scenes, uint32_t n) {
-  const SceneDev& S = scenes[0];
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+// Cell build, pass 1: the cell of every live particle (packed x|y<<10|z<<20, or the
+// sentinel when !inGrid, fluid.ts:318-322) and the bounding box of occupied cells. The
+// first block of a scene also clears the contact counter (fluid.ts:302-304) and the
+// bucket-overflow flag.
+__global__ void k_cell_key(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
+  Work w = get_work(work);
+  const SceneDev& S = scenes[w.obj];
+  if (substep >= S.substeps) return;
+  uint32_t count = work_count(S);
+  uint32_t i = w.first + threadIdx.x;
+  if (w.first == 0 && threadIdx.x == 0) {
+    S.contacts->count = 0u;
+    S.gs->overflow = 0u;
+  }
   uint32_t lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
   uint32_t hinv[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu};
-  if (i < n) {
-    const float4 p = S.parts[i].a;
+  if (i < count && threadIdx.x < w.n) {
+    float4 p = S.parts[i].a;
     int cx, cy, cz;
     cell_of(S, p.x, p.y, p.z, cx, cy, cz);
-    if (in_grid(S, cx, cy, cz)) {
+    bool in = cx >= 0 && cy >= 0 && cz >= 0 && cx < S.G && cy < S.G && cz < S.G;
+    uint32_t key = kSentinel;
+    if (in) {
+      key = static_cast<uint32_t>(cx) | (static_cast<uint32_t>(cy) << 10) | (static_cast<uint32_t>(cz) << 20);
       lo[0] = cx;
       lo[1] = cy;
       lo[2] = cz;
@@ -638,6 +624,7 @@ __global__ void k_cell_box(const SceneDev* __restrict__ scenes, uint32_t n) {
       hinv[1] = ~static_cast<uint32_t>(cy);
       hinv[2] = ~static_cast<uint32_t>(cz);
     }
+    S.key[i] = key;
   }
   // warp then block reduction of the box
 #pragma unroll
@@ -663,13 +650,8 @@ __global__ void k_cell_box(const SceneDev* __restrict__ scenes, uint32_t n) {
   }
 }
 
-// Cell build, pass 1: every live particle's cell (fluid.ts:318-322: the out-of-grid bucket L
-// when !inGrid) as its local index in the box of occupied cells, which the writes of the
-// positions accumulated (emission, the last integrate, or k_cell_box after an upload), and
-// per-cell counts with warp-aggregated atomics; every particle keeps its provisional slot.
-// The scene's first block publishes the box for the later passes. A box that holds more than
-// the occupied cells changes nothing: the cells keep their (z, y, x) order and the extra ones
-// stay empty.
+// Cell build, pass 2: per-cell counts with warp-aggregated atomics; every particle keeps
+// its provisional slot. The scene's first block publishes the box for the later passes.
 __global__ void k_cell_count(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
@@ -690,18 +672,7 @@ __global__ void k_cell_count(const SceneDev* __restrict__ scenes, const Work* __
   bool act = i < count && threadIdx.x < w.n;
   uint32_t l = 0xffffffffu;
   if (act) {
-    const float4 p = S.parts[i].a;
-    int cx, cy, cz;
-    cell_of(S, p.x, p.y, p.z, cx, cy, cz);
-    l = b.L;
-    if (in_grid(S, cx, cy, cz)) {
-      const int x = cx - b.x0, y = cy - b.y0, z = cz - b.z0;
-      // every cell written since the last build is in the box; one outside it (none, by
-      // construction) would join the out-of-grid bucket rather than count past the grid
-      if (x >= 0 && y >= 0 && z >= 0 && x < static_cast<int>(b.bx) && y < static_cast<int>(b.by) &&
-          z < static_cast<int>(b.bz))
-        l = static_cast<uint32_t>(x) + b.bx * (static_cast<uint32_t>(y) + b.by * static_cast<uint32_t>(z));
-    }
+    l = local_of(b, S.key[i]);
     S.key[i] = l;
   }
   // warp-aggregated increment: one atomic per distinct cell per warp
@@ -714,23 +685,18 @@ __global__ void k_cell_count(const SceneDev* __restrict__ scenes, const Work* __
     base = __shfl_sync(peers, base, leader);
     uint32_t rank = base + __popc(peers & ((1u << lane) - 1u));
     S.rank[i] = rank;
+    if (l != b.L && base + __popc(peers) > S.bucket) S.gs->overflow = 1u;
   }
 }
 
-// Cell build, pass 2a: partial sums of the counts of [0, L] split into `parts_scan`
-// parts. Part 0 also clears the contact counter (fluid.ts:302-304) and the bucket-overflow
-// flag (the final scan sets it), and resets the box accumulators, which the positions this
-// substep's integrate writes fill again for the next build.
+// Cell build, pass 3a: partial sums of the counts of [0, L] split into `parts_scan`
+// parts. Part 0 also resets the box accumulators for the next substep.
 __global__ void k_scan_partial(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
   if (substep >= S.substeps) return;
-  GridState* gs = S.gs;
-  if (w.sub == 0 && threadIdx.x == 0) {
-    S.contacts->count = 0u;
-    gs->overflow = 0u;
-  }
   if (work_count(S) == 0) return;
+  GridState* gs = S.gs;
   uint32_t n = gs->L + 1;
   uint32_t P = S.parts_scan;
   uint32_t per = (n + P - 1) / P;
@@ -752,14 +718,13 @@ __global__ void k_scan_partial(const SceneDev* __restrict__ scenes, const Work* 
   }
 }
 
-// Cell build, pass 2b: exclusive scan into cell_start[0 .. L+1], counts cleared behind; a
-// grid cell holding more than `bucket` particles sets the overflow flag (fluid.ts:323-329).
+// Cell build, pass 3b: exclusive scan into cell_start[0 .. L+1], counts cleared behind.
 __global__ void k_scan_final(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
   if (substep >= S.substeps) return;
   if (work_count(S) == 0) return;
-  GridState* gs = S.gs;
+  const GridState* gs = S.gs;
   uint32_t n = gs->L + 1;
   uint32_t P = S.parts_scan;
   uint32_t per = (n + P - 1) / P;
@@ -799,7 +764,6 @@ __global__ void k_scan_final(const SceneDev* __restrict__ scenes, const Work* __
     if (c < end) {
       S.cell_start[c] = run + before;
       S.counts[c] = 0u;
-      if (c + 1u < n && v > S.bucket) gs->overflow = 1u;  // cell n - 1 = L is the out-of-grid bucket
     }
     uint32_t tot = s_warp[nw - 1];
     __syncthreads();
@@ -809,7 +773,7 @@ __global__ void k_scan_final(const SceneDev* __restrict__ scenes, const Work* __
   if (n == 0 && threadIdx.x == 0 && w.sub == 0) S.cell_start[0] = 0;
 }
 
-// Cell build, pass 3: provisional placement.
+// Cell build, pass 4: provisional placement.
 __global__ void k_cell_scatter(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
   Work w = get_work(work);
   const SceneDev& S = scenes[w.obj];
@@ -820,7 +784,7 @@ __global__ void k_cell_scatter(const SceneDev* __restrict__ scenes, const Work* 
   S.tmp[S.cell_start[S.key[i]] + S.rank[i]] = i;
 }
 
-// Cell build, pass 4: deterministic order inside each cell (ascending particle index, so
+// Cell build, pass 5: deterministic order inside each cell (ascending particle index, so
 // a full cell keeps its `bucket` lowest indices, fluid.ts:323-329) and the gather of the
 // particle state into cell order.
 __global__ void k_cell_order(const SceneDev* __restrict__ scenes, const Work* __restrict__ work, int substep) {
@@ -1135,9 +1099,6 @@ __device__ __forceinline__ void integrate_particle(const SceneDev& S, const Para
   out.b = make_float4(clx == px ? vx : 0.0f, cly == py ? vy : 0.0f, clz == pz ? vz : 0.0f, mdp.y);
   out.c = make_float4(nvx, nvy, nvz, 0.0f);
   S.parts[S.sorted_id[k]] = out;
-  int cx, cy, cz;
-  cell_of(S, clx, cly, clz, cx, cy, cz);
-  box_accumulate(S.gs, in_grid(S, cx, cy, cz), cx, cy, cz);
 }
 
 // forces (fluid.ts:370-439) fused with integrate (fluid.ts:449-491). The neighbour pass

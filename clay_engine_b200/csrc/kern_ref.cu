@@ -24,10 +24,8 @@ void count_launches(uint64_t n) { g_launches.fetch_add(n); }
 cudaError_t L_emit(const SceneDev* s, const Work* w, int blocks, int threads, cudaStream_t st) {
   CLAY_LAUNCH(k_emit, blocks, threads, st, s, w);
 }
-cudaError_t L_cell_box(const SceneDev* s, uint32_t n, cudaStream_t st) {
-  const int blocks = static_cast<int>((n + 255u) / 256u);
-  if (blocks == 0) return cudaSuccess;
-  CLAY_LAUNCH(k_cell_box, blocks, 256, st, s, n);
+cudaError_t L_cell_key(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
+  CLAY_LAUNCH(k_cell_key, blocks, threads, st, s, w, sub);
 }
 cudaError_t L_cell_count(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st) {
   CLAY_LAUNCH(k_cell_count, blocks, threads, st, s, w, sub);

@@ -25,7 +25,7 @@ constexpr int kBlock = 256;
 constexpr int kDensityVariant = 0;
 
 cudaError_t L_emit(const SceneDev* s, const Work* w, int blocks, int threads, cudaStream_t st);
-cudaError_t L_cell_box(const SceneDev* s, uint32_t n, cudaStream_t st);
+cudaError_t L_cell_key(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
 cudaError_t L_cell_count(const SceneDev* s, const Work* w, int blocks, int threads, int sub, cudaStream_t st);
 cudaError_t L_scan_partial(const SceneDev* s, const Work* w, int blocks, int sub, cudaStream_t st);
 cudaError_t L_scan_final(const SceneDev* s, const Work* w, int blocks, int sub, cudaStream_t st);
