@@ -264,10 +264,9 @@ def test_wide_sheet_bit_exact(root, oracle):
 
 
 def test_upload_far_away_after_stepping_bit_exact(root, oracle):
-    """The cell build starts from a box of occupied cells that the writes of positions keep
-    (emission, the integrate, and a box pass after an upload). A sim stepped at one place and
-    then given particles at another, far outside the old box, must still sort and step them
-    exactly as the oracle does; then a spawn adds particles outside the new box too."""
+    """A sim stepped at one place and then given particles at another, far outside its old box
+    of occupied cells, sorts and steps them exactly as the oracle does (the cell build takes
+    the box from the records every substep); then a spawn adds particles outside the new box."""
     sim, ref, keep = make_pair(root, oracle, dict(CFG1), blob(12, center=(-6.0, 2.0, -6.0)), with_collider=False)
     for frame in range(2):
         sim.step()
