@@ -936,8 +936,9 @@ int fluid_options(const clay_fluid_opts& o, clay_fluid* f) {
     for (int k = 0; k < 3; k++) org[k] = o.origin[k];
   for (int k = 0; k < 3; k++) f->origin[k] = org[k];
   f->substeps = (o.set & CLAY_FLUID_SUBSTEPS) ? o.substeps : 3;
-  if (f->capacity <= 0 || f->capacity > (1ll << 30))
-    return fail(CLAY_EINVAL, "FluidSim: capacity %lld must be in 1..2^30", static_cast<long long>(f->capacity));
+  if (f->capacity <= 0 || f->capacity > kMaxCapacity)
+    return fail(CLAY_EINVAL, "FluidSim: capacity %lld must be in 1..%lld", static_cast<long long>(f->capacity),
+                static_cast<long long>(kMaxCapacity));
   if (!(f->spacing > 0) || !(f->h > 0) || f->bucket <= 0 || f->substeps < 0)
     return fail(CLAY_EINVAL, "FluidSim: spacing, smoothing and bucket must be positive and substeps non-negative");
   return CLAY_OK;

@@ -18,6 +18,10 @@ constexpr int kMaxLeaves = 8;
 constexpr int kMaxParts = 64;
 constexpr int kMaxMips = 8;
 constexpr uint32_t kMaxNbr = 64;  // neighbour-list slots per particle
+// Largest scene: the neighbour list is addressed in 32-bit words, slot-major (slot j of particle
+// k at word (j / 4) * 4 * capacity + j % 4), so every such offset must stay below 2^32.
+constexpr int64_t kMaxCapacity = int64_t{1} << 26;
+static_assert((kMaxNbr / 4) * 4 * static_cast<uint64_t>(kMaxCapacity) <= (uint64_t{1} << 32), "list offsets");
 constexpr int kSplatWarps = 8;  // warps per block of the splat pass
 constexpr int kSplatItems = 2048;  // compacted (brick, slice) items of the sphere block walk
 constexpr int kSplatStencil = 2048;  // voxel offsets of the own-box walk's stencil (8 KB of shared memory)

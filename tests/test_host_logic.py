@@ -55,3 +55,17 @@ def test_solver_rejects_unknown_options_before_device_work():
     with pytest.raises(ce.ClayError) as e:
         ce.ClaySolver(None, None, 1, None, 1, None, {"bogus": 1})
     assert "unknown option" in str(e.value)
+
+
+def test_capacity_limit_keeps_list_offsets_in_32_bits():
+    """A scene's neighbour list is addressed in 32-bit words (slot-major, slot j of particle k at
+    (j / 4) * 4 * capacity + j % 4): capacities above 2^26 are refused before any allocation."""
+    import pytest as _pytest
+
+    from clay_engine_b200 import core
+
+    base = dict(spacing=0.1, radius=0.05, substeps=2, worldSize=24.0, origin=(-12.0, -4.0, -12.0),
+                bakeResolution=64, bakeMipLevels=3, bakeBand=4.0)
+    assert core.fluid_estimate_bytes(dict(base, capacity=1 << 26)) > (1 << 26) * 384
+    with _pytest.raises(Exception, match="capacity"):
+        core.fluid_estimate_bytes(dict(base, capacity=(1 << 26) + 1))
