@@ -288,7 +288,7 @@ enum {
  * fluid.ts:141-160,184-203. */
 typedef struct clay_fluid_opts {
   uint32_t set;
-  int64_t capacity;        /* ?? 8192 */
+  int64_t capacity;        /* ?? 8192; at most 2^26 (the neighbour list is addressed in 32-bit words) */
   double spacing;          /* ?? 0.45 */
   double smoothing;        /* ?? spacing * 2.2 */
   int32_t bucket;          /* ?? 64 */
